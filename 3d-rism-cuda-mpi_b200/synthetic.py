@@ -1,0 +1,126 @@
+"""Seeded synthetic solutes for the benchmark configurations, written as the
+reference's .inp decks (read_input.cu:21-97 format) so that the reference
+build, the CPU oracle and this solver all read the same input.
+
+Configurations (sizes and distributions of the headline benchmark):
+  c1  20 atoms in a 6 A sphere, min pair distance 1.1 A, sigma U(2.5, 3.8) A,
+      eps U(0.05, 0.25) kcal/mol, q N(0, 0.35) neutralised; 32 A box, 64^3
+      grid, KH, pure water.
+  c2  2,000-atom compact globule at ~0.05 atoms/A^3 (R ~ 21.2 A), min
+      separation 1.0 A, element labels 50/25/15/10 % C/H/O/N (labels only),
+      sigma U(1.0, 3.8) A, eps U(0.05, 0.25) kcal/mol, q N(0, 0.4)
+      neutralised; 128 A box, 256^3 grid, KH, 0.2 M NaCl water (n = 4).
+  c3  12,877 atoms, same recipe (R ~ 39.5 A); 256 A box, 512^3 grid.
+  small(N, grid, box) the same recipe at any size, for tests.
+"""
+import math
+import os
+
+import numpy as np
+
+KCAL2J = 4184.0
+SEEDS = {"c1": 1001, "c2": 2002, "c3": 3003, "c4": 4004, "c5": 5005}
+
+
+def _sphere_points(rng, n, radius, dmin):
+    """Rejection-sample n points uniformly in a sphere with a minimum
+    pairwise distance, using a cell hash so large n stays fast."""
+    cell = dmin
+    grid = {}
+    pts = np.empty((n, 3))
+    k = 0
+    tries = 0
+    while k < n:
+        tries += 1
+        if tries > 200 * n + 10000:
+            raise RuntimeError("cannot place atoms: sphere too dense")
+        p = rng.uniform(-radius, radius, 3)
+        if p @ p > radius * radius:
+            continue
+        c = tuple(np.floor(p / cell).astype(int))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
+                        d = pts[j] - p
+                        if d @ d < dmin * dmin:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if not ok:
+            continue
+        pts[k] = p
+        grid.setdefault(c, []).append(k)
+        k += 1
+    return pts
+
+
+def make_solute(nu, seed, radius=None, dmin=1.0, sig=(1.0, 3.8), eps=(0.05, 0.25),
+                qsd=0.4, density=0.05):
+    rng = np.random.default_rng(seed)
+    if radius is None:
+        radius = (3.0 * nu / (4.0 * math.pi * density)) ** (1.0 / 3.0)
+    r = _sphere_points(rng, nu, radius, dmin)
+    s = rng.uniform(sig[0], sig[1], nu)
+    e = rng.uniform(eps[0], eps[1], nu) * KCAL2J
+    q = rng.normal(0.0, qsd, nu)
+    q -= q.mean()
+    labels = rng.choice(np.array(list("CHON")), nu, p=[0.5, 0.25, 0.15, 0.10])
+    return dict(sig=s, eps=e, q=q, r=r, labels=labels)
+
+
+def write_inp(path, solute, box, grid, solvent, closure="KH", tol=1e-6,
+              maxstep=10000, mixer=(2, 0.6, 0.2), outlist="m"):
+    """Write a .inp deck in the reference's format (version 20220301)."""
+    with open(path, "w") as f:
+        f.write(f" {outlist}    0\t 20220301\n")
+        f.write(f" {closure}\n {solvent}\n")
+        f.write(f" {tol:.1e}   {maxstep}\n")
+        f.write(f" {mixer[0]}   {mixer[1]}   {mixer[2]}\n")
+        f.write("  {}  {}  {}\n".format(*[repr(float(b)) for b in box]))
+        f.write("  {}  {}  {}\n".format(*[int(g) for g in grid]))
+        nu = len(solute["q"])
+        f.write(f" {nu}\n")
+        for i in range(nu):
+            x, y, z = solute["r"][i]
+            f.write(f"{solute['sig'][i]:.6f} {solute['eps'][i]:.6f} {solute['q'][i]:.8f} "
+                    f"{x:.6f} {y:.6f} {z:.6f}\n")
+    return path
+
+
+def config(name, outdir, solvent_dir=None, **over):
+    """Write the deck for one named configuration; returns the .inp path.
+    `solvent_dir`: where the .xvk files live (copied next to the deck by the
+    caller or referenced by absolute path)."""
+    os.makedirs(outdir, exist_ok=True)
+    if name == "c1":
+        sol = make_solute(20, SEEDS["c1"], radius=6.0, dmin=1.1, sig=(2.5, 3.8), qsd=0.35)
+        kw = dict(box=(32.0,) * 3, grid=(64,) * 3, solvent="h2o_vv.xvk")
+    elif name == "c2":
+        sol = make_solute(2000, SEEDS["c2"])
+        kw = dict(box=(128.0,) * 3, grid=(256,) * 3, solvent="naclaq_vv.xvk")
+    elif name == "c3":
+        sol = make_solute(12877, SEEDS["c3"])
+        kw = dict(box=(256.0,) * 3, grid=(512,) * 3, solvent="naclaq_vv.xvk")
+    else:
+        raise ValueError(name)
+    kw.update(over)
+    if solvent_dir:
+        kw["solvent"] = os.path.join(solvent_dir, kw["solvent"])
+    return write_inp(os.path.join(outdir, f"{name}.inp"), sol, **kw)
+
+
+def small(outdir, nu=12, grid=32, box=16.0, solvent="h2o_vv.xvk", seed=7, closure="KH",
+          name="small", mixer=(2, 0.6, 0.2), **kw):
+    """A small deck for parity tests."""
+    g = grid if isinstance(grid, (tuple, list)) else (grid,) * 3
+    b = box if isinstance(box, (tuple, list)) else (box,) * 3
+    sol = make_solute(nu, seed, radius=min(3.0, min(b) / 5), dmin=1.1, sig=(2.5, 3.8), qsd=0.35)
+    return write_inp(os.path.join(outdir, f"{name}.inp"), sol, b, g, solvent,
+                     closure=closure, mixer=mixer, **kw)
