@@ -1,0 +1,1182 @@
+// r3d_api.cu -- C-ABI and host runtime of the B200 3D-RISM solver.
+//
+// A context mirrors one RISM3D object of the reference (rism3d.h:21-105):
+// load the control/solute deck and the solvent table, initialise the grids,
+// iterate, output.  All device memory is owned by the context; one iteration
+// is captured once as a CUDA graph and replayed, with convergence decided on
+// the device (see k_reduce) so the host only polls every few iterations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rism3d_b200.h"
+#include "r3d_internal.h"
+
+namespace r3d {
+struct Batch {
+  const Desc *d;
+  const int *prefix;
+  int ns;
+};
+struct AtomTab {
+  const double *x, *y, *z, *q;
+  const double *isig2, *eps4;
+  int nu;
+};
+size_t smem_x(int hx, int n, int S, size_t csz);
+size_t smem_y(int ny, int P, size_t csz);
+size_t smem_z(int nz, int n, int P, size_t csz);
+void kernels_set_smem(bool fp64, size_t maxbytes);
+template <typename P>
+void launch_fwd_x(Batch, int, size_t, cudaStream_t, int, const void *);
+template <typename P>
+void launch_fft_y(Batch, int, size_t, cudaStream_t, int, int);
+template <typename P>
+void launch_zoz(Batch, int, size_t, cudaStream_t, int, int);
+template <typename P>
+void launch_inv_x(Batch, int, size_t, cudaStream_t, int, void *, int);
+void launch_reduce(const Desc *, const int *, int, int, cudaStream_t);
+template <typename P>
+void launch_mix_an2(Batch, int, cudaStream_t);
+template <typename P>
+void launch_anm(Batch, int, const Desc *, const int *, int, cudaStream_t, int);
+template <typename P>
+void launch_potential(const Desc &, const AtomTab &, double, double,
+                      const double *, int, double *, cudaStream_t);
+void launch_phase_tables(double2 *, double2 *, double2 *, const double *,
+                         const double *, const double *, int, int, int, int,
+                         const double *, cudaStream_t);
+void launch_fk(const Desc &, double2 *, const double2 *, const double2 *,
+               const double2 *, const double *, int, double, const double *,
+               double, cudaStream_t);
+template <typename P>
+void launch_cref(const Desc &, double *, cudaStream_t);
+template <typename P>
+void launch_lr_update(const double *, void *, long long, cudaStream_t);
+void launch_kidx(const Desc &, const uint32_t *, int, cudaStream_t);
+template <typename P>
+void launch_thermo(const Desc &, const void *, double *, int, cudaStream_t);
+template <typename P>
+void launch_gh(const Desc &, const void *, double *, double *, cudaStream_t);
+template <typename P>
+void launch_to_double(const void *, double *, long long, int, cudaStream_t);
+template <typename P>
+void launch_from_double(const double *, void *, long long, int, cudaStream_t);
+template <typename P>
+void launch_shift_qfr(const Desc &, const void *, double *, double, int,
+                      cudaStream_t);
+template <typename P>
+void launch_set_short(const Desc &, const double *, void *, cudaStream_t);
+
+namespace phys {
+constexpr double avogadro = 6.02214076e23;
+constexpr double bohr = 0.5291771500001;
+constexpr double boltzmann = 1.380649e-23;
+constexpr double hartree = 4.359744722207185e-18;
+}  // namespace phys
+
+constexpr size_t kSmemBudget = 100 * 1024;  // per CTA: two CTAs per SM
+constexpr size_t kSmemMax = 220 * 1024;
+constexpr int kNumSM = 148;
+
+}  // namespace r3d
+
+using namespace r3d;
+
+static std::string g_last_error;
+
+// Launch geometry of the five grid passes for one (grid, sites, precision).
+struct Geo {
+  int tiles_x = 0, tiles_y = 0, tiles_z = 0, ix_ctas = 0, ix_per = 1, mix_ctas = 0;
+  size_t smx = 0, smy = 0, smz = 0;
+};
+
+struct r3d_ctx {
+  r3d_opts opts{};
+  Problem prob;
+  std::string err;
+  bool fp64 = true;
+  size_t rsz = 8;
+  int mixer = MIX_AN2, history = 2;
+  double damping = -1;  // <0: use the .inp m
+  std::string inp_dir;
+  cudaStream_t stream = nullptr;
+  bool initialized = false;
+  // device memory
+  std::vector<void *> allocs;
+  size_t bytes = 0;
+  void *u = nullptr, *t = nullptr, *fr = nullptr, *res = nullptr, *w = nullptr,
+       *fk = nullptr, *chi = nullptr, *lr = nullptr, *hist_a = nullptr,
+       *hist_b = nullptr, *cref = nullptr, *chi64 = nullptr;
+  double next_refresh = 0;  // mixed path: refresh when rms drops below this
+  uint32_t *kidx = nullptr;
+  double *partials = nullptr, *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  Ctl *ctl = nullptr;
+  Desc *ddesc = nullptr;
+  int *dprefix = nullptr;  // [5][2]: prefix arrays of the passes + ix ctas
+  Desc desc{};
+  int nshell = 0;
+  // launch geometry
+  int tiles_x = 0, tiles_y = 0, tiles_z = 0, ix_ctas = 0, ix_per = 1,
+      mix_ctas = 0;
+  size_t smx = 0, smy = 0, smz = 0;
+  // graph of one iteration
+  cudaGraphExec_t gexec = nullptr;
+  double ms_per_iter = 0;
+  int kernels_per_iter = 0;
+};
+
+// ------------------------------------------------------------------ utils
+static int fail(r3d_ctx *c, int code, const std::string &m) {
+  if (c) c->err = m;
+  g_last_error = m;
+  return code;
+}
+#define CK(call)                                                          \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess)                                                \
+      return fail(c, R3D_ECUDA, std::string(#call) + ": " +               \
+                                    cudaGetErrorString(e_));              \
+  } while (0)
+
+static int dalloc(r3d_ctx *c, void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(c, R3D_ENOMEM, "cudaMalloc(" + std::to_string(bytes) +
+                                   ") failed: " + cudaGetErrorString(e));
+  }
+  c->allocs.push_back(*p);
+  c->bytes += bytes;
+  return R3D_OK;
+}
+
+static void free_all(r3d_ctx *c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+  for (void *p : c->allocs) cudaFree(p);
+  c->allocs.clear();
+  c->bytes = 0;
+  c->initialized = false;
+}
+
+// ------------------------------------------------------------- lifetime
+extern "C" int r3d_create(const r3d_opts *opts, r3d_ctx **out) {
+  if (!out) return fail(nullptr, R3D_EINVAL, "out is NULL");
+  *out = nullptr;
+  r3d_ctx *c = new r3d_ctx();
+  if (opts) c->opts = *opts;
+  if (c->opts.precision != R3D_FP64 && c->opts.precision != R3D_MIXED) {
+    delete c;
+    return fail(nullptr, R3D_EINVAL, "precision must be R3D_FP64 or R3D_MIXED");
+  }
+  c->fp64 = c->opts.precision == R3D_FP64;
+  c->rsz = c->fp64 ? 8 : 4;
+  if (c->opts.device < 0) {  // host-only context: loaders, planning, no GPU
+    *out = c;
+    return R3D_OK;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    delete c;
+    return fail(nullptr, R3D_ECUDA, std::string("no CUDA device: ") +
+                                        cudaGetErrorString(e));
+  }
+  if (c->opts.device < 0 || c->opts.device >= ndev) {
+    delete c;
+    return fail(nullptr, R3D_EINVAL, "device ordinal out of range");
+  }
+  e = cudaSetDevice(c->opts.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(nullptr, R3D_ECUDA, std::string("stream: ") + cudaGetErrorString(e));
+  }
+  *out = c;
+  return R3D_OK;
+}
+
+extern "C" int r3d_destroy(r3d_ctx *c) {
+  if (!c) return R3D_OK;
+  if (c->opts.device < 0) {
+    delete c;
+    return R3D_OK;
+  }
+  cudaSetDevice(c->opts.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return R3D_OK;
+}
+
+extern "C" const char *r3d_last_error(const r3d_ctx *c) {
+  return c ? c->err.c_str() : g_last_error.c_str();
+}
+
+// ---------------------------------------------------------------- input
+extern "C" int r3d_set_ad(r3d_ctx *c, double lambda, int adswitch) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (c->initialized) return fail(c, R3D_ESTATE, "set_ad after initialize");
+  c->prob.lambda = lambda;
+  c->prob.adswitch = adswitch;
+  return R3D_OK;
+}
+
+extern "C" int r3d_load_inp(r3d_ctx *c, const char *inp, const char *structure,
+                            int centering, int q0) {
+  if (!c || !inp) return fail(c, R3D_EINVAL, "ctx or inp is NULL");
+  if (c->initialized) return fail(c, R3D_ESTATE, "load_inp after initialize");
+  Problem p;
+  p.adswitch = c->prob.adswitch;
+  p.lambda = c->prob.lambda;
+  std::string m = parse_inp(p, inp, structure ? structure : "", centering != 0, q0 != 0);
+  if (!m.empty())
+    return fail(c, m.rfind("cannot open", 0) == 0 ? R3D_EIO : R3D_EINVAL, m);
+  // keep a solvent that was loaded before
+  if (c->prob.has_solvent) {
+    p.natv = c->prob.natv;
+    p.ntab = c->prob.ntab;
+    p.temper = c->prob.temper;
+    p.xt = c->prob.xt;
+    p.sigv = c->prob.sigv;
+    p.epsv = c->prob.epsv;
+    p.qv = c->prob.qv;
+    p.rhov = c->prob.rhov;
+    p.ttab = c->prob.ttab;
+    p.xvv = c->prob.xvv;
+    p.has_solvent = true;
+  }
+  c->prob = std::move(p);
+  std::string ip(inp);
+  size_t sl = ip.rfind('/');
+  c->inp_dir = sl == std::string::npos ? std::string() : ip.substr(0, sl + 1);
+  return R3D_OK;
+}
+
+extern "C" int r3d_load_xvk(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (c->initialized) return fail(c, R3D_ESTATE, "load_xvk after initialize");
+  std::string p;
+  if (path) {
+    p = path;
+  } else {
+    if (c->prob.fsolvent.empty())
+      return fail(c, R3D_ESTATE, "no solvent file named: load an .inp first");
+    p = c->prob.fsolvent;
+    FILE *f = std::fopen(p.c_str(), "r");
+    if (f)
+      std::fclose(f);
+    else if (p[0] != '/')
+      p = c->inp_dir + p;
+  }
+  std::string m = parse_xvk(c->prob, p);
+  if (!m.empty())
+    return fail(c, m.find("could not be opened") != std::string::npos ? R3D_EIO : R3D_EINVAL, m);
+  return R3D_OK;
+}
+
+extern "C" int r3d_set_problem(r3d_ctx *c, const r3d_problem *q) {
+  if (!c || !q) return fail(c, R3D_EINVAL, "ctx or problem is NULL");
+  if (c->initialized) return fail(c, R3D_ESTATE, "set_problem after initialize");
+  if (q->nu < 0 || q->natv <= 0 || q->natv > kMaxSites || q->ntab < 4 || !(q->dr > 0))
+    return fail(c, R3D_EINVAL, "bad problem sizes");
+  Problem p;
+  p.adswitch = c->prob.adswitch;
+  p.lambda = c->prob.lambda;
+  for (int d = 0; d < 3; ++d) {
+    p.grid[d] = q->grid[d];
+    p.box[d] = q->box[d];
+    if (p.grid[d] < 4 || (p.grid[d] & 1) || p.grid[d] > 2048 || !(p.box[d] > 0))
+      return fail(c, R3D_EINVAL, "grid must be even, 4..2048, and the box positive");
+  }
+  p.clos = q->closure;
+  p.pse_n = q->closure == R3D_KH ? 1 : std::max(1, q->pse_n);
+  p.convergence = q->convergence;
+  p.maxstep = q->maxstep;
+  p.count = q->count;
+  p.mix_m = q->m;
+  p.mix_mp = q->mp;
+  p.sig.assign(q->sig, q->sig + q->nu);
+  p.eps.assign(q->eps, q->eps + q->nu);
+  p.q.assign(q->q, q->q + q->nu);
+  p.r.assign(q->xyz, q->xyz + 3 * q->nu);
+  p.natv = q->natv;
+  p.sigv.assign(q->sigv, q->sigv + q->natv);
+  p.epsv.assign(q->epsv, q->epsv + q->natv);
+  p.qv.assign(q->qv, q->qv + q->natv);
+  p.rhov.assign(q->rhov, q->rhov + q->natv);
+  p.temper = q->temper;
+  p.xt = q->xt;
+  p.ntab = q->ntab;
+  p.xvv.assign(q->xvv, q->xvv + (size_t)q->natv * q->natv * q->ntab);
+  double dk = M_PI / (q->dr * q->ntab);
+  p.ttab.resize(q->ntab);
+  for (int i = 0; i < q->ntab; ++i) p.ttab[i] = dk * (i + 1);
+  p.fname = "r3d";
+  p.has_solute = p.has_solvent = true;
+  c->prob = std::move(p);
+  return R3D_OK;
+}
+
+extern "C" int r3d_set_closure(r3d_ctx *c, int clos, int pse_n) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (clos < R3D_KH || clos > R3D_PSE || (clos == R3D_PSE && pse_n < 1))
+    return fail(c, R3D_EINVAL, "unknown closure");
+  c->prob.clos = clos;
+  c->prob.pse_n = clos == R3D_KH ? 1 : pse_n;
+  if (c->initialized) {
+    c->desc.clos = c->prob.clos;
+    c->desc.pse_n = c->prob.pse_n;
+    CK(cudaMemcpy(c->ddesc, &c->desc, sizeof(Desc), cudaMemcpyHostToDevice));
+  }
+  return R3D_OK;
+}
+
+extern "C" int r3d_set_mixer(r3d_ctx *c, int mixer, int history, double damping) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (c->initialized) return fail(c, R3D_ESTATE, "set_mixer after initialize");
+  if (mixer != R3D_MIX_AN2 && mixer != R3D_MIX_ANM)
+    return fail(c, R3D_EINVAL, "unknown mixer");
+  if (mixer == R3D_MIX_ANM && (history < 1 || history > kMaxHistory))
+    return fail(c, R3D_EINVAL, "history must be 1.." + std::to_string(kMaxHistory));
+  c->mixer = mixer;
+  c->history = mixer == R3D_MIX_AN2 ? 2 : history;
+  c->damping = damping;
+  return R3D_OK;
+}
+
+extern "C" int r3d_set_control(r3d_ctx *c, double convergence, int maxstep) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (convergence > 0) c->prob.convergence = convergence;
+  if (maxstep > 0) c->prob.maxstep = maxstep;
+  return R3D_OK;
+}
+
+// ------------------------------------------------------------ geometry
+static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites);
+static int plan_geometry(r3d_ctx *c, Desc &d) {
+  Geo g;
+  int rc = plan_geo(c, d, g, c->fp64, c->prob.natv);
+  if (rc) return rc;
+  c->tiles_x = g.tiles_x;
+  c->tiles_y = g.tiles_y;
+  c->tiles_z = g.tiles_z;
+  c->ix_ctas = g.ix_ctas;
+  c->ix_per = g.ix_per;
+  c->mix_ctas = g.mix_ctas;
+  c->smx = g.smx;
+  c->smy = g.smy;
+  c->smz = g.smz;
+  return R3D_OK;
+}
+
+static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
+  const Problem &p = c->prob;
+  d.nx = p.grid[0];
+  d.ny = p.grid[1];
+  d.nz = p.grid[2];
+  d.n = nsites;
+  d.hx = d.nx / 2;
+  d.N = (long long)d.nx * d.ny * d.nz;
+  d.Nh = (long long)d.hx * d.ny * d.nz;
+  d.nrad_x = factor_length(d.hx, d.rad_x);
+  d.nrad_y = factor_length(d.ny, d.rad_y);
+  d.nrad_z = factor_length(d.nz, d.rad_z);
+  if (d.nrad_x < 0 || d.nrad_y < 0 || d.nrad_z < 0)
+    return fail(c, R3D_EINVAL, "grid sizes must factor into primes <= 13");
+  const size_t cs = fp64 ? 16 : 8;
+  const int rowsN = d.ny * d.nz;
+  int S = 16;
+  while (S > 1 && (rowsN % S || smem_x(d.hx, d.n, S, cs) > kSmemBudget)) S >>= 1;
+  while (S > 1 && rowsN / S < 2 * kNumSM) S >>= 1;
+  int Py = fp64 ? 8 : 16;
+  while (Py > 1 && (d.hx % Py || smem_y(d.ny, Py, cs) > kSmemBudget)) Py >>= 1;
+  int Pz = fp64 ? 4 : 8;
+  while (Pz > 1 && (d.hx % Pz || smem_z(d.nz, d.n, Pz, cs) > kSmemBudget)) Pz >>= 1;
+  d.rows = S;
+  d.ycols = Py;
+  d.zcols = Pz;
+  g.smx = smem_x(d.hx, d.n, S, cs);
+  g.smy = smem_y(d.ny, Py, cs);
+  g.smz = smem_z(d.nz, d.n, Pz, cs);
+  if (g.smx > kSmemMax || g.smy > kSmemMax || g.smz > kSmemMax)
+    return fail(c, R3D_EINVAL, "grid too large for one CTA's shared memory");
+  d.tiles_x = rowsN / S;
+  d.tiles_y = d.n * d.nz * (d.hx / Py);
+  d.tiles_z = d.ny * (d.hx / Pz);
+  g.tiles_x = d.tiles_x;
+  g.tiles_y = d.tiles_y;
+  g.tiles_z = d.tiles_z;
+  g.ix_ctas = std::min(d.tiles_x, 4 * kNumSM);
+  g.ix_per = (d.tiles_x + g.ix_ctas - 1) / g.ix_ctas;
+  g.ix_ctas = (d.tiles_x + g.ix_per - 1) / g.ix_per;
+  long long niv = (long long)d.n * d.N;
+  g.mix_ctas = (int)std::min<long long>((niv + kThreads - 1) / kThreads, 8 * kNumSM);
+  return R3D_OK;
+}
+
+// Refresh (also the setup's long-range term): freeze c_ref = c_s(t) (zero at
+// setup) and set lr = 1 + h_ref, h_ref = F^-1[chi (F(c_ref) - q phi_L(k))],
+// with the FP64 pass kernels.  Leaves t, R and the mixer state untouched: the
+// residual of the current t is unchanged in exact arithmetic.
+template <typename P>
+static int refresh(r3d_ctx *c, bool zero) {
+  const Desc &d = c->desc;
+  const int n = d.n;
+  const long long N = d.N, Nh = d.Nh;
+  cudaStream_t s = c->stream;
+  Desc dr{};
+  Geo g;
+  int rc = plan_geo(c, dr, g, true, n);
+  if (rc) return rc;
+  char *tmp = nullptr;
+  const size_t bytes = (size_t)n * N * 8 + (size_t)n * Nh * 16 + sizeof(Desc) + sizeof(Ctl) + 64;
+  CK(cudaMalloc((void **)&tmp, bytes));
+  double *c64 = (double *)tmp;                      // c_ref, then h_ref
+  double2 *w64 = (double2 *)(c64 + (size_t)n * N);  // n half spectra
+  Desc *dd = (Desc *)(w64 + (size_t)n * Nh);
+  Ctl *ctl = (Ctl *)((char *)dd + sizeof(Desc));
+  int *pre = (int *)((char *)ctl + sizeof(Ctl));
+  if (zero)
+    CK(cudaMemsetAsync(c64, 0, (size_t)n * N * 8, s));
+  else
+    launch_cref<P>(d, c64, s);
+  for (int v = 0; v < n; ++v) dr.qv[v] = d.qv[v];
+  dr.clos = d.clos;
+  dr.pse_n = d.pse_n;
+  dr.w = w64;
+  dr.chi = c->chi64;
+  dr.kidx = c->kidx;
+  dr.fk = c->fk;
+  dr.ctl = ctl;
+  int pf[8] = {0, g.tiles_x, 0, g.tiles_y, 0, g.tiles_z, 0, g.ix_ctas};
+  CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
+  CK(cudaMemcpyAsync(dd, &dr, sizeof(Desc), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(pre, pf, sizeof(pf), cudaMemcpyHostToDevice, s));
+  kernels_set_smem(true, kSmemMax);
+  launch_fwd_x<P64>(Batch{dd, pre, 1}, g.tiles_x, g.smx, s, 0, c64);
+  launch_fft_y<P64>(Batch{dd, pre + 2, 1}, g.tiles_y, g.smy, s, -1, 0);
+  launch_zoz<P64>(Batch{dd, pre + 4, 1}, g.tiles_z, g.smz, s, 2, 0);
+  launch_fft_y<P64>(Batch{dd, pre + 2, 1}, g.tiles_y, g.smy, s, 1, 0);
+  launch_inv_x<P64>(Batch{dd, pre + 6, 1}, g.ix_ctas, g.smx, s, 0, c64, g.ix_per);
+  launch_lr_update<P>(c64, c->lr, (long long)n * N, s);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  cudaFree(tmp);
+  return R3D_OK;
+}
+
+static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
+  const size_t R = c->rsz, T = 8, N = (size_t)d.N, n = (size_t)d.n;
+  size_t b = 0;
+  b += 3 * n * N * R + n * N * T;  // u, res, lr (grid type), t (state type)
+  b += n * N * R;                  // w (n half spectra)
+  b += N * R + N * 8;              // fr, fk (FP64 half spectrum)
+  if (!c->fp64) b += n * N * R + (size_t)nshell * n * n * 8;  // cref, chi64
+  b += (size_t)d.Nh * 4;           // kidx
+  b += (size_t)nshell * n * n * R;
+  size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
+  b += slots * n * N * (R + T);    // mixer history (residuals, states)
+  b += (size_t)std::max(c->ix_ctas, c->mix_ctas) * kPartials * 8;
+  b += (size_t)(c->prob.maxstep + 1) * 8 + sizeof(Ctl) + sizeof(Desc) + 4096;
+  return b;
+}
+
+template <typename P>
+static int init_typed(r3d_ctx *c, const ShellTable &st) {
+  using R = typename P::R;
+  using T = typename P::T;
+  Problem &p = c->prob;
+  Desc &d = c->desc;
+  cudaStream_t s = c->stream;
+  const int n = d.n, nu = (int)p.q.size();
+  const long long N = d.N, Nh = d.Nh;
+  int rc;
+  // grids
+  if ((rc = dalloc(c, &c->u, n * N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->t, n * N * sizeof(T)))) return rc;
+  if ((rc = dalloc(c, &c->res, n * N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->lr, n * N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->w, n * Nh * 2 * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->fr, N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->fk, Nh * sizeof(double2)))) return rc;
+  if ((rc = dalloc(c, (void **)&c->kidx, Nh * 4))) return rc;
+  if ((rc = dalloc(c, &c->chi, (size_t)st.nshell * n * n * sizeof(R)))) return rc;
+  // AN2: hist_a = t slots (T), hist_b = residual slots (R);
+  // ANM: hist_a = residual ring (R), hist_b = z ring (T)
+  const size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
+  const size_t ha = c->mixer == MIX_AN2 ? sizeof(T) : sizeof(R);
+  const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
+  if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
+  if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
+  const int npart = std::max(c->ix_ctas, c->mix_ctas);
+  if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;
+  double *rmslog;
+  if ((rc = dalloc(c, (void **)&rmslog, (size_t)(p.maxstep + 1) * 8))) return rc;
+  if ((rc = dalloc(c, (void **)&c->ctl, sizeof(Ctl)))) return rc;
+  if ((rc = dalloc(c, (void **)&c->ddesc, sizeof(Desc)))) return rc;
+  if ((rc = dalloc(c, (void **)&c->dprefix, 16 * sizeof(int)))) return rc;
+  CK(cudaMemsetAsync(c->hist_a, 0, slots * n * N * ha, s));
+  CK(cudaMemsetAsync(c->hist_b, 0, slots * n * N * hb, s));
+  CK(cudaMemsetAsync(c->res, 0, n * N * sizeof(R), s));
+  CK(cudaMemsetAsync(c->fr, 0, N * sizeof(R), s));
+  CK(cudaMemsetAsync(c->fk, 0, Nh * sizeof(double2), s));
+  if (!c->fp64) {
+    if ((rc = dalloc(c, &c->cref, n * N * sizeof(R)))) return rc;
+    if ((rc = dalloc(c, &c->chi64, (size_t)st.nshell * n * n * 8))) return rc;
+    CK(cudaMemsetAsync(c->cref, 0, n * N * sizeof(R), s));
+  }
+  CK(cudaMemsetAsync(c->partials, 0, (size_t)npart * kPartials * 8, s));
+
+  d.clos = p.clos;
+  d.pse_n = p.pse_n;
+  d.mixer = c->mixer;
+  d.history = c->history;
+  d.beta = c->damping >= 0 ? c->damping : p.mix_m;
+  d.m = p.mix_m;
+  d.mp = p.mix_mp;
+  for (int v = 0; v < n; ++v) {
+    d.irho[v] = 1.0 / p.rhov[v];
+    d.qv[v] = p.qv[v];
+  }
+  d.u = c->u;
+  d.t = c->t;
+  d.fr = c->fr;
+  d.res = c->res;
+  d.w = c->w;
+  d.fk = nullptr;  // phi_L(k) enters through lr (see refresh)
+  d.chi = c->chi;
+  d.lr = c->lr;
+  d.cref = c->cref;
+  d.kidx = c->kidx;
+  d.hist_a = c->hist_a;
+  d.hist_b = c->hist_b;
+  d.partials = c->partials;
+  d.ctl = c->ctl;
+  d.partial_base = 0;
+  d.rmslog = rmslog;
+
+  // chi shell table, scaled by 2/N (the unnormalised transforms' factor)
+  std::vector<double> chi64(st.chi.size());
+  {
+    std::vector<R> chi(st.chi.size());
+    const double sc = 2.0 / (double)N;
+    for (size_t i = 0; i < chi.size(); ++i) {
+      chi64[i] = st.chi[i] * sc;
+      chi[i] = (R)chi64[i];
+    }
+    CK(cudaMemcpyAsync(c->chi, chi.data(), chi.size() * sizeof(R), cudaMemcpyHostToDevice, s));
+    if (c->fp64)
+      c->chi64 = c->chi;
+    else
+      CK(cudaMemcpyAsync(c->chi64, chi64.data(), chi64.size() * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  // shell index of every half-spectrum point
+  {
+    uint32_t *dtuple = nullptr;
+    if (!st.cubic) {
+      if ((rc = dalloc(c, (void **)&dtuple, st.tuple_idx.size() * 4))) return rc;
+      CK(cudaMemcpyAsync(dtuple, st.tuple_idx.data(), st.tuple_idx.size() * 4,
+                         cudaMemcpyHostToDevice, s));
+    }
+    launch_kidx(d, dtuple, st.cubic ? 1 : 0, s);
+    CK(cudaGetLastError());
+  }
+  // potentials: atom tables (cal_LJ.cu:33-40 mixing rules)
+  {
+    const double lambda1 = p.adswitch == 1 ? p.lambda : 1.0;
+    std::vector<double> ax(nu), ay(nu), az(nu), isig2((size_t)n * nu), eps4((size_t)n * nu);
+    for (int iu = 0; iu < nu; ++iu) {
+      ax[iu] = p.r[3 * iu];
+      ay[iu] = p.r[3 * iu + 1];
+      az[iu] = p.r[3 * iu + 2];
+    }
+    for (int v = 0; v < n; ++v)
+      for (int iu = 0; iu < nu; ++iu) {
+        double sg = (p.sig[iu] + p.sigv[v]) * 0.5 * lambda1;
+        isig2[(size_t)v * nu + iu] = 1.0 / (sg * sg);
+        eps4[(size_t)v * nu + iu] = std::sqrt(p.eps[iu] * p.epsv[v]) * 4.0;
+      }
+    double *dat;
+    const size_t natom = std::max(nu, 1);
+    if ((rc = dalloc(c, (void **)&dat, (4 + 2 * (size_t)n) * natom * 8))) return rc;
+    double *dx = dat, *dy = dat + natom, *dz = dat + 2 * natom, *dq = dat + 3 * natom;
+    double *dsig = dat + 4 * natom, *deps = dsig + (size_t)n * natom;
+    if (nu > 0) {
+      CK(cudaMemcpyAsync(dx, ax.data(), nu * 8, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(dy, ay.data(), nu * 8, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(dz, az.data(), nu * 8, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync(dq, p.q.data(), nu * 8, cudaMemcpyHostToDevice, s));
+      for (int v = 0; v < n; ++v) {
+        CK(cudaMemcpyAsync(dsig + (size_t)v * natom, isig2.data() + (size_t)v * nu, nu * 8,
+                           cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(deps + (size_t)v * natom, eps4.data() + (size_t)v * nu, nu * 8,
+                           cudaMemcpyHostToDevice, s));
+      }
+    }
+    AtomTab at{dx, dy, dz, dq, dsig, deps, nu};
+    // the kernel indexes isig2/eps4 as [v * nu + i]; pass nu as the stride
+    const double ikbt = 1.0 / (phys::avogadro * phys::boltzmann * p.temper);
+    const int coulomb = p.adswitch != 1;
+    const double lambda2 = p.adswitch == 2 ? p.lambda : 1.0;
+    const double ubeta = phys::hartree * phys::bohr / (phys::boltzmann * p.temper) * lambda2;
+    double dr[3] = {p.box[0] / d.nx, p.box[1] / d.ny, p.box[2] / d.nz};
+    // FP64 phase tables of the k-space Coulomb sum (setup scratch)
+    const size_t ntab = (size_t)std::max(nu, 1) * (d.hx + d.ny + d.nz);
+    double2 *tabs = nullptr;
+    cudaError_t e = cudaMalloc((void **)&tabs, ntab * sizeof(double2));
+    if (e != cudaSuccess) return fail(c, R3D_ENOMEM, "setup scratch");
+    double *fr64 = nullptr;
+    if (nu > 0) {
+      if (natom != (size_t)nu) return fail(c, R3D_EINVAL, "internal: atom stride");
+      launch_potential<P>(d, at, ikbt, ubeta, dr, coulomb, fr64, s);
+      CK(cudaGetLastError());
+    } else {
+      CK(cudaMemsetAsync(c->u, 0, n * N * sizeof(R), s));
+      CK(cudaMemsetAsync(c->t, 0, n * N * sizeof(T), s));
+    }
+    if (coulomb && nu > 0) {
+      double2 *ex = tabs, *ey = tabs + (size_t)nu * d.hx, *ez = ey + (size_t)nu * d.ny;
+      launch_phase_tables(ex, ey, ez, dx, dy, dz, nu, d.nx, d.ny, d.nz, p.box, s);
+      const double dv = p.box[0] * p.box[1] * p.box[2] / (double)N;
+      launch_fk(d, (double2 *)c->fk, ex, ey, ez, dq, nu, ubeta, p.box, dv, s);
+      CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(s));
+    cudaFree(tabs);
+    // long-range h term: lr = 1 - F^-1[chi q phi_L(k)]  (refresh, c_ref = 0)
+    if ((rc = refresh<P>(c, true))) return rc;
+  }
+  // control block and descriptor
+  {
+    Ctl h{};
+    h.status = RUNNING;
+    h.maxstep = p.maxstep;
+    h.tol = p.convergence;
+    h.count_left = p.count;
+    CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(c->ddesc, &d, sizeof(Desc), cudaMemcpyHostToDevice, s));
+    int pre[16] = {0, c->tiles_x, 0, c->tiles_y, 0, c->tiles_z, 0, c->ix_ctas,
+                   0, c->mix_ctas, c->ix_ctas, c->mix_ctas, 0, 0, 0, 0};
+    CK(cudaMemcpyAsync(c->dprefix, pre, sizeof(pre), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  // the attribute is a per-function limit shared by every context: always
+  // allow the largest tile any context may choose
+  kernels_set_smem(c->fp64, kSmemMax);
+  CK(cudaGetLastError());
+  return R3D_OK;
+}
+
+extern "C" int r3d_initialize(r3d_ctx *c) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (c->initialized) return fail(c, R3D_ESTATE, "already initialized");
+  if (!c->prob.has_solute) return fail(c, R3D_ESTATE, "no solute/control loaded");
+  if (!c->prob.has_solvent) return fail(c, R3D_ESTATE, "no solvent loaded");
+  if (c->prob.natv > kMaxSites) return fail(c, R3D_EINVAL, "too many solvent sites");
+  if (c->prob.maxstep < 1) return fail(c, R3D_EINVAL, "maxstep must be >= 1");
+  if (c->opts.device < 0) return fail(c, R3D_ESTATE, "host-only context (device < 0)");
+  CK(cudaSetDevice(c->opts.device));
+  Desc d{};
+  int rc = plan_geometry(c, d);
+  if (rc) return rc;
+  ShellTable st;
+  std::string m = build_shells(c->prob, st);
+  if (!m.empty()) return fail(c, R3D_EINVAL, m);
+  c->nshell = st.nshell;
+  size_t need = plan_bytes(c, d, st.nshell);
+  if (c->opts.hbm_budget && need > c->opts.hbm_budget)
+    return fail(c, R3D_EBUDGET, "problem needs " + std::to_string(need) +
+                                    " device bytes, budget " +
+                                    std::to_string(c->opts.hbm_budget));
+  size_t fre = 0, tot = 0;
+  CK(cudaMemGetInfo(&fre, &tot));
+  if (need > fre) return fail(c, R3D_ENOMEM, "problem needs " + std::to_string(need) +
+                                                 " device bytes, " + std::to_string(fre) + " free");
+  c->desc = d;
+  rc = c->fp64 ? init_typed<P64>(c, st) : init_typed<PMix>(c, st);
+  if (rc) {
+    free_all(c);
+    return rc;
+  }
+  c->initialized = true;
+  return R3D_OK;
+}
+
+// --------------------------------------------------------------- iterate
+// stage: 0 = full iteration (evaluate, decide, mix), 1 = evaluate only
+// (calculate), 2 = mix only (anderson)
+template <typename P>
+static void enqueue(r3d_ctx *c, int stage) {
+  cudaStream_t s = c->stream;
+  const int *pf = c->dprefix;
+  Batch bx{c->ddesc, pf + 0, 1}, by{c->ddesc, pf + 2, 1}, bz{c->ddesc, pf + 4, 1},
+      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1};
+  int k = 0;
+  if (stage != 2) {
+    launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 1, nullptr);
+    launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 1);
+    launch_zoz<P>(bz, c->tiles_z, c->smz, s, 2, 1);
+    launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 1);
+    launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 1, nullptr, c->ix_per);
+    k += 5;
+    if (c->mixer == MIX_ANM) {
+      launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 0);
+      ++k;
+    }
+    launch_reduce(c->ddesc, pf + 10, 1, stage == 0 ? 0 : 2, s);
+    ++k;
+  } else {
+    launch_reduce(c->ddesc, pf + 10, 1, 1, s);
+    ++k;
+  }
+  if (stage != 1) {
+    if (c->mixer == MIX_AN2) {
+      launch_mix_an2<P>(bmx, c->mix_ctas, s);
+      ++k;
+    } else {
+      launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 1);
+      launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 2);
+      k += 2;
+    }
+  }
+  if (stage == 0) c->kernels_per_iter = k;
+}
+
+static int read_ctl(r3d_ctx *c, Ctl &h) {
+  CK(cudaMemcpyAsync(&h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return R3D_OK;
+}
+static int set_running(r3d_ctx *c) {
+  int st = RUNNING;
+  CK(cudaMemcpyAsync(&c->ctl->status, &st, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  return R3D_OK;
+}
+
+extern "C" int r3d_calculate(r3d_ctx *c, double *rms) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "calculate before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  int rc = set_running(c);
+  if (rc) return rc;
+  if (c->fp64)
+    enqueue<P64>(c, 1);
+  else
+    enqueue<PMix>(c, 1);
+  CK(cudaGetLastError());
+  Ctl h;
+  if ((rc = read_ctl(c, h))) return rc;
+  if (rms) *rms = h.rms;
+  return R3D_OK;
+}
+
+extern "C" int r3d_anderson(r3d_ctx *c) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "anderson before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  int rc = set_running(c);
+  if (rc) return rc;
+  if (c->fp64)
+    enqueue<P64>(c, 2);
+  else
+    enqueue<PMix>(c, 2);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return R3D_OK;
+}
+
+extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "iterate before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  cudaStream_t s = c->stream;
+  // AN2::initialize inside iterate (iterate.cu:39): fresh mixer state
+  {
+    Ctl h{};
+    h.status = RUNNING;
+    h.maxstep = c->prob.maxstep;
+    h.tol = c->prob.convergence;
+    h.count_left = c->prob.count;
+    CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+  }
+  if (!c->gexec) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    if (c->fp64)
+      enqueue<P64>(c, 0);
+    else
+      enqueue<PMix>(c, 0);
+    CK(cudaStreamEndCapture(s, &g));
+    cudaError_t e = cudaGraphInstantiate(&c->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+      return fail(c, R3D_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  if (c->opts.verbose) std::printf("relaxing 3D UV RISM:\n");
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s));
+  Ctl h{};
+  int printed = 0;
+  const int chunk = 8;
+  std::vector<double> log;
+  c->next_refresh = 1e-3;
+  for (;;) {
+    for (int i = 0; i < chunk; ++i) CK(cudaGraphLaunch(c->gexec, s));
+    int rc = read_ctl(c, h);
+    if (rc) return rc;
+    if (!c->fp64 && h.status == RUNNING && h.rms < c->next_refresh) {
+      // mixed path: move the converged part of c into the FP64 reference
+      if ((rc = refresh<PMix>(c, false))) return rc;
+      c->next_refresh *= 1e-2;
+    }
+    if (c->opts.verbose && h.step > printed) {
+      log.resize(h.step);
+      CK(cudaMemcpy(log.data(), c->desc.rmslog, sizeof(double) * h.step, cudaMemcpyDeviceToHost));
+      for (int i = printed; i < h.step; ++i)
+        std::printf(" Step = %d Reside = %g\n", i + 1, log[i]);
+      printed = h.step;
+    }
+    if (h.status != RUNNING) break;
+  }
+  CK(cudaEventRecord(e1, s));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->ms_per_iter = h.step > 0 ? ms / h.step : 0;
+  int st = h.status == CONVERGED ? R3D_CONVERGED
+                                 : (h.status == DIVERGED ? R3D_DIVERGED : R3D_MAXSTEP);
+  if (c->opts.verbose) {
+    if (st == R3D_DIVERGED)
+      std::printf("Calculation diverged.\n");
+    else if (st == R3D_MAXSTEP)
+      std::printf("3D UV RISM: reached limit # of relaxation steps: %d\n", c->prob.maxstep);
+  }
+  if (steps) *steps = h.step;
+  if (rms) *rms = h.rms;
+  if (status) *status = st;
+  return R3D_OK;
+}
+
+// ------------------------------------------------------------ read-back
+// Grid of t that produced the last residual: t itself, unless the last step
+// also mixed (maxstep reached), in which case AN2 left the old t in its
+// history slot (anderson_cuda.cu:11-22).
+static const void *t_of_residual(r3d_ctx *c, const Ctl &h) {
+  if (h.status == MAXSTEP && h.mix_flag && c->mixer == MIX_AN2) {
+    size_t off = (size_t)h.coef[3] * c->desc.n * c->desc.N * sizeof(double);
+    return (const char *)c->hist_a + off;
+  }
+  return c->t;
+}
+
+static int ensure_scratch(r3d_ctx *c, size_t bytes) {
+  if (c->scratch_bytes >= bytes) return R3D_OK;
+  if (c->scratch) {
+    cudaFree(c->scratch);
+    c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), (void *)c->scratch));
+    c->bytes -= c->scratch_bytes;
+  }
+  c->scratch = nullptr;
+  c->scratch_bytes = 0;
+  int rc = dalloc(c, (void **)&c->scratch, bytes);
+  if (rc) return rc;
+  c->scratch_bytes = bytes;
+  return R3D_OK;
+}
+
+extern "C" int r3d_thermo(r3d_ctx *c, double *xmu, double *xmu2, double *pmv,
+                          double *pressure) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "thermo before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  const Desc &d = c->desc;
+  const int ctas = 2 * kNumSM;
+  int rc = ensure_scratch(c, (size_t)ctas * d.n * 4 * 8);
+  if (rc) return rc;
+  Ctl h;
+  if ((rc = read_ctl(c, h))) return rc;
+  const void *tg = t_of_residual(c, h);
+  if (c->fp64)
+    launch_thermo<P64>(d, tg, c->scratch, ctas, c->stream);
+  else
+    launch_thermo<PMix>(d, tg, c->scratch, ctas, c->stream);
+  CK(cudaGetLastError());
+  std::vector<double> part((size_t)ctas * d.n * 4);
+  CK(cudaMemcpyAsync(part.data(), c->scratch, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const Problem &p = c->prob;
+  const double dv = p.box[0] * p.box[1] * p.box[2] / (double)d.N;
+  double cuv = 0;
+  for (int v = 0; v < d.n; ++v) {
+    double s[4] = {0, 0, 0, 0};
+    for (int k = 0; k < ctas; ++k)
+      for (int j = 0; j < 4; ++j) s[j] += part[((size_t)k * d.n + v) * 4 + j];
+    if (xmu) {
+      xmu[v] = s[0] * p.rhov[v] * dv;
+      xmu[d.n + v] = s[2] * p.rhov[v] * dv;
+    }
+    if (xmu2) xmu2[v] = s[1] * p.rhov[v] * dv;
+    cuv += s[3] * p.rhov[v];
+  }
+  cuv *= dv;
+  const double ibeta = phys::avogadro * phys::boltzmann * p.temper;
+  if (pmv) *pmv = p.xt * (1.0 - cuv) * ibeta;  // cal_pmv.cu:19-23
+  double pr = 0;
+  for (int v = 0; v < d.n; ++v) pr += p.rhov[v];  // cal_pressure.cu:8-19
+  pr *= 1.0e30 / phys::avogadro;
+  if (pressure) *pressure = 0.5 * (pr + 1.0 / (p.xt * ibeta));
+  return R3D_OK;
+}
+
+extern "C" int r3d_write_xmu(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  const int n = c->prob.natv;
+  std::vector<double> xmu(2 * n), xmu2(n);
+  double pmv, pr;
+  int rc = r3d_thermo(c, xmu.data(), xmu2.data(), &pmv, &pr);
+  if (rc) return rc;
+  std::string out = path ? path : c->prob.fname + (c->prob.zero ? ".xmu0" : ".xmu");
+  std::string m = write_xmu(c->prob, xmu.data(), xmu2.data(), pmv, pr, out);
+  if (!m.empty()) return fail(c, R3D_EIO, m);
+  return R3D_OK;
+}
+
+extern "C" int r3d_get_grid(r3d_ctx *c, int which, double *host) {
+  if (!c || !host) return fail(c, R3D_EINVAL, "ctx or host is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "get_grid before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  const Desc &d = c->desc;
+  const long long niv = (long long)d.n * d.N;
+  cudaStream_t s = c->stream;
+  long long count = 0;
+  int rc;
+  Ctl h;
+  if ((rc = read_ctl(c, h))) return rc;
+  switch (which) {
+    case R3D_GRID_U: case R3D_GRID_T: {  // short-range part + q_v phi_L(r)
+      const void *src = which == R3D_GRID_U ? c->u : c->t;
+      count = niv;
+      if ((rc = ensure_scratch(c, count * 8))) return rc;
+      const int x = which == R3D_GRID_T ? 1 : 0;
+      if (c->fp64)
+        launch_shift_qfr<P64>(d, src, c->scratch, 1.0, x, s);
+      else
+        launch_shift_qfr<PMix>(d, src, c->scratch, 1.0, x, s);
+      break;
+    }
+    case R3D_GRID_R: case R3D_GRID_FR: {
+      const void *src = which == R3D_GRID_R ? c->res : c->fr;
+      count = which == R3D_GRID_FR ? d.N : niv;
+      if ((rc = ensure_scratch(c, count * 8))) return rc;
+      if (c->fp64)
+        launch_to_double<P64>(src, c->scratch, count, 0, s);
+      else
+        launch_to_double<PMix>(src, c->scratch, count, 0, s);
+      break;
+    }
+    case R3D_GRID_G: case R3D_GRID_H: {
+      count = niv;
+      if ((rc = ensure_scratch(c, count * 8))) return rc;
+      const void *tg = t_of_residual(c, h);
+      double *g = which == R3D_GRID_G ? c->scratch : nullptr;
+      double *hh = which == R3D_GRID_H ? c->scratch : nullptr;
+      if (c->fp64)
+        launch_gh<P64>(d, tg, g, hh, s);
+      else
+        launch_gh<PMix>(d, tg, g, hh, s);
+      break;
+    }
+    case R3D_GRID_FK: {
+      count = 2 * d.Nh;
+      if ((rc = ensure_scratch(c, count * 8))) return rc;
+      launch_to_double<P64>(c->fk, c->scratch, count, 0, s);  // FP64 always
+      break;
+    }
+    default:
+      return fail(c, R3D_EINVAL, "unknown grid");
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, c->scratch, count * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (which == R3D_GRID_FK) {  // transform units -> physical beta phi_L(k)
+    const Problem &p = c->prob;
+    const double dv = p.box[0] * p.box[1] * p.box[2] / (double)d.N;
+    const int par0 = ((d.nx + d.ny + d.nz) / 2) & 1;
+    for (long long i = 0; i < d.Nh; ++i) {
+      int pp = (int)(i % d.hx), y = (int)((i / d.hx) % d.ny), z = (int)(i / ((long long)d.hx * d.ny));
+      double sg = ((2 * pp + y + z + par0) & 1) ? -1.0 : 1.0;
+      double a = host[2 * i], b = host[2 * i + 1];
+      // F = dv * C * raw, C = -i sigma:  (a + ib)(-i) = b - i a
+      host[2 * i] = dv * sg * b;
+      host[2 * i + 1] = -dv * sg * a;
+    }
+  }
+  return R3D_OK;
+}
+
+extern "C" int r3d_set_t(r3d_ctx *c, const double *host) {
+  if (!c || !host) return fail(c, R3D_EINVAL, "ctx or host is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "set_t before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  const long long niv = (long long)c->desc.n * c->desc.N;
+  int rc = ensure_scratch(c, niv * 8);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(c->scratch, host, niv * 8, cudaMemcpyHostToDevice, c->stream));
+  if (c->fp64)
+    launch_set_short<P64>(c->desc, c->scratch, c->t, c->stream);
+  else
+    launch_set_short<PMix>(c->desc, c->scratch, c->t, c->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return R3D_OK;
+}
+
+extern "C" int r3d_info(const r3d_ctx *c, int *grid3, int *natv, long long *ngrid, int *nu) {
+  if (!c) return R3D_EINVAL;
+  if (grid3)
+    for (int d = 0; d < 3; ++d) grid3[d] = c->prob.grid[d];
+  if (natv) *natv = c->prob.natv;
+  if (ngrid) *ngrid = (long long)c->prob.grid[0] * c->prob.grid[1] * c->prob.grid[2];
+  if (nu) *nu = (int)c->prob.q.size();
+  return R3D_OK;
+}
+
+extern "C" int r3d_device_bytes(const r3d_ctx *c, unsigned long long *bytes) {
+  if (!c || !bytes) return R3D_EINVAL;
+  if (c->initialized) {
+    *bytes = c->bytes;
+    return R3D_OK;
+  }
+  r3d_ctx tmp = *c;
+  tmp.allocs.clear();
+  Desc d{};
+  if (plan_geometry(&tmp, d)) return R3D_EINVAL;
+  long long smax = 3LL * (d.nx - 1) * (d.nx - 1);
+  int nshell = (int)std::min<long long>((smax - 3) / 8 + 1, d.Nh);
+  *bytes = plan_bytes(&tmp, d, nshell);
+  return R3D_OK;
+}
+
+extern "C" int r3d_iter_timing(const r3d_ctx *c, double *ms, int *kernels) {
+  if (!c) return R3D_EINVAL;
+  if (ms) *ms = c->ms_per_iter;
+  if (kernels) *kernels = c->kernels_per_iter;
+  return R3D_OK;
+}
+
+// ---------------------------------------------------------- fft3d seam
+template <typename P>
+static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int dir,
+                     const double *in, double *out) {
+  using R = typename P::R;
+  Desc &d = c->desc;
+  cudaStream_t s = c->stream;
+  const long long N = d.N, Nh = d.Nh;
+  int rc;
+  void *src, *w, *ctl, *ddesc, *pre, *hbuf;
+  if ((rc = dalloc(c, &src, N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &w, Nh * 2 * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &ctl, sizeof(Ctl)))) return rc;
+  if ((rc = dalloc(c, &ddesc, sizeof(Desc)))) return rc;
+  if ((rc = dalloc(c, &pre, 16 * sizeof(int)))) return rc;
+  if ((rc = dalloc(c, &hbuf, std::max(N, 2 * Nh) * 8))) return rc;
+  CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
+  d.w = w;
+  d.ctl = (Ctl *)ctl;
+  CK(cudaMemcpyAsync(ddesc, &d, sizeof(Desc), cudaMemcpyHostToDevice, s));
+  int pf[16] = {0, c->tiles_x, 0, c->tiles_y, 0, c->tiles_z, 0, c->ix_ctas};
+  CK(cudaMemcpyAsync(pre, pf, sizeof(pf), cudaMemcpyHostToDevice, s));
+  const int *dp = (const int *)pre;
+  Batch bx{(Desc *)ddesc, dp, 1}, by{(Desc *)ddesc, dp + 2, 1}, bz{(Desc *)ddesc, dp + 4, 1},
+      bix{(Desc *)ddesc, dp + 6, 1};
+  kernels_set_smem(c->fp64, kSmemMax);
+  const double dv = box[0] * box[1] * box[2] / (double)N;
+  const int par0 = ((nx + ny + nz) / 2) & 1;
+  std::vector<double> tmp(std::max(N, 2 * Nh));
+  if (dir < 0) {
+    CK(cudaMemcpyAsync(hbuf, in, N * 8, cudaMemcpyHostToDevice, s));
+    launch_from_double<P>((const double *)hbuf, src, N, 0, s);
+    launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 0, src);
+    launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 0);
+    launch_zoz<P>(bz, c->tiles_z, c->smz, s, 0, 0);
+    launch_to_double<P>(w, (double *)hbuf, 2 * Nh, 0, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, hbuf, 2 * Nh * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (long long i = 0; i < Nh; ++i) {
+      int pp = (int)(i % d.hx), y = (int)((i / d.hx) % ny), z = (int)(i / ((long long)d.hx * ny));
+      double sg = ((2 * pp + y + z + par0) & 1) ? -1.0 : 1.0;
+      double a = out[2 * i], b = out[2 * i + 1];
+      out[2 * i] = dv * sg * b;  // dv * (-i sigma) * (a + i b)
+      out[2 * i + 1] = -dv * sg * a;
+    }
+  } else {
+    for (long long i = 0; i < Nh; ++i) {
+      int pp = (int)(i % d.hx), y = (int)((i / d.hx) % ny), z = (int)(i / ((long long)d.hx * ny));
+      double sg = ((2 * pp + y + z + par0) & 1) ? -1.0 : 1.0;
+      double a = in[2 * i], b = in[2 * i + 1];
+      // raw = F conj(C) / dv = F (i sigma) / dv
+      tmp[2 * i] = -b * sg / dv;
+      tmp[2 * i + 1] = a * sg / dv;
+    }
+    CK(cudaMemcpyAsync(hbuf, tmp.data(), 2 * Nh * 8, cudaMemcpyHostToDevice, s));
+    launch_from_double<P>((const double *)hbuf, w, 2 * Nh, 0, s);
+    launch_zoz<P>(bz, c->tiles_z, c->smz, s, 1, 0);
+    launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 0);
+    launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 0, src, c->ix_per);
+    launch_to_double<P>(src, (double *)hbuf, N, 0, s);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, hbuf, N * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double sc = 2.0 / (double)N;
+    for (long long i = 0; i < N; ++i) out[i] *= sc;
+  }
+  return R3D_OK;
+}
+
+extern "C" int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
+                         const double *box, int dir, const double *in, double *out) {
+  if (!box || !in || !out || (dir != -1 && dir != 1))
+    return fail(nullptr, R3D_EINVAL, "bad fft3d arguments");
+  r3d_opts o{};
+  o.device = device;
+  o.precision = precision;
+  r3d_ctx *c = nullptr;
+  int rc = r3d_create(&o, &c);
+  if (rc) return rc;
+  c->prob.grid[0] = nx;
+  c->prob.grid[1] = ny;
+  c->prob.grid[2] = nz;
+  c->prob.natv = 1;
+  if (nx < 4 || ny < 2 || nz < 2 || (nx & 1)) {
+    r3d_destroy(c);
+    return fail(nullptr, R3D_EINVAL, "fft3d: nx must be even >= 4");
+  }
+  Desc d{};
+  rc = plan_geometry(c, d);
+  if (!rc) {
+    c->desc = d;
+    rc = c->fp64 ? fft_typed<P64>(c, nx, ny, nz, box, dir, in, out)
+                 : fft_typed<PMix>(c, nx, ny, nz, box, dir, in, out);
+  }
+  if (rc) g_last_error = c->err;
+  r3d_destroy(c);
+  return rc;
+}

@@ -1,0 +1,1319 @@
+// r3d_kernels.cu -- sm_100a kernels of the 3D-RISM solve.
+//
+// One iteration (the reference's RISM3D::calculate + cal_rms + AN2::calculate,
+// calculate.cu:4-65, cal_rms.cu:14-26, anderson.cu:43-130) is five grid passes
+// plus two tiny control kernels:
+//
+//   FX   closure + c_s + checkerboard + packed real->complex x transform
+//   FY   y transform of the half spectrum                     (in place)
+//   ZOZ  z transform, Ornstein-Zernike h_a(k) = sum_b chi_ab(|k|) c_b(k),
+//        inverse z transform                                  (in place)
+//   IY   inverse y transform                                  (in place)
+//   IX   inverse packed x transform + g, residual R = h + 1 - g,
+//        sum R^2 and the AN2 Gram dots (per-CTA partials)
+//
+// Long-range electrostatics and refinement.  The reference adds
+// q_v beta phi_L(r) to c in r space (trm1mt) and subtracts q_v beta phi_L(k) in
+// k space (mqvfk).  Here the solve runs on the short-range parts
+// t_s = t - q_v beta phi_L(r) and u_s = beta u - q_v beta phi_L(r), so that
+// c_s = g - 1 - t_s, and h is split around a frozen c_ref:
+//   h_a = F^-1[ sum_b chi_ab F(c_s,b - c_ref,b) ] + h_ref,a
+//   h_ref,a = F^-1[ sum_b chi_ab (F(c_ref,b) - q_b beta phi_L(k)) ]
+// with h_ref computed in FP64 (the "refresh", which with c_ref = 0 is the
+// setup's long-range term).  This is the reference's iteration exactly; in the
+// mixed path the FP32 transforms only ever see the small correction
+// c_s - c_ref, so their rounding noise shrinks as the solve converges instead
+// of flooring the residual at ~1e-6.
+//   reduce/coef (1 CTA)  RMS, convergence, mixing coefficients on the device
+//   mix   AN2 or history-M Anderson update of t
+//
+// The transform is the reference's half-shifted one (fft3d.cu):
+//   F(k) = dv sum_r f(r) e^{-i k.r},  r = (i - n/2) dr,  k = 2 pi (j - n/2 + 1/2)/L
+// computed as: checkerboard (-1)^{x+y+z} on r, odd-frequency DFT per axis
+// (x via a half-length packed complex FFT, y/z via a half-sample twiddle), and
+// the constant per-point phase dv*C(k) is folded into phi_L(k) and chi, so the
+// iteration never applies it.  All passes take a descriptor table so that one
+// launch can serve many solves of different grids (batching).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "r3d_fft.cuh"
+#include "r3d_internal.h"
+
+namespace r3d {
+
+// ------------------------------------------------------------------ helpers
+struct Batch {
+  const Desc *d;       // [ns]
+  const int *prefix;   // [ns + 1] CTA prefix of this pass
+  int ns;
+};
+
+__device__ __forceinline__ int find_solve(const Batch &b, int cta) {
+  int lo = 0, hi = b.ns - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (b.prefix[mid] <= cta)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename R>
+__device__ __forceinline__ R closure_g(int clos, int pse_n, R earg) {
+  // calculate_cuda.cu:1-16 (KH, HNC); PSE-n: sum_{i<=n} t*^i / i! for t* > 0.
+  if (clos == HNC) return exp(earg);
+  if (earg >= (R)0) {
+    if (clos == KH || pse_n == 1) return (R)1 + earg;
+    R term = (R)1, sum = (R)1;
+    for (int i = 1; i <= pse_n; ++i) {
+      term *= earg / (R)i;
+      sum += term;
+    }
+    return sum;
+  }
+  return exp(earg);
+}
+
+template <typename R>
+__device__ __forceinline__ bool solve_running(const Desc &d) {
+  return d.ctl->status == RUNNING;
+}
+
+// Shared-memory carve-up: twiddles, digit-reversal table, pack twiddles, data.
+template <typename C>
+struct Smem {
+  C *tw;
+  int16_t *perm;
+  C *ptw;  // half-sample twiddles e^{-i pi a / n}
+  C *buf;
+};
+template <typename C>
+__device__ __forceinline__ Smem<C> carve(char *sm, int L, int Lp) {
+  Smem<C> s;
+  s.tw = (C *)sm;
+  size_t off = sizeof(C) * L;
+  s.ptw = (C *)(sm + off);
+  off += sizeof(C) * Lp;
+  s.perm = (int16_t *)(sm + off);
+  off += ((sizeof(int16_t) * L + 15) / 16) * 16;
+  s.buf = (C *)(sm + off);
+  return s;
+}
+// e^{-i pi a / n} for a in [0, L)
+template <typename C>
+__device__ void half_twiddles(C *ptw, int L, int n) {
+  for (int a = threadIdx.x; a < L; a += blockDim.x) {
+    double s, c;
+    sincospi(-(double)a / (double)n, &s, &c);
+    ptw[a].x = c;
+    ptw[a].y = s;
+  }
+}
+
+// ======================================================================
+// FX: forward x pass.  MODE 0: plain real input `src` ([n][N]);
+// MODE 1: closure fused (reads t, u, fr).
+// ======================================================================
+template <typename P, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_fwd_x(Batch b, const typename P::R *src) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) char smem[];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (MODE == 1 && !solve_running<R>(d)) return;
+  const int tile = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, nx = d.nx, ny = d.ny, n = d.n, S = d.rows;
+  Smem<C> sm = carve<C>(smem, hx, hx);
+  splan_init(sm.tw, sm.perm, hx, d.rad_x, d.nrad_x);
+  half_twiddles(sm.ptw, hx, nx);
+  __syncthreads();
+  SPlan<C> pl{hx, d.nrad_x, {}, sm.tw, sm.perm};
+  for (int k = 0; k < d.nrad_x; ++k) pl.rad[k] = d.rad_x[k];
+
+  const long long row0 = (long long)tile * S;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *cref = (const R *)d.cref;
+  const int total = n * S * hx;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    int m = e % hx, sr = e / hx, r = sr % S, v = sr / S;
+    long long row = row0 + r;
+    int y = (int)(row % ny), z = (int)(row / ny);
+    long long base = (long long)v * d.N + row * nx;
+    R f0, f1;
+    if (MODE == 0) {
+      f0 = src[base + m];
+      f1 = src[base + m + hx];
+    } else {
+      // trm1mt on the short-range parts: c_s = g - 1 - t_s (closure in the
+      // state precision, rounded once to the grid type)
+      double t0 = t[base + m], t1 = t[base + m + hx];
+      double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
+      double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + hx] + t1);
+      double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
+      if (cref) {
+        c0 -= (double)cref[base + m];
+        c1 -= (double)cref[base + m + hx];
+      }
+      f0 = (R)c0;
+      f1 = (R)c1;
+    }
+    if ((m + y + z) & 1) f0 = -f0;
+    if ((m + hx + y + z) & 1) f1 = -f1;
+    C zc = cmul(C{f0, -f1}, sm.ptw[m]);
+    sm.buf[sr * hx + sm.perm[m]] = zc;
+  }
+  __syncthreads();
+  fft_dit<-1>(sm.buf, n * S, 1 << 30, 0, hx, 1, pl);
+  C *w = (C *)d.w;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    int p = e % hx, sr = e / hx, r = sr % S, v = sr / S;
+    w[(long long)v * d.Nh + (row0 + r) * hx + p] = sm.buf[sr * hx + p];
+  }
+}
+
+// ======================================================================
+// FY / IY: y transform of the half spectrum, tile = (site, z, x-columns).
+// ======================================================================
+template <typename P, int DIR>
+__global__ void __launch_bounds__(kThreads)
+    k_fft_y(Batch b, int check_status) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) char smem[];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (check_status && !solve_running<R>(d)) return;
+  int tile = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, ny = d.ny, nz = d.nz, PC = d.ycols;
+  const int ptiles = hx / PC;
+  const int pt = tile % ptiles;
+  tile /= ptiles;
+  const int z = tile % nz, v = tile / nz;
+  Smem<C> sm = carve<C>(smem, ny, ny);
+  splan_init(sm.tw, sm.perm, ny, d.rad_y, d.nrad_y);
+  half_twiddles(sm.ptw, ny, ny);
+  __syncthreads();
+  SPlan<C> pl{ny, d.nrad_y, {}, sm.tw, sm.perm};
+  for (int k = 0; k < d.nrad_y; ++k) pl.rad[k] = d.rad_y[k];
+  C *w = (C *)d.w + (long long)v * d.Nh + (long long)z * ny * hx + pt * PC;
+  const int total = ny * PC;
+  if (DIR < 0) {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, y = e / PC;
+      sm.buf[sm.perm[y] * PC + p] = cmul(w[(long long)y * hx + p], sm.ptw[y]);
+    }
+    __syncthreads();
+    fft_dit<-1>(sm.buf, PC, 1 << 30, 0, 1, PC, pl);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, y = e / PC;
+      w[(long long)y * hx + p] = sm.buf[y * PC + p];
+    }
+  } else {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, y = e / PC;
+      sm.buf[y * PC + p] = w[(long long)y * hx + p];
+    }
+    __syncthreads();
+    fft_dif<1>(sm.buf, PC, 1 << 30, 0, 1, PC, pl);
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, y = e / PC;
+      w[(long long)y * hx + p] = cmul(sm.buf[sm.perm[y] * PC + p], cconj(sm.ptw[y]));
+    }
+  }
+}
+
+// ======================================================================
+// ZOZ: tile = (y, x-columns), all sites.  MODE 0: forward z only;
+// MODE 1: inverse z only; MODE 2: forward z + mqvfk + OZ + inverse z.
+// ======================================================================
+template <typename R, int NS>
+__device__ __forceinline__ void oz_point(typename Cx<R>::T *buf, int n, int stride,
+                                         const R *chi, const double2 *fk,
+                                         const double *qv) {
+  using C = typename Cx<R>::T;
+  constexpr int M = NS > 0 ? NS : kMaxSites;
+  const int nn = NS > 0 ? NS : n;
+  C c[M];
+#pragma unroll
+  for (int bb = 0; bb < M; ++bb)
+    if (bb < nn) c[bb] = buf[bb * stride];
+  if (fk) {  // mqvfk (refresh pipeline only)
+    const double2 f = *fk;
+#pragma unroll
+    for (int bb = 0; bb < M; ++bb)
+      if (bb < nn) {
+        c[bb].x -= (R)(qv[bb] * f.x);
+        c[bb].y -= (R)(qv[bb] * f.y);
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < M; ++a) {
+    if (a < nn) {
+      R hr = 0, hi = 0;  // oz: h_a = sum_b chi[a][b] c_b
+#pragma unroll
+      for (int bb = 0; bb < M; ++bb) {
+        if (bb < nn) {
+          R x = chi[a * nn + bb];
+          hr += c[bb].x * x;
+          hi += c[bb].y * x;
+        }
+      }
+      buf[a * stride] = C{hr, hi};
+    }
+  }
+}
+
+template <typename P, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_zoz(Batch b, int check_status) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) char smem[];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (check_status && !solve_running<R>(d)) return;
+  int tile = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, ny = d.ny, nz = d.nz, n = d.n, PC = d.zcols;
+  const int ptiles = hx / PC;
+  const int pt = tile % ptiles, y = tile / ptiles;
+  Smem<C> sm = carve<C>(smem, nz, nz);
+  splan_init(sm.tw, sm.perm, nz, d.rad_z, d.nrad_z);
+  half_twiddles(sm.ptw, nz, nz);
+  __syncthreads();
+  SPlan<C> pl{nz, d.nrad_z, {}, sm.tw, sm.perm};
+  for (int k = 0; k < d.nrad_z; ++k) pl.rad[k] = d.rad_z[k];
+  const long long zs = (long long)ny * hx;  // z stride in the half spectrum
+  C *w = (C *)d.w + (long long)y * hx + pt * PC;
+  const int total = n * nz * PC;
+  const int sA = nz * PC;
+  if (MODE != 1) {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
+      sm.buf[(v * nz + sm.perm[z]) * PC + p] =
+          cmul(w[(long long)v * d.Nh + z * zs + p], sm.ptw[z]);
+    }
+    __syncthreads();
+    fft_dit<-1>(sm.buf, n * PC, PC, sA, 1, PC, pl);
+  } else {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
+      sm.buf[(v * nz + z) * PC + p] = w[(long long)v * d.Nh + z * zs + p];
+    }
+    __syncthreads();
+  }
+  if (MODE == 0) {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
+      w[(long long)v * d.Nh + z * zs + p] = sm.buf[(v * nz + z) * PC + p];
+    }
+    return;
+  }
+  if (MODE == 2) {
+    const uint32_t *kidx = d.kidx + (long long)y * hx + pt * PC;
+    const double2 *fk = d.fk ? (const double2 *)d.fk + (long long)y * hx + pt * PC : nullptr;
+    const R *chi = (const R *)d.chi;
+    const int nn = n * n;
+    for (int e = threadIdx.x; e < nz * PC; e += blockDim.x) {
+      int p = e % PC, z = e / PC;
+      const R *ch = chi + (size_t)kidx[z * zs + p] * nn;
+      const double2 *f = fk ? fk + z * zs + p : nullptr;
+      C *bp = sm.buf + z * PC + p;
+      switch (n) {
+        case 1: oz_point<R, 1>(bp, n, sA, ch, f, d.qv); break;
+        case 2: oz_point<R, 2>(bp, n, sA, ch, f, d.qv); break;
+        case 3: oz_point<R, 3>(bp, n, sA, ch, f, d.qv); break;
+        case 4: oz_point<R, 4>(bp, n, sA, ch, f, d.qv); break;
+        default: oz_point<R, 0>(bp, n, sA, ch, f, d.qv); break;
+      }
+    }
+    __syncthreads();
+  }
+  fft_dif<1>(sm.buf, n * PC, PC, sA, 1, PC, pl);
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
+    w[(long long)v * d.Nh + z * zs + p] =
+        cmul(sm.buf[(v * nz + sm.perm[z]) * PC + p], cconj(sm.ptw[z]));
+  }
+}
+
+// ======================================================================
+// IX: inverse x pass.  MODE 0: plain real output `dst` ([n][N]);
+// MODE 1: g, residual R = h + 1 - g (calculate_cuda.cu:54-60), partial sums
+// of R^2 (cal_rms.cu) and, when AN2 is past its Picard warm-up, the five
+// theta dots per site (anderson_cuda.cu:25-67).  A CTA handles `per` tiles.
+// ======================================================================
+template <typename R>
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+  return s;  // valid in thread 0
+}
+
+template <typename P, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_inv_x(Batch b, typename P::R *dst, int per) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) char smem[];
+  __shared__ double red[kThreads / 32];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (MODE == 1 && !solve_running<R>(d)) return;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, nx = d.nx, ny = d.ny, n = d.n, S = d.rows;
+  Smem<C> sm = carve<C>(smem, hx, hx);
+  splan_init(sm.tw, sm.perm, hx, d.rad_x, d.nrad_x);
+  half_twiddles(sm.ptw, hx, nx);
+  __syncthreads();
+  SPlan<C> pl{hx, d.nrad_x, {}, sm.tw, sm.perm};
+  for (int k = 0; k < d.nrad_x; ++k) pl.rad[k] = d.rad_x[k];
+
+  const bool dots = MODE == 1 && d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *lr = (const R *)d.lr;
+  R *res = (R *)d.res;
+  const R *rp = (const R *)d.hist_b;
+  const long long niv = (long long)n * d.N;
+  double acc_ss = 0;
+  double acc[kMaxSites][5];
+  for (int v = 0; v < kMaxSites; ++v)
+    for (int k = 0; k < 5; ++k) acc[v][k] = 0;
+
+  const C *w = (const C *)d.w;
+  const int ntile = d.tiles_x;
+  for (int it = 0; it < per; ++it) {
+    const int tile = cta * per + it;
+    if (tile >= ntile) break;
+    const long long row0 = (long long)tile * S;
+    const int total = n * S * hx;
+    __syncthreads();
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      int p = e % hx, sr = e / hx, r = sr % S, v = sr / S;
+      sm.buf[sr * hx + p] = w[(long long)v * d.Nh + (row0 + r) * hx + p];
+    }
+    __syncthreads();
+    fft_dif<1>(sm.buf, n * S, 1 << 30, 0, hx, 1, pl);
+    for (int v = 0; v < n; ++v) {
+      const R q = (R)d.qv[v];
+      (void)q;
+      double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+      for (int e = threadIdx.x; e < S * hx; e += blockDim.x) {
+        int m = e % hx, r = e / hx, sr = v * S + r;
+        long long row = row0 + r;
+        int y = (int)(row % ny), z = (int)(row / ny);
+        C zc = cmul(sm.buf[sr * hx + sm.perm[m]], cconj(sm.ptw[m]));
+        R h0 = zc.x, h1 = -zc.y;
+        if ((m + y + z) & 1) h0 = -h0;
+        if ((m + hx + y + z) & 1) h1 = -h1;
+        long long base = (long long)v * d.N + row * nx;
+        if (MODE == 0) {
+          dst[base + m] = h0;
+          dst[base + m + hx] = h1;
+        } else {
+          double t0 = t[base + m], t1 = t[base + m + hx];
+          double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
+          double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + hx] + t1);
+          // tr: R = h + 1 - g with h = h_s - L, evaluated in FP64 and rounded
+          // once (R is small near convergence, g need not be)
+          R r0 = (R)((double)h0 + (double)lr[base + m] - g0);
+          R r1 = (R)((double)h1 + (double)lr[base + m + hx] - g1);
+          res[base + m] = r0;
+          res[base + m + hx] = r1;
+          acc_ss += (double)r0 * r0 + (double)r1 * r1;
+          if (dots) {
+            R a0 = rp[base + m], a1 = rp[base + m + hx];
+            R b0 = rp[niv + base + m], b1 = rp[niv + base + m + hx];
+            double t10 = (double)r0 - a0, t20 = (double)r0 - b0;
+            double t11 = (double)r1 - a1, t21 = (double)r1 - b1;
+            s0 += r0 * t10 + r1 * t11;
+            s1 += r0 * t20 + r1 * t21;
+            s2 += t10 * t10 + t11 * t11;
+            s3 += t10 * t20 + t11 * t21;
+            s4 += t20 * t20 + t21 * t21;
+          }
+        }
+      }
+      if (dots) {
+        acc[v][0] += s0;
+        acc[v][1] += s1;
+        acc[v][2] += s2;
+        acc[v][3] += s3;
+        acc[v][4] += s4;
+      }
+    }
+  }
+  if (MODE == 0) return;
+  double *part = d.partials + (size_t)cta * kPartials;
+  double s = block_sum<R>(acc_ss, red);
+  if (threadIdx.x == 0) part[0] = s;
+  if (dots) {
+    for (int v = 0; v < n; ++v)
+      for (int k = 0; k < 5; ++k) {
+        double x = block_sum<R>(acc[v][k], red);
+        if (threadIdx.x == 0) part[1 + 5 * v + k] = x;
+      }
+  }
+}
+
+// ======================================================================
+// Control kernels (1 CTA per solve).
+// ======================================================================
+// leg (anderson.cu:105-130): 2x2 Gaussian elimination, no pivoting.
+__device__ void leg2(double *a, double *x, double *bb) {
+  double p = a[0];
+  a[1] /= p;
+  double r = bb[0] /= p;
+  double q = a[2];
+  a[3] -= q * a[1];
+  bb[1] -= q * r;
+  x[1] = bb[1] / a[3];
+  x[0] = bb[0] - a[1] * x[1];
+}
+
+// Dense solve with partial pivoting (ANM); returns false when singular.
+__device__ bool solve_pp(double *A, double *x, int m) {
+  for (int k = 0; k < m; ++k) {
+    int piv = k;
+    double best = fabs(A[k * m + k]);
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(A[i * m + k]) > best) {
+        best = fabs(A[i * m + k]);
+        piv = i;
+      }
+    if (!(best > 1e-300)) return false;
+    if (piv != k) {
+      for (int j = 0; j < m; ++j) {
+        double tt = A[k * m + j];
+        A[k * m + j] = A[piv * m + j];
+        A[piv * m + j] = tt;
+      }
+      double tt = x[k];
+      x[k] = x[piv];
+      x[piv] = tt;
+    }
+    for (int i = k + 1; i < m; ++i) {
+      double f = A[i * m + k] / A[k * m + k];
+      for (int j = k; j < m; ++j) A[i * m + j] -= f * A[k * m + j];
+      x[i] -= f * x[k];
+    }
+  }
+  for (int k = m - 1; k >= 0; --k) {
+    double acc = x[k];
+    for (int j = k + 1; j < m; ++j) acc -= A[k * m + j] * x[j];
+    x[k] = acc / A[k * m + k];
+  }
+  for (int k = 0; k < m; ++k)
+    if (!isfinite(x[k])) return false;
+  return true;
+}
+
+// Reduce the IX partials of every solve: RMS and convergence/divergence
+// (iterate.cu:48-59, cal_rms.cu:14-26).  Grid = one CTA per solve.
+// AN2 coefficients (anderson.cu:54-73) are computed here too, so that the
+// mix kernel only reads them.  `force` = mix regardless of convergence
+// (the explicit anderson() API call).
+__global__ void __launch_bounds__(kThreads)
+    k_reduce(const Desc *descs, const int *ix_ctas, int mode_force) {
+  __shared__ double red[kThreads / 32];
+  __shared__ double sums[kPartials];
+  const Desc &d = descs[blockIdx.x];
+  Ctl *c = d.ctl;
+  if (c->status != RUNNING && mode_force == 0) {
+    if (threadIdx.x == 0) c->mix_flag = 0;
+    return;
+  }
+  const int nct = ix_ctas[blockIdx.x];
+  const int np = 1 + 5 * d.n;
+  const bool dots = d.mixer == MIX_AN2 && c->count_left <= 0;
+  for (int k = 0; k < np; ++k) {
+    if (k > 0 && !dots) break;
+    double v = 0;
+    for (int i = threadIdx.x; i < nct; i += blockDim.x)
+      v += d.partials[(size_t)i * kPartials + k];
+    double s = block_sum<double>(v, red);
+    if (threadIdx.x == 0) sums[k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  if (mode_force == 2) {  // calculate() only: record the rms, decide nothing
+    c->ss = sums[0];
+    c->rms = sqrt(sums[0] / ((double)d.N * d.n));
+    c->step += 1;
+    return;
+  }
+  if (mode_force == 0) {
+    c->ss = sums[0];
+    c->rms = sqrt(sums[0] / ((double)d.N * d.n));
+    c->step += 1;
+    if (c->step <= c->maxstep) d.rmslog[c->step - 1] = c->rms;
+    if (!isfinite(c->rms)) {
+      c->status = DIVERGED;
+      c->mix_flag = 0;
+      return;
+    }
+    if (c->rms <= c->tol) {
+      c->status = CONVERGED;
+      c->mix_flag = 0;
+      return;
+    }
+    if (c->step >= c->maxstep) c->status = MAXSTEP;  // still mixes this step
+  }
+  c->mix_flag = 1;
+  if (d.mixer == MIX_AN2) {
+    if (c->count_left > 0) {  // newdt0 (Picard) step
+      c->count_left -= 1;
+      c->coef[0] = 0;
+      c->coef[1] = 0;
+      c->coef[2] = -1.0;  // marker: Picard
+      c->coef[3] = (double)c->binary;
+    } else {
+      double a[4], cc[2], x[2];
+      cc[0] = cc[1] = a[0] = a[1] = a[3] = 0.0;
+      for (int v = 0; v < d.n; ++v) {  // cal_theta, anderson.cu:81-102
+        cc[0] += sums[1 + 5 * v + 0] * d.irho[v];
+        cc[1] += sums[1 + 5 * v + 1] * d.irho[v];
+        a[0] += sums[1 + 5 * v + 2] * d.irho[v];
+        a[1] += sums[1 + 5 * v + 3] * d.irho[v];
+        a[3] += sums[1 + 5 * v + 4] * d.irho[v];
+      }
+      a[2] = a[1];
+      leg2(a, x, cc);
+      c->coef[0] = x[0] + d.mp * ((c->binary == 0) ? 0 : 1);
+      c->coef[1] = x[1] + d.mp * ((c->binary == 0) ? 1 : 0);
+      c->coef[2] = 1.0;
+      c->coef[3] = (double)c->binary;
+    }
+    c->binary = (c->binary == 0) ? 1 : 0;
+  }
+}
+
+// AN2 mix: newdt0 / newdt (anderson_cuda.cu:1-22), all sites in one launch.
+template <typename P>
+__global__ void __launch_bounds__(kThreads)
+    k_mix_an2(Batch b) {
+  using R = typename P::R;
+  using T = typename P::T;
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  const Ctl *c = d.ctl;
+  if (!c->mix_flag) return;
+  const long long niv = (long long)d.n * d.N;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int nct = b.prefix[si + 1] - b.prefix[si];
+  T *t = (T *)d.t;
+  const R *r = (const R *)d.res;
+  T *tp = (T *)d.hist_a;
+  R *rp = (R *)d.hist_b;
+  const bool picard = c->coef[2] < 0;
+  const long long boff = (long long)c->coef[3] * niv;
+  const double s1 = c->coef[0], s2 = c->coef[1], m = d.m;
+  for (long long i = (long long)cta * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)nct * blockDim.x) {
+    T ti = t[i];
+    R ri = r[i];
+    if (picard) {
+      tp[boff + i] = ti;
+      rp[boff + i] = ri;
+      t[i] = ti + (T)ri;
+    } else {
+      double tt = ti, rr = ri;
+      double tp0 = tp[i], tp1 = tp[i + niv];
+      double rp0 = rp[i], rp1 = rp[i + niv];
+      double uu = tt + s1 * (tp0 - tt) + s2 * (tp1 - tt);
+      double vv = tt + rr + s1 * (tp0 + rp0 - tt - rr) + s2 * (tp1 + rp1 - tt - rr);
+      tp[boff + i] = ti;
+      rp[boff + i] = ri;
+      t[i] = (T)(uu + m * (vv - uu));
+    }
+  }
+}
+
+// ANM dots: <f_k, f_slot> (1/rho weighted) for the newest residual against
+// every stored residual.  Writes per-CTA partials [slot].
+template <typename P>
+__global__ void __launch_bounds__(kThreads)
+    k_anm_dots(Batch b) {
+  using R = typename P::R;
+  __shared__ double red[kThreads / 32];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  const Ctl *c = d.ctl;
+  if (c->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int nct = b.prefix[si + 1] - b.prefix[si];
+  const int H1 = d.history + 1;
+  const long long niv = (long long)d.n * d.N;
+  const R *f = (const R *)d.hist_a;
+  const R *res = (const R *)d.res;
+  double *part = d.partials + (size_t)cta * kPartials;
+  for (int i = 0; i <= c->hcount; ++i) {
+    // i == 0: self dot; i >= 1: history slot (head - i) mod H1
+    int slot = (c->hhead - i + 2 * H1) % H1;
+    const R *fi = i == 0 ? res : f + (long long)slot * niv;
+    double acc = 0;
+    for (int v = 0; v < d.n; ++v) {
+      double sv = 0;
+      const R *a = res + (long long)v * d.N, *bq = fi + (long long)v * d.N;
+      for (long long x = (long long)cta * blockDim.x + threadIdx.x; x < d.N;
+           x += (long long)nct * blockDim.x)
+        sv += (double)a[x] * (double)bq[x];
+      acc += sv * d.irho[v];
+    }
+    double s = block_sum<double>(acc, red);
+    if (threadIdx.x == 0) part[1 + i] = s;
+  }
+}
+
+// ANM coefficients: update the ring Gram, solve for alpha (1 thread/solve).
+__global__ void k_anm_coef(const Desc *descs, const int *ctas, int force) {
+  const Desc &d = descs[blockIdx.x];
+  Ctl *c = d.ctl;
+  if (threadIdx.x != 0) return;
+  if (!c->mix_flag) return;
+  const int nct = ctas[blockIdx.x];
+  const int H = d.history, H1 = H + 1, m = c->hcount;
+  double dot[kMaxHistory + 1];
+  for (int i = 0; i <= m; ++i) {
+    double s = 0;
+    for (int k = 0; k < nct; ++k) s += d.partials[(size_t)k * kPartials + 1 + i];
+    dot[i] = s;
+  }
+  const int head = c->hhead;
+  // Gram rows of the newest residual (stored under the head slot)
+  c->gram[head * H1 + head] = dot[0];
+  int slot[kMaxHistory];
+  for (int i = 1; i <= m; ++i) {
+    slot[i - 1] = (head - i + 2 * H1) % H1;
+    c->gram[head * H1 + slot[i - 1]] = dot[i];
+    c->gram[slot[i - 1] * H1 + head] = dot[i];
+  }
+  double A[kMaxHistory * kMaxHistory], x[kMaxHistory];
+  const double Fkk = dot[0];
+  for (int i = 0; i < m; ++i) {
+    x[i] = Fkk - dot[i + 1];
+    for (int j = 0; j < m; ++j)
+      A[i * m + j] = Fkk - dot[i + 1] - dot[j + 1] +
+                     c->gram[slot[i] * H1 + slot[j]];
+  }
+  bool ok = m > 0 && solve_pp(A, x, m);
+  double wsum = 0;
+  for (int i = 0; i < m; ++i) {
+    if (!ok) x[i] = 0;
+    wsum += x[i];
+  }
+  c->coef[0] = 1.0 - wsum;  // weight of the newest pair
+  for (int i = 0; i < m; ++i) {
+    c->coef[1 + i] = x[i];
+    c->mix_slots[i] = slot[i];
+  }
+  c->mix_m = m;
+  c->mix_head = head;
+  // the newest pair joins the history
+  c->hhead = (head + 1) % H1;
+  if (c->hcount < H) c->hcount += 1;
+  (void)force;
+}
+
+// ANM mix: t_{k+1} = w_k (t_k + beta R_k) + sum_i alpha_i z_i ; the newest
+// pair (R_k, z_k = t_k + beta R_k) is written into the ring under `head`.
+template <typename P>
+__global__ void __launch_bounds__(kThreads)
+    k_mix_anm(Batch b) {
+  using R = typename P::R;
+  using T = typename P::T;
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  const Ctl *c = d.ctl;
+  if (!c->mix_flag) return;
+  const long long niv = (long long)d.n * d.N;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int nct = b.prefix[si + 1] - b.prefix[si];
+  const int head = c->mix_head, m = c->mix_m;
+  T *t = (T *)d.t;
+  const R *res = (const R *)d.res;
+  R *f = (R *)d.hist_a;
+  T *zr = (T *)d.hist_b;
+  const double beta = d.beta, w0 = c->coef[0];
+  for (long long i = (long long)cta * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)nct * blockDim.x) {
+    double rk = res[i];
+    double zk = (double)t[i] + beta * rk;
+    double acc = w0 * zk;
+    for (int j = 0; j < m; ++j)
+      acc += c->coef[1 + j] * (double)zr[(long long)c->mix_slots[j] * niv + i];
+    f[(long long)head * niv + i] = (R)rk;
+    zr[(long long)head * niv + i] = (T)zk;
+    t[i] = (T)acc;
+  }
+}
+
+// ======================================================================
+// Setup kernels: potentials (cal_LJ.cu, cal_Coulomb.cu, cal_potential.cu,
+// initialize_tuv.cu), phi_L(k), shell indices.
+// ======================================================================
+struct AtomTab {
+  const double *x, *y, *z, *q;  // [nu]
+  const double *isig2, *eps4;   // [n][nu]: 1/sigma_uv^2, 4 eps_uv
+  int nu;
+};
+
+constexpr int kAtomTile = 128;
+
+// One thread per voxel: LJ for every site, Coulomb real space; writes
+// u[v] = beta u_LJ + q_v beta phi(r), fr = beta phi_L(r), t0[v] = q_v fr.
+template <typename P, int NS>
+__global__ void __launch_bounds__(kThreads)
+    k_potential(Desc d, AtomTab at, double ikbt, double ubeta, double dx,
+                double dy, double dz, int coulomb, double *fr64) {
+  using R = typename P::R;
+  using T = typename P::T;
+  constexpr int M = NS > 0 ? NS : kMaxSites;
+  __shared__ double sx[kAtomTile], sy[kAtomTile], sz[kAtomTile], sq[kAtomTile];
+  __shared__ double ss[kMaxSites][kAtomTile], se[kMaxSites][kAtomTile];
+  const long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = ip < d.N;
+  const int n = d.n;
+  int x = 0, y = 0, z = 0;
+  if (live) {
+    x = (int)(ip % d.nx);
+    y = (int)((ip / d.nx) % d.ny);
+    z = (int)(ip / ((long long)d.nx * d.ny));
+  }
+  const double rx = (x - d.nx / 2) * dx, ry = (y - d.ny / 2) * dy,
+               rz = (z - d.nz / 2) * dz;
+  double lj[M];
+#pragma unroll
+  for (int v = 0; v < M; ++v) lj[v] = 0;
+  double e = 0, f = 0;
+  const double cut2 = 2.0e-3 * 2.0e-3;
+  for (int a0 = 0; a0 < at.nu; a0 += kAtomTile) {
+    const int na = min(kAtomTile, at.nu - a0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < na; i += blockDim.x) {
+      sx[i] = at.x[a0 + i];
+      sy[i] = at.y[a0 + i];
+      sz[i] = at.z[a0 + i];
+      sq[i] = at.q[a0 + i];
+      for (int v = 0; v < n; ++v) {
+        ss[v][i] = at.isig2[v * at.nu + a0 + i];
+        se[v][i] = at.eps4[v * at.nu + a0 + i];
+      }
+    }
+    __syncthreads();
+    for (int i = 0; i < na; ++i) {
+      double ddx = rx - sx[i], ddy = ry - sy[i], ddz = rz - sz[i];
+      double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+#pragma unroll
+      for (int v = 0; v < M; ++v) {  // LJ, cal_LJ.cu:56-81
+        if (NS > 0 || v < n) {
+          double rs2 = r2 * ss[v][i];
+          if (rs2 < cut2) rs2 = cut2;
+          double irs6 = 1.0 / (rs2 * rs2 * rs2);
+          lj[v] += se[v][i] * irs6 * (irs6 - 1.0);
+        }
+      }
+      if (coulomb) {  // coulomb, cal_Coulomb.cu:40-62
+        double ra = sqrt(r2);
+        if (ra >= 1.0e-5) {
+          double qr = sq[i] / ra;
+          e += qr;
+          f += qr * (1 - exp(-ra));
+        } else {
+          f += sq[i];
+        }
+      }
+    }
+  }
+  if (!live) return;
+  R *u = (R *)d.u, *fr = (R *)d.fr;
+  T *t = (T *)d.t;
+  const double bfr = f * ubeta, bde = e * ubeta;  // betar
+  fr[ip] = (R)bfr;
+  if (fr64) fr64[ip] = bfr;
+#pragma unroll
+  for (int v = 0; v < M; ++v) {
+    if (NS > 0 || v < n) {
+      // set_du, minus the long-range part; init_tuv's t0 = q_v fr is
+      // t_s = 0 on the short-range side
+      u[(long long)v * d.N + ip] = (R)(lj[v] * ikbt + d.qv[v] * bde - d.qv[v] * bfr);
+      t[(long long)v * d.N + ip] = (T)0;
+    }
+  }
+}
+
+// Per-axis phase tables e^{-i k_j x_u} (FP64): ex[u][p] (k index j = 2p),
+// ey[u][y], ez[u][z].
+__global__ void k_phase_tables(double2 *ex, double2 *ey, double2 *ez,
+                               const double *ax, const double *ay,
+                               const double *az, int nu, int nx, int ny,
+                               int nz, double bx, double by, double bz) {
+  const int hx = nx / 2;
+  const long long tot = (long long)nu * (hx + ny + nz);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
+       i += (long long)gridDim.x * blockDim.x) {
+    int u = (int)(i / (hx + ny + nz)), j = (int)(i % (hx + ny + nz));
+    double k, r;
+    double2 *dst;
+    if (j < hx) {
+      k = 2.0 * M_PI * (2 * j - nx / 2.0 + 0.5) / bx;
+      r = ax[u];
+      dst = ex + (long long)u * hx + j;
+    } else if (j < hx + ny) {
+      j -= hx;
+      k = 2.0 * M_PI * (j - ny / 2.0 + 0.5) / by;
+      r = ay[u];
+      dst = ey + (long long)u * ny + j;
+    } else {
+      j -= hx + ny;
+      k = 2.0 * M_PI * (j - nz / 2.0 + 0.5) / bz;
+      r = az[u];
+      dst = ez + (long long)u * nz + j;
+    }
+    double s, c;
+    sincos(k * r, &s, &c);
+    *dst = make_double2(c, -s);
+  }
+}
+
+// phi_L(k) in transform units: fk = ubeta sum_u 4 pi q_u / (k^2 (k^2+1))
+// e^{-i k.r_u} (cal_Coulomb.cu:65-95), divided by dv * C(k) with
+// C(k) = -i (-1)^{jx+jy+jz+(nx+ny+nz)/2}.  One thread per k point.
+__global__ void __launch_bounds__(kThreads)
+    k_fk(Desc d, double2 *fk64, const double2 *ex, const double2 *ey,
+         const double2 *ez, const double *q, int nu, double ubeta, double bx,
+         double by, double bz, double dv) {
+  __shared__ double2 sey[kAtomTile], sez[kAtomTile];
+  __shared__ double sq[kAtomTile];
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < d.Nh;
+  const int hx = d.hx;
+  int p = 0, y = 0, z = 0;
+  if (live) {
+    p = (int)(i % hx);
+    y = (int)((i / hx) % d.ny);
+    z = (int)(i / ((long long)hx * d.ny));
+  }
+  // all threads of a CTA share (y, z) only if hx >= blockDim; otherwise read
+  // ey / ez per thread through L1.
+  double re = 0, im = 0;
+  for (int a0 = 0; a0 < nu; a0 += kAtomTile) {
+    const int na = min(kAtomTile, nu - a0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < na; k += blockDim.x) sq[k] = q[a0 + k];
+    __syncthreads();
+    if (live) {
+      for (int k = 0; k < na; ++k) {
+        const int uu = a0 + k;
+        double2 a = ex[(long long)uu * hx + p];
+        double2 b2 = ey[(long long)uu * d.ny + y];
+        double2 c2 = ez[(long long)uu * d.nz + z];
+        double abr = a.x * b2.x - a.y * b2.y, abi = a.x * b2.y + a.y * b2.x;
+        double pr = abr * c2.x - abi * c2.y, pi = abr * c2.y + abi * c2.x;
+        re += sq[k] * pr;
+        im += sq[k] * pi;
+      }
+    }
+  }
+  (void)sey;
+  (void)sez;
+  if (!live) return;
+  const double kx = 2.0 * M_PI * (2 * p - d.nx / 2.0 + 0.5) / bx;
+  const double ky = 2.0 * M_PI * (y - d.ny / 2.0 + 0.5) / by;
+  const double kz = 2.0 * M_PI * (z - d.nz / 2.0 + 0.5) / bz;
+  const double rk2 = kx * kx + ky * ky + kz * kz;
+  const double rk4i = 1.0 / (rk2 * (rk2 + 1.0));
+  const double sc = 4.0 * M_PI * rk4i * ubeta;
+  re *= sc;
+  im *= sc;
+  // divide by dv * C:  (re + i im) * conj(C) / dv, conj(C) = i * sigma
+  int par = (2 * p + y + z + (d.nx + d.ny + d.nz) / 2) & 1;
+  double sg = par ? -1.0 : 1.0;
+  fk64[i] = make_double2(-im * sg / dv, re * sg / dv);
+}
+
+// Refresh, step 1: freeze c_ref = c_s(t) in the grid type, and an FP64 copy
+// of exactly the stored values for the FP64 transform.
+template <typename P>
+__global__ void k_cref(Desc d, double *c64) {
+  using R = typename P::R;
+  using T = typename P::T;
+  const long long niv = (long long)d.n * d.N;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u;
+  R *cref = (R *)d.cref;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)gridDim.x * blockDim.x) {
+    double g = closure_g<double>(d.clos, d.pse_n, -(double)u[i] + (double)t[i]);
+    R c = (R)(g - 1.0 - (double)t[i]);
+    cref[i] = c;
+    c64[i] = (double)c;
+  }
+}
+
+// Refresh, step 2: lr = 1 + h_ref (h_ref from the FP64 transform).
+template <typename P>
+__global__ void k_lr_update(const double *href, typename P::R *lr, long long niv) {
+  using R = typename P::R;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)gridDim.x * blockDim.x)
+    lr[i] = (R)(1.0 + href[i]);
+}
+
+// Shell index of each half-spectrum point.  Cubic boxes: (s - 3) / 8 with
+// s = ax^2 + ay^2 + az^2 over the odd integers a = 2j - n + 1; otherwise a
+// lookup in the host-built table of (|ax|, |ay|, |az|) tuples.
+__global__ void k_kidx(Desc d, const uint32_t *tuple_idx, int cubic) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.Nh) return;
+  const int hx = d.hx;
+  int p = (int)(i % hx), y = (int)((i / hx) % d.ny),
+      z = (int)(i / ((long long)hx * d.ny));
+  int ax = 4 * p - d.nx + 1, ay = 2 * y - d.ny + 1, az = 2 * z - d.nz + 1;
+  uint32_t s;
+  if (cubic) {
+    long long ss = (long long)ax * ax + (long long)ay * ay + (long long)az * az;
+    s = (uint32_t)((ss - 3) / 8);
+  } else {
+    int ix = (abs(ax) - 1) / 2, iy = (abs(ay) - 1) / 2, iz = (abs(az) - 1) / 2;
+    s = tuple_idx[((long long)iz * (d.ny / 2) + iy) * (d.nx / 2) + ix];
+  }
+  ((uint32_t *)d.kidx)[i] = s;
+}
+
+// ======================================================================
+// Thermodynamics (cal_exchem.cu:55-155, cal_pmv.cu:27-57): per-site sums of
+// the closure functional, HNC functional, GF functional and c = h - t.
+// g is rebuilt from (tg, u), h = R - 1 + g; c uses the current t.
+// ======================================================================
+template <typename P>
+__global__ void __launch_bounds__(kThreads)
+    k_thermo(Desc d, const typename P::T *tg, double *out /* [ctas][n][4] */) {
+  using R = typename P::R;
+  using T = typename P::T;
+  __shared__ double red[kThreads / 32];
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *res = (const R *)d.res;
+  const R *fr = (const R *)d.fr;
+  for (int v = 0; v < d.n; ++v) {
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < d.N;
+         x += (long long)gridDim.x * blockDim.x) {
+      long long i = (long long)v * d.N + x;
+      // physical t = t_s + q_v beta phi_L(r); t* = t - beta u = t_s - u_s
+      double tt = (double)t[i] + d.qv[v] * (double)fr[x];
+      double ts = -(double)u[i] + (double)tg[i];
+      double g = closure_g<double>(d.clos, d.pse_n, ts);
+      double h = (double)res[i] - 1.0 + g;
+      double c = h - tt;
+      double ehnc = h * 0.5 * tt - c;
+      double egf = -(h * 0.5 + 1.0) * c;
+      double esc;
+      if (d.clos == HNC) {
+        esc = ehnc;
+      } else if (h > 0.0) {
+        if (d.clos == KH || d.pse_n == 1) {
+          esc = egf;
+        } else {
+          double term = 1.0;
+          for (int k = 1; k <= d.pse_n + 1; ++k) term *= ts / k;
+          esc = 0.5 * h * h - c - 0.5 * h * c - term;
+        }
+      } else {
+        esc = ehnc;
+      }
+      a0 += esc;
+      a1 += ehnc;
+      a2 += egf;
+      a3 += c;
+    }
+    double s0 = block_sum<double>(a0, red);
+    double s1 = block_sum<double>(a1, red);
+    double s2 = block_sum<double>(a2, red);
+    double s3 = block_sum<double>(a3, red);
+    if (threadIdx.x == 0) {
+      double *o = out + ((size_t)blockIdx.x * d.n + v) * 4;
+      o[0] = s0;
+      o[1] = s1;
+      o[2] = s2;
+      o[3] = s3;
+    }
+  }
+}
+
+// g (and h) grids for read-back: g = closure(t - u), h = R - 1 + g.
+template <typename P>
+__global__ void k_gh(Desc d, const typename P::T *tg, double *g, double *h) {
+  using R = typename P::R;
+  const long long niv = (long long)d.n * d.N;
+  const R *u = (const R *)d.u, *res = (const R *)d.res;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)gridDim.x * blockDim.x) {
+    double gv = closure_g<double>(d.clos, d.pse_n, -(double)u[i] + (double)tg[i]);
+    if (g) g[i] = gv;
+    if (h) h[i] = (double)res[i] - 1.0 + gv;
+  }
+}
+
+template <typename R>
+__global__ void k_to_double(const R *src, double *dst, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+template <typename R>
+__global__ void k_from_double(const double *src, R *dst, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (R)src[i];
+}
+// short-range -> physical: dst = src + sign * q_v fr  (per-site grids)
+template <typename P, typename X>
+__global__ void k_shift_qfr(Desc d, const X *src, double *dst, double sign) {
+  using R = typename P::R;
+  const long long niv = (long long)d.n * d.N;
+  const R *fr = (const R *)d.fr;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)gridDim.x * blockDim.x) {
+    int v = (int)(i / d.N);
+    dst[i] = (double)src[i] + sign * d.qv[v] * (double)fr[i % d.N];
+  }
+}
+// physical -> short-range: dst = src - q_v fr
+template <typename P>
+__global__ void k_set_short(Desc d, const double *src, typename P::T *dst) {
+  using R = typename P::R;
+  using T = typename P::T;
+  const long long niv = (long long)d.n * d.N;
+  const R *fr = (const R *)d.fr;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
+       i += (long long)gridDim.x * blockDim.x) {
+    int v = (int)(i / d.N);
+    dst[i] = (T)(src[i] - d.qv[v] * (double)fr[i % d.N]);
+  }
+}
+
+// ======================================================================
+// Host-side launch wrappers
+// ======================================================================
+size_t smem_x(int hx, int n, int S, size_t csz) {
+  return csz * hx * 2 + ((2 * hx + 15) / 16) * 16 + csz * (size_t)n * S * hx;
+}
+size_t smem_y(int ny, int P, size_t csz) {
+  return csz * ny * 2 + ((2 * ny + 15) / 16) * 16 + csz * (size_t)ny * P;
+}
+size_t smem_z(int nz, int n, int P, size_t csz) {
+  return csz * nz * 2 + ((2 * nz + 15) / 16) * 16 + csz * (size_t)n * nz * P;
+}
+
+template <typename P>
+static void set_smem_attrs(size_t maxbytes) {
+  const int mb = (int)maxbytes;
+  const auto a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaFuncSetAttribute(k_fwd_x<P, 0>, a, mb);
+  cudaFuncSetAttribute(k_fwd_x<P, 1>, a, mb);
+  cudaFuncSetAttribute(k_fft_y<P, -1>, a, mb);
+  cudaFuncSetAttribute(k_fft_y<P, 1>, a, mb);
+  cudaFuncSetAttribute(k_zoz<P, 0>, a, mb);
+  cudaFuncSetAttribute(k_zoz<P, 1>, a, mb);
+  cudaFuncSetAttribute(k_zoz<P, 2>, a, mb);
+  cudaFuncSetAttribute(k_inv_x<P, 0>, a, mb);
+  cudaFuncSetAttribute(k_inv_x<P, 1>, a, mb);
+}
+
+void kernels_set_smem(bool fp64, size_t maxbytes) {
+  if (fp64)
+    set_smem_attrs<P64>(maxbytes);
+  else
+    set_smem_attrs<PMix>(maxbytes);
+}
+
+// Pass launchers.  `grid` = total CTAs of the pass over all solves in the
+// batch; `smem` = dynamic shared memory (max over solves).
+template <typename P>
+void launch_fwd_x(Batch b, int grid, size_t smem, cudaStream_t s, int mode,
+                  const void *src) {
+  using R = typename P::R;
+  if (mode == 0)
+    k_fwd_x<P, 0><<<grid, kThreads, smem, s>>>(b, (const R *)src);
+  else
+    k_fwd_x<P, 1><<<grid, kThreads, smem, s>>>(b, nullptr);
+}
+template <typename P>
+void launch_fft_y(Batch b, int grid, size_t smem, cudaStream_t s, int dir,
+                  int check) {
+  if (dir < 0)
+    k_fft_y<P, -1><<<grid, kThreads, smem, s>>>(b, check);
+  else
+    k_fft_y<P, 1><<<grid, kThreads, smem, s>>>(b, check);
+}
+template <typename P>
+void launch_zoz(Batch b, int grid, size_t smem, cudaStream_t s, int mode,
+                int check) {
+  if (mode == 0)
+    k_zoz<P, 0><<<grid, kThreads, smem, s>>>(b, check);
+  else if (mode == 1)
+    k_zoz<P, 1><<<grid, kThreads, smem, s>>>(b, check);
+  else
+    k_zoz<P, 2><<<grid, kThreads, smem, s>>>(b, check);
+}
+template <typename P>
+void launch_inv_x(Batch b, int grid, size_t smem, cudaStream_t s, int mode,
+                  void *dst, int per) {
+  using R = typename P::R;
+  if (mode == 0)
+    k_inv_x<P, 0><<<grid, kThreads, smem, s>>>(b, (R *)dst, per);
+  else
+    k_inv_x<P, 1><<<grid, kThreads, smem, s>>>(b, nullptr, per);
+}
+void launch_reduce(const Desc *d, const int *ctas, int ns, int force,
+                   cudaStream_t s) {
+  k_reduce<<<ns, kThreads, 0, s>>>(d, ctas, force);
+}
+template <typename P>
+void launch_mix_an2(Batch b, int grid, cudaStream_t s) {
+  k_mix_an2<P><<<grid, kThreads, 0, s>>>(b);
+}
+template <typename P>
+void launch_anm(Batch b, int grid, const Desc *d, const int *ctas, int ns,
+                cudaStream_t s, int stage) {
+  if (stage == 0)
+    k_anm_dots<P><<<grid, kThreads, 0, s>>>(b);
+  else if (stage == 1)
+    k_anm_coef<<<ns, 32, 0, s>>>(d, ctas, 0);
+  else
+    k_mix_anm<P><<<grid, kThreads, 0, s>>>(b);
+}
+template <typename P>
+void launch_potential(const Desc &d, const AtomTab &at, double ikbt,
+                      double ubeta, const double *dr, int coulomb,
+                      double *fr64, cudaStream_t s) {
+  int grid = (int)((d.N + kThreads - 1) / kThreads);
+#define R3D_POT(NS)                                                        \
+  k_potential<P, NS><<<grid, kThreads, 0, s>>>(d, at, ikbt, ubeta, dr[0], \
+                                               dr[1], dr[2], coulomb, fr64)
+  switch (d.n) {
+    case 1: R3D_POT(1); break;
+    case 2: R3D_POT(2); break;
+    case 3: R3D_POT(3); break;
+    case 4: R3D_POT(4); break;
+    default: R3D_POT(0); break;
+  }
+#undef R3D_POT
+}
+void launch_phase_tables(double2 *ex, double2 *ey, double2 *ez,
+                         const double *ax, const double *ay, const double *az,
+                         int nu, int nx, int ny, int nz, const double *box,
+                         cudaStream_t s) {
+  k_phase_tables<<<1184, kThreads, 0, s>>>(ex, ey, ez, ax, ay, az, nu, nx, ny,
+                                           nz, box[0], box[1], box[2]);
+}
+void launch_fk(const Desc &d, double2 *fk64, const double2 *ex,
+               const double2 *ey, const double2 *ez, const double *q, int nu,
+               double ubeta, const double *box, double dv, cudaStream_t s) {
+  int grid = (int)((d.Nh + kThreads - 1) / kThreads);
+  k_fk<<<grid, kThreads, 0, s>>>(d, fk64, ex, ey, ez, q, nu, ubeta, box[0],
+                                 box[1], box[2], dv);
+}
+template <typename P>
+void launch_cref(const Desc &d, double *c64, cudaStream_t s) {
+  k_cref<P><<<1184, kThreads, 0, s>>>(d, c64);
+}
+template <typename P>
+void launch_lr_update(const double *href, void *lr, long long niv,
+                      cudaStream_t s) {
+  k_lr_update<P><<<1184, kThreads, 0, s>>>(href, (typename P::R *)lr, niv);
+}
+void launch_kidx(const Desc &d, const uint32_t *tuple_idx, int cubic,
+                 cudaStream_t s) {
+  int grid = (int)((d.Nh + kThreads - 1) / kThreads);
+  k_kidx<<<grid, kThreads, 0, s>>>(d, tuple_idx, cubic);
+}
+template <typename P>
+void launch_thermo(const Desc &d, const void *tg, double *out, int ctas,
+                   cudaStream_t s) {
+  k_thermo<P><<<ctas, kThreads, 0, s>>>(d, (const typename P::T *)tg, out);
+}
+template <typename P>
+void launch_gh(const Desc &d, const void *tg, double *g, double *h,
+               cudaStream_t s) {
+  k_gh<P><<<1184, kThreads, 0, s>>>(d, (const typename P::T *)tg, g, h);
+}
+// element-type conversions: x = 0 grid type R, x = 1 state type T
+template <typename P>
+void launch_to_double(const void *src, double *dst, long long n, int x,
+                      cudaStream_t s) {
+  if (x == 0)
+    k_to_double<typename P::R><<<1184, kThreads, 0, s>>>((const typename P::R *)src, dst, n);
+  else
+    k_to_double<typename P::T><<<1184, kThreads, 0, s>>>((const typename P::T *)src, dst, n);
+}
+template <typename P>
+void launch_from_double(const double *src, void *dst, long long n, int x,
+                        cudaStream_t s) {
+  if (x == 0)
+    k_from_double<typename P::R><<<1184, kThreads, 0, s>>>(src, (typename P::R *)dst, n);
+  else
+    k_from_double<typename P::T><<<1184, kThreads, 0, s>>>(src, (typename P::T *)dst, n);
+}
+template <typename P>
+void launch_shift_qfr(const Desc &d, const void *src, double *dst, double sign,
+                      int x, cudaStream_t s) {
+  if (x == 0)
+    k_shift_qfr<P, typename P::R><<<1184, kThreads, 0, s>>>(
+        d, (const typename P::R *)src, dst, sign);
+  else
+    k_shift_qfr<P, typename P::T><<<1184, kThreads, 0, s>>>(
+        d, (const typename P::T *)src, dst, sign);
+}
+template <typename P>
+void launch_set_short(const Desc &d, const double *src, void *dst,
+                      cudaStream_t s) {
+  k_set_short<P><<<1184, kThreads, 0, s>>>(d, src, (typename P::T *)dst);
+}
+
+#define R3D_INST(P)                                                            \
+  template void launch_fwd_x<P>(Batch, int, size_t, cudaStream_t, int,         \
+                                const void *);                                 \
+  template void launch_fft_y<P>(Batch, int, size_t, cudaStream_t, int, int);   \
+  template void launch_zoz<P>(Batch, int, size_t, cudaStream_t, int, int);     \
+  template void launch_inv_x<P>(Batch, int, size_t, cudaStream_t, int, void *, \
+                                int);                                          \
+  template void launch_mix_an2<P>(Batch, int, cudaStream_t);                   \
+  template void launch_anm<P>(Batch, int, const Desc *, const int *, int,      \
+                              cudaStream_t, int);                              \
+  template void launch_potential<P>(const Desc &, const AtomTab &, double,     \
+                                    double, const double *, int, double *,     \
+                                    cudaStream_t);                             \
+  template void launch_cref<P>(const Desc &, double *, cudaStream_t);          \
+  template void launch_lr_update<P>(const double *, void *, long long,         \
+                                    cudaStream_t);                             \
+  template void launch_thermo<P>(const Desc &, const void *, double *, int,    \
+                                 cudaStream_t);                                \
+  template void launch_gh<P>(const Desc &, const void *, double *, double *,   \
+                             cudaStream_t);                                    \
+  template void launch_to_double<P>(const void *, double *, long long, int,    \
+                                    cudaStream_t);                             \
+  template void launch_from_double<P>(const double *, void *, long long, int,  \
+                                      cudaStream_t);                           \
+  template void launch_shift_qfr<P>(const Desc &, const void *, double *,      \
+                                    double, int, cudaStream_t);                \
+  template void launch_set_short<P>(const Desc &, const double *, void *,      \
+                                    cudaStream_t);
+R3D_INST(P64)
+R3D_INST(PMix)
+
+}  // namespace r3d

@@ -1,0 +1,226 @@
+"""Python host mirror of the reference's RISM3D class over the B200 solver's
+C-ABI (include/rism3d_b200.h, lib/librism3d_b200.so).
+
+    s = RISM3D(precision="fp64")          # rism3d.h:21-105
+    s.initialize("test1.inp")             # initialize.cu:4-44 (+ .xvk)
+    steps, rms, status = s.iterate()      # iterate.cu:6-107
+    s.output()                            # output.cu 'm': writes test1.xmu
+
+The CUDA library is the only implementation: if it is missing this module
+raises at import, and there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "librism3d_b200.so")
+
+FP64, MIXED = 0, 1
+KH, HNC, PSE = 0, 1, 2
+MIX_AN2, MIX_ANM = 0, 1
+CONVERGED, MAXSTEP, DIVERGED = 0, 1, 2
+STATUS = {CONVERGED: "converged", MAXSTEP: "maxstep", DIVERGED: "diverged"}
+GRID = {"u": 0, "t": 1, "g": 2, "h": 3, "R": 4, "fr": 5, "fk": 6}
+ERRORS = {1: "EINVAL", 2: "EIO", 3: "ECUDA", 4: "ENOMEM", 5: "ESTATE", 6: "EBUDGET"}
+
+# every entry point include/rism3d_b200.h declares
+EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_load_inp",
+           "r3d_load_xvk", "r3d_set_problem", "r3d_set_closure", "r3d_set_mixer",
+           "r3d_set_control", "r3d_initialize", "r3d_calculate", "r3d_anderson",
+           "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
+           "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_fft3d"]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int),
+                ("hbm_budget", ctypes.c_ulonglong), ("verbose", ctypes.c_int)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built: run `make -C {_HERE}` (nvcc, sm_100a)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    ci, cd, cs = ctypes.c_int, ctypes.c_double, ctypes.c_char_p
+    sig = {
+        "r3d_create": [ctypes.POINTER(Opts), ctypes.POINTER(vp)],
+        "r3d_destroy": [vp],
+        "r3d_set_ad": [vp, cd, ci],
+        "r3d_load_inp": [vp, cs, cs, ci, ci],
+        "r3d_load_xvk": [vp, cs],
+        "r3d_set_problem": [vp, vp],
+        "r3d_set_closure": [vp, ci, ci],
+        "r3d_set_mixer": [vp, ci, ci, cd],
+        "r3d_set_control": [vp, cd, ci],
+        "r3d_initialize": [vp],
+        "r3d_calculate": [vp, dp],
+        "r3d_anderson": [vp],
+        "r3d_iterate": [vp, ip, dp, ip],
+        "r3d_thermo": [vp, dp, dp, dp, dp],
+        "r3d_write_xmu": [vp, cs],
+        "r3d_get_grid": [vp, ci, dp],
+        "r3d_set_t": [vp, dp],
+        "r3d_info": [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong), ip],
+        "r3d_device_bytes": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
+        "r3d_iter_timing": [vp, dp, ip],
+        "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ci
+    L.r3d_last_error.argtypes = [vp]
+    L.r3d_last_error.restype = cs
+    return L
+
+
+lib = _load()
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class R3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class RISM3D:
+    """One 3D-RISM solve on one GPU (device < 0: host-only, for planning)."""
+
+    def __init__(self, device=0, precision="fp64", hbm_budget=0, verbose=False):
+        o = Opts(device, FP64 if precision in ("fp64", FP64) else MIXED, hbm_budget, int(verbose))
+        h = ctypes.c_void_p()
+        self._check(lib.r3d_create(ctypes.byref(o), ctypes.byref(h)), None)
+        self.h = h
+        self.precision = precision
+
+    def _check(self, rc, h=-1):
+        if rc:
+            msg = lib.r3d_last_error(self.h if h == -1 else h)
+            raise R3DError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.r3d_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- RISM3D public interface (rism3d.h:26-29) ---------------------------
+    def set_ad(self, lam, switch):
+        self._check(lib.r3d_set_ad(self.h, lam, switch))
+
+    def load(self, control, structure=None, centering=True, q0=False, xvk=None):
+        self._check(lib.r3d_load_inp(self.h, control.encode(),
+                                     structure.encode() if structure else None,
+                                     int(centering), int(q0)))
+        self._check(lib.r3d_load_xvk(self.h, xvk.encode() if xvk else None))
+
+    def initialize(self, control=None, structure=None, centering=True, q0=False, xvk=None):
+        if control is not None:
+            self.load(control, structure, centering, q0, xvk)
+        self._check(lib.r3d_initialize(self.h))
+
+    def iterate(self):
+        st, rms, status = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        self._check(lib.r3d_iterate(self.h, ctypes.byref(st), ctypes.byref(rms),
+                                    ctypes.byref(status)))
+        return st.value, rms.value, STATUS[status.value]
+
+    def output(self, path=None):
+        self._check(lib.r3d_write_xmu(self.h, path.encode() if path else None))
+
+    # --- internal seams kept by the drop-in ---------------------------------
+    def calculate(self):
+        r = ctypes.c_double()
+        self._check(lib.r3d_calculate(self.h, ctypes.byref(r)))
+        return r.value
+
+    def anderson(self):
+        self._check(lib.r3d_anderson(self.h))
+
+    # --- extensions --------------------------------------------------------
+    def set_closure(self, clos, pse_n=1):
+        self._check(lib.r3d_set_closure(self.h, clos, pse_n))
+
+    def set_mixer(self, mixer, history=2, damping=-1.0):
+        self._check(lib.r3d_set_mixer(self.h, mixer, history, damping))
+
+    def set_control(self, convergence=0.0, maxstep=0):
+        self._check(lib.r3d_set_control(self.h, convergence, maxstep))
+
+    def info(self):
+        g = (ctypes.c_int * 3)()
+        n, nu = ctypes.c_int(), ctypes.c_int()
+        N = ctypes.c_longlong()
+        self._check(lib.r3d_info(self.h, g, ctypes.byref(n), ctypes.byref(N), ctypes.byref(nu)))
+        return dict(grid=tuple(g), natv=n.value, ngrid=N.value, nu=nu.value)
+
+    def device_bytes(self):
+        b = ctypes.c_ulonglong()
+        self._check(lib.r3d_device_bytes(self.h, ctypes.byref(b)))
+        return b.value
+
+    def timing(self):
+        ms, k = ctypes.c_double(), ctypes.c_int()
+        self._check(lib.r3d_iter_timing(self.h, ctypes.byref(ms), ctypes.byref(k)))
+        return ms.value, k.value
+
+    def thermo(self):
+        n = self.info()["natv"]
+        xmu, xmu2 = np.zeros(2 * n), np.zeros(n)
+        pmv, pr = ctypes.c_double(), ctypes.c_double()
+        self._check(lib.r3d_thermo(self.h, _dp(xmu), _dp(xmu2), ctypes.byref(pmv), ctypes.byref(pr)))
+        return xmu, xmu2, pmv.value, pr.value
+
+    def get(self, which):
+        inf = self.info()
+        nx, ny, nz = inf["grid"]
+        n = inf["natv"]
+        k = GRID[which]
+        if k == GRID["fk"]:
+            out = np.zeros(2 * (nx // 2) * ny * nz)
+            self._check(lib.r3d_get_grid(self.h, k, _dp(out)))
+            return (out[0::2] + 1j * out[1::2]).reshape(nz, ny, nx // 2)
+        out = np.zeros((1 if k == GRID["fr"] else n) * nx * ny * nz)
+        self._check(lib.r3d_get_grid(self.h, k, _dp(out)))
+        return out.reshape(nz, ny, nx) if k == GRID["fr"] else out.reshape(n, nz, ny, nx)
+
+    def set_t(self, t):
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        self._check(lib.r3d_set_t(self.h, _dp(t)))
+
+
+def fft3d(data, box, direction, precision="fp64", device=0):
+    """FFT3D::execute seam: real [nz,ny,nx] -> half spectrum [nz,ny,nx/2]
+    (direction -1) or back (+1); k_x index 2p of the reference's grid."""
+    b = np.asarray(box, dtype=np.float64)
+    prec = FP64 if precision == "fp64" else MIXED
+    if direction == -1:
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        nz, ny, nx = a.shape
+        out = np.zeros(2 * (nx // 2) * ny * nz)
+        rc = lib.r3d_fft3d(device, prec, nx, ny, nz, _dp(b), -1, _dp(a), _dp(out))
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+        return (out[0::2] + 1j * out[1::2]).reshape(nz, ny, nx // 2)
+    a = np.ascontiguousarray(data, dtype=np.complex128)
+    nz, ny, hx = a.shape
+    nx = 2 * hx
+    flat = a.view(np.float64).reshape(-1).copy()
+    out = np.zeros(nx * ny * nz)
+    rc = lib.r3d_fft3d(device, prec, nx, ny, nz, _dp(b), 1, _dp(flat), _dp(out))
+    if rc:
+        raise R3DError(rc, lib.r3d_last_error(None).decode())
+    return out.reshape(nz, ny, nx)

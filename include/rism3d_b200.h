@@ -1,0 +1,169 @@
+/*
+ * rism3d_b200.h -- C-ABI of the B200-native 3D-RISM solver.
+ *
+ * The reference solver (rismical-dev/3D-RISM-CUDA-MPI) exposes no library
+ * interface: its solve path is the C++ class RISM3D (src-cuda-mpi/rism3d.h:21-105)
+ * driven by main() (main.cu:6-69).  This header is the drop-in boundary for
+ * that path.  Each entry point names the reference member it replaces.
+ *
+ * Conventions
+ *  - Every call returns an int status (R3D_OK on success); the message of the
+ *    last failure is r3d_last_error(ctx).  Nothing calls exit().
+ *  - A context owns all of its device memory and one CUDA stream.  A context
+ *    is not thread-safe; distinct contexts may be used from distinct threads.
+ *  - Grids are x-fastest: index = x + nx*(y + ny*z); per-site arrays are
+ *    [site][z][y][x].  Host arrays are always FP64, whatever the precision.
+ *  - Plain pointers and sizes only; no C++ or framework types.
+ */
+#ifndef RISM3D_B200_H
+#define RISM3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define R3D_OK 0
+#define R3D_EINVAL 1   /* bad argument or unsupported problem */
+#define R3D_EIO 2      /* file could not be read or written */
+#define R3D_ECUDA 3    /* CUDA runtime error */
+#define R3D_ENOMEM 4   /* device allocation failed */
+#define R3D_ESTATE 5   /* call out of order (e.g. iterate before initialize) */
+#define R3D_EBUDGET 6  /* problem does not fit the context's HBM budget */
+
+/* precision */
+#define R3D_FP64 0   /* everything in FP64 (parity path) */
+#define R3D_MIXED 1  /* FP32 grids/FFT/closure/OZ; FP64 reductions and solves */
+
+/* closures */
+#define R3D_KH 0
+#define R3D_HNC 1
+#define R3D_PSE 2 /* PSE-n, n given separately; PSE-1 == KH */
+
+/* mixers */
+#define R3D_MIX_AN2 0 /* the reference's modified Anderson (anderson.cu) */
+#define R3D_MIX_ANM 1 /* Anderson with history depth m and fixed damping */
+
+/* solve outcome (iterate.cu:73-82) */
+#define R3D_CONVERGED 0
+#define R3D_MAXSTEP 1
+#define R3D_DIVERGED 2
+
+/* grids for r3d_get_grid */
+#define R3D_GRID_U 0   /* beta*u_v(r), per site                        */
+#define R3D_GRID_T 1   /* t_v(r) = h - c, per site                      */
+#define R3D_GRID_G 2   /* g_v(r), per site                              */
+#define R3D_GRID_H 3   /* h_v(r), per site                              */
+#define R3D_GRID_R 4   /* residual h + 1 - g of the last evaluation     */
+#define R3D_GRID_FR 5  /* beta*phi_L(r) (one grid)                      */
+#define R3D_GRID_FK 6  /* beta*phi_L(k) on the stored half spectrum,
+                          complex interleaved [z][y][p], k_x index 2p   */
+
+typedef struct r3d_ctx r3d_ctx;
+
+typedef struct r3d_opts {
+  int device;                    /* CUDA device ordinal                      */
+  int precision;                 /* R3D_FP64 or R3D_MIXED                    */
+  unsigned long long hbm_budget; /* bytes this context may hold; 0 = any     */
+  int verbose;                   /* 1: print " Step = i Reside = rms"        */
+} r3d_opts;
+
+/* Context lifetime (replaces `new RISM3D` / delete, main.cu:14). */
+int r3d_create(const r3d_opts *opts, r3d_ctx **out);
+int r3d_destroy(r3d_ctx *ctx);
+const char *r3d_last_error(const r3d_ctx *ctx); /* ctx may be NULL */
+
+/* RISM3D::set_ad (set_ad.cu:5-8): -l (adswitch 1) / -e (adswitch 2). */
+int r3d_set_ad(r3d_ctx *ctx, double lambda, int adswitch);
+
+/* RISM3D::read_input (read_input.cu:21-97) with Solute::centering/zero
+ * (solute.cu:18-54) and set_fname (set_fname.cu:5-12).  structure may be
+ * NULL (atoms follow in the .inp).  Reads the control deck only. */
+int r3d_load_inp(r3d_ctx *ctx, const char *inp, const char *structure,
+                 int centering, int q0);
+
+/* Solvent::read (solvent_read.cc:10-94).  path NULL: the file named in the
+ * .inp, opened relative to the working directory, else next to the .inp. */
+int r3d_load_xvk(r3d_ctx *ctx, const char *path);
+
+/* In-memory problem (alternative to the two loaders). Arrays are copied. */
+typedef struct r3d_problem {
+  int grid[3];
+  double box[3];
+  int closure, pse_n;
+  double convergence;
+  int maxstep;
+  int count;       /* AN2 Picard warm-up steps */
+  double m, mp;    /* AN2 damping and newest-slot bias */
+  int nu;          /* solute atoms */
+  const double *sig, *eps, *q; /* [nu]; eps in J/mol, q in e */
+  const double *xyz;           /* [nu][3], Angstrom (used as given) */
+  int natv;        /* unique solvent sites */
+  const double *sigv, *epsv, *qv, *rhov; /* [natv]; rhov in 1/A^3 */
+  double temper, xt;           /* K, 1/Pa */
+  int ntab;
+  double dr;                   /* table spacing: k_i = (i+1) pi / (dr ntab) */
+  const double *xvv;           /* [natv][natv][ntab] */
+} r3d_problem;
+int r3d_set_problem(r3d_ctx *ctx, const r3d_problem *p);
+
+/* Extensions of the input surface (the .inp keeps the reference's format). */
+int r3d_set_closure(r3d_ctx *ctx, int closure, int pse_n);
+int r3d_set_mixer(r3d_ctx *ctx, int mixer, int history, double damping);
+int r3d_set_control(r3d_ctx *ctx, double convergence, int maxstep);
+
+/* RISM3D::initialize after read_input (initialize.cu:4-44): k shells and
+ * chi (initialize_g.cu, solvent_spline.cu), potentials (cal_potential.cu,
+ * cal_LJ.cu, cal_Coulomb.cu) and t0 (initialize_tuv.cu). */
+int r3d_initialize(r3d_ctx *ctx);
+
+/* RISM3D::calculate + cal_rms (calculate.cu:4-65, cal_rms.cu:14-26):
+ * one Picard evaluation; *rms receives sqrt(sum R^2 / (N n)). */
+int r3d_calculate(r3d_ctx *ctx, double *rms);
+
+/* AN2::calculate (anderson.cu:43-78) or the history-m mixer: one update of t
+ * from the last evaluation. */
+int r3d_anderson(r3d_ctx *ctx);
+
+/* RISM3D::iterate (iterate.cu:6-107): evaluate, test, mix until converged,
+ * diverged or maxstep.  status: R3D_CONVERGED / R3D_MAXSTEP / R3D_DIVERGED. */
+int r3d_iterate(r3d_ctx *ctx, int *steps, double *rms, int *status);
+
+/* RISM3D::output 'm' branch (output.cu:23-46): xmu[2*natv] (closure SFE per
+ * site, then GF per site), xmu2[natv] (HNC functional on a KH solution),
+ * pmv (m^3/mol), pressure (P/kT) -- the values cal_exchem, cal_pmv and
+ * cal_pressure return, before output_xmu's unit conversion. */
+int r3d_thermo(r3d_ctx *ctx, double *xmu, double *xmu2, double *pmv,
+               double *pressure);
+
+/* output_xmu (output_xmu.cu:7-82). path NULL: <stem>.xmu (or .xmu0 for -z). */
+int r3d_write_xmu(r3d_ctx *ctx, const char *path);
+
+/* Device -> host copy of a grid (FP64), see R3D_GRID_*. */
+int r3d_get_grid(r3d_ctx *ctx, int which, double *host);
+/* Host -> device t (FP64 [natv][N]); e.g. a restart. */
+int r3d_set_t(r3d_ctx *ctx, const double *host);
+
+/* Problem facts. */
+int r3d_info(const r3d_ctx *ctx, int *grid3, int *natv, long long *ngrid,
+             int *nu);
+/* Device bytes the context holds (after initialize) or will need (before). */
+int r3d_device_bytes(const r3d_ctx *ctx, unsigned long long *bytes);
+/* CUDA-event time of the last r3d_iterate loop, ms per iteration, and the
+ * number of kernels one iteration launches. */
+int r3d_iter_timing(const r3d_ctx *ctx, double *ms_per_iter,
+                    int *kernels_per_iter);
+
+/* FFT3D::execute (fft3d.cu:72-78), stand-alone test seam: the reference's
+ * half-shifted 3D transform F(k) = dv sum_r f(r) e^{-i k.r} of a real grid.
+ * dir -1: in = real [N], out = complex interleaved half spectrum [z][y][p]
+ *         (k_x index 2p of the full grid, all k_y, k_z);
+ * dir +1: in = that half spectrum, out = real f(r) = (1/V) sum_k F(k) e^{ik.r}.
+ * Runs on `device` with `precision`; allocates and frees its own buffers. */
+int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
+              const double *box, int dir, const double *in, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RISM3D_B200_H */

@@ -1,0 +1,132 @@
+"""Parity of the CUDA solver (through its C-ABI) with the CPU oracle and the
+reference's own outputs.  FP64 tolerances follow the parity bar: g within
+1e-8 relative, excess chemical potential within 1e-6 kcal/mol; the mixed
+(FP32-grid) path: mu_ex within 0.01 kcal/mol, PMV within 0.1 A^3."""
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD_REF = os.path.join(os.path.dirname(__file__), "golden", "ref")
+KCAL = 4184.0
+A3_PER_LMOL = 1e-27 * 6.02214076e23 * 1e3  # 1 A^3 per molecule in L/mol
+
+
+@pytest.fixture(scope="module")
+def R():
+    import rism3d
+    return rism3d
+
+
+def _xmu_numbers(text):
+    return [float(x) for x in re.findall(r"=\s*(-?[0-9.]+(?:e[-+]?\d+)?)", text)]
+
+
+def _meta(case):
+    return json.load(open(os.path.join(GOLD_REF, case + ".json")))
+
+
+@pytest.mark.parametrize("shape", [(8, 12, 16), (16, 8, 20), (12, 12, 12), (24, 10, 32)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("mixed", 2e-5)])
+def test_fft_forward_matches_oracle(R, shape, prec, tol):
+    """The closed-form shifted DFT for every even n; the oracle (= the
+    reference's fft3d.cu) agrees with it only when every n = 0 mod 4, since
+    the reference drops the constant phase e^{-i pi n/2} of each axis."""
+    from test_oracle import _direct_shifted_dft
+    rng = np.random.default_rng(5)
+    nz, ny, nx = shape
+    box = (nx * 0.5, ny * 0.45, nz * 0.55)
+    f = rng.standard_normal(shape)
+    ref = _direct_shifted_dft(f, box)[:, :, 0::2]  # kept k_x indices 2p
+    if all(n % 4 == 0 for n in shape):
+        np.testing.assert_allclose(O.fft3d(f, box, -1)[:, :, 0::2], ref, atol=1e-11 * np.abs(ref).max())
+    got = R.fft3d(f, box, -1, precision=prec)
+    scale = np.abs(ref).max()
+    np.testing.assert_allclose(got, ref, atol=tol * scale)
+    back = R.fft3d(got, box, +1, precision=prec)
+    np.testing.assert_allclose(back, f, atol=tol * 10 * np.abs(f).max())
+
+
+def _solver(R, inp, xvk, prec="fp64"):
+    s = R.RISM3D(precision=prec)
+    s.initialize(inp, xvk=xvk)
+    return s
+
+
+def test_potentials_match_oracle(R, refcase):
+    inp, xvk = refcase("s64kh")
+    o = O.Oracle(inp, xvk=xvk)
+    o.initialize()
+    s = _solver(R, inp, xvk)
+    u_ref, u = o.get("u"), s.get("u")
+    np.testing.assert_allclose(u, u_ref, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(s.get("fr"), o.get("fr"), rtol=1e-12, atol=1e-13)
+    fk_ref = o.get("fk")[:, :, 0::2]
+    np.testing.assert_allclose(s.get("fk"), fk_ref, rtol=1e-9, atol=1e-9 * np.abs(fk_ref).max())
+    np.testing.assert_allclose(s.get("t"), o.get("t"), rtol=1e-12, atol=1e-13)
+
+
+def test_one_evaluation_matches_oracle(R, refcase):
+    inp, xvk = refcase("s64nacl")
+    o = O.Oracle(inp, xvk=xvk)
+    o.initialize()
+    s = _solver(R, inp, xvk)
+    for _ in range(3):
+        r_ref = o.calculate()
+        r = s.calculate()
+        assert r == pytest.approx(r_ref, rel=1e-10)
+        np.testing.assert_allclose(s.get("R"), o.get("R"), atol=1e-10)
+        np.testing.assert_allclose(s.get("g"), o.get("g"), rtol=1e-10, atol=1e-12)
+        o.mix()
+        s.anderson()
+        np.testing.assert_allclose(s.get("t"), o.get("t"), atol=1e-10)
+
+
+@pytest.mark.parametrize("case", ["s64kh", "s_rect", "c1", "s64nacl", "test1"])
+def test_fp64_solve_matches_reference(R, refcase, case, tmp_path):
+    inp, xvk = refcase(case)
+    meta = _meta(case)
+    s = _solver(R, inp, xvk)
+    steps, rms, status = s.iterate()
+    assert status == "converged"
+    assert abs(steps - meta["steps"]) <= 1
+    out = tmp_path / "gpu.xmu"
+    s.output(str(out))
+    ref = _xmu_numbers(open(os.path.join(GOLD_REF, case + ".xmu")).read())
+    got = _xmu_numbers(out.read_text())
+    assert len(got) == len(ref)
+    # SFE terms in J/mol: 1e-6 kcal/mol; PMV in L/mol; pressure is input-only
+    np.testing.assert_allclose(got, ref, rtol=1e-9, atol=1e-6 * KCAL)
+    gp = os.path.join(GOLD_REF, case + "_guv.npz")
+    if os.path.exists(gp):
+        g = np.load(gp)
+        mine = s.get("g").reshape(len(g["sum"]), -1)
+        np.testing.assert_allclose(mine[:, g["idx"]], g["g"], rtol=1e-8, atol=1e-9)
+
+
+def test_divergence_detected(R, refcase):
+    inp, xvk = refcase("s64hnc")
+    s = _solver(R, inp, xvk)
+    steps, rms, status = s.iterate()
+    assert status == "diverged" and steps == 2
+
+
+@pytest.mark.parametrize("case", ["s64kh", "c1", "s64nacl"])
+def test_mixed_precision_within_tolerance(R, refcase, case, tmp_path):
+    inp, xvk = refcase(case)
+    s = _solver(R, inp, xvk, prec="mixed")
+    steps, rms, status = s.iterate()
+    assert status == "converged"
+    out = tmp_path / "mixed.xmu"
+    s.output(str(out))
+    ref = _xmu_numbers(open(os.path.join(GOLD_REF, case + ".xmu")).read())
+    got = _xmu_numbers(out.read_text())
+    sfe = [i for i, l in enumerate(open(os.path.join(GOLD_REF, case + ".xmu")).read().split("\n"))]
+    # first number is SFE_SC (total), PMV is the third-to-last
+    assert abs(got[0] - ref[0]) <= 0.01 * KCAL
+    assert abs(got[-3] - ref[-3]) <= 0.1 * A3_PER_LMOL

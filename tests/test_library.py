@@ -1,0 +1,77 @@
+"""CPU checks of the C-ABI library: it loads, exports every entry point the
+header declares, and its host-side input surface works without a GPU."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rism3d_b200.h")
+
+
+@pytest.fixture(scope="module")
+def R():
+    import rism3d
+    return rism3d
+
+
+def test_header_symbols_exported(R):
+    decl = re.findall(r"^\w[\w\s\*]*?\b(r3d_\w+)\s*\(", open(HEADER).read(), re.M)
+    assert decl, "no declarations found"
+    assert sorted(set(decl)) == sorted(set(R.EXPORTS))
+    for name in decl:
+        assert hasattr(R.lib, name), name
+
+
+def test_host_only_context_parses_decks(R, refcase):
+    inp, xvk = refcase("c1")
+    with R.RISM3D(device=-1) as s:
+        s.load(inp, xvk=xvk)
+        inf = s.info()
+        assert inf["grid"] == (64, 64, 64) and inf["natv"] == 2 and inf["nu"] == 20
+        assert s.device_bytes() > 64 ** 3 * 8 * 10
+        with pytest.raises(R.R3DError, match="ESTATE"):
+            s.initialize()
+
+
+def test_split_control_and_structure(R, solvents, tmp_path):
+    from conftest import unpack
+    d = str(tmp_path)
+    c = unpack("test1_c", d)
+    st = unpack("test1_s", d)
+    with R.RISM3D(device=-1) as s:
+        s.load(c, structure=st, xvk=solvents["h2o_vv"])
+        assert s.info()["nu"] == 3 and s.info()["grid"] == (128, 128, 128)
+
+
+@pytest.mark.parametrize("name,nu,grid", [("test2.inp", 754, (256,) * 3),
+                                          ("cygnus_test2.inp.gz", 12877, (512,) * 3)])
+def test_shipped_decks_parse(R, solvents, tmp_path, name, nu, grid):
+    from conftest import unpack
+    p = unpack(name, str(tmp_path))
+    with R.RISM3D(device=-1) as s:
+        s.load(p, xvk=solvents["naclaq_vv"])
+        inf = s.info()
+        assert inf["nu"] == nu and inf["grid"] == grid
+
+
+def test_bad_inputs_are_errors_not_exits(R, tmp_path, solvents):
+    bad = tmp_path / "bad.inp"
+    bad.write_text(" m 0 19990101\n KH\n h2o_vv.xvk\n")
+    with R.RISM3D(device=-1) as s:
+        with pytest.raises(R.R3DError, match="old version"):
+            s.load(str(bad), xvk=solvents["h2o_vv"])
+    bad.write_text(" m 0 20220301\n XYZ\n h2o_vv.xvk\n")
+    with R.RISM3D(device=-1) as s:
+        with pytest.raises(R.R3DError, match="closure"):
+            s.load(str(bad), xvk=solvents["h2o_vv"])
+    trunc = tmp_path / "trunc.xvk"
+    trunc.write_text("".join(open(solvents["h2o_vv"]).readlines()[:20]))
+    good = os.path.join(os.path.dirname(__file__), "golden", "test1.inp")
+    with R.RISM3D(device=-1) as s:
+        with pytest.raises(R.R3DError, match="truncated"):
+            s.load(good, xvk=str(trunc))
+    with R.RISM3D(device=-1) as s:
+        with pytest.raises(R.R3DError, match="EIO"):
+            s.load(str(tmp_path / "missing.inp"))
