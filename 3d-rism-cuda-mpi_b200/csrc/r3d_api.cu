@@ -131,6 +131,7 @@ struct r3d_ctx {
   cudaGraphExec_t gexec = nullptr;
   double ms_per_iter = 0;
   int kernels_per_iter = 0;
+  unsigned long long h2d = 0, d2h = 0;  // bytes copied each way
 };
 
 // ------------------------------------------------------------------ utils
@@ -146,6 +147,18 @@ static int fail(r3d_ctx *c, int code, const std::string &m) {
       return fail(c, R3D_ECUDA, std::string(#call) + ": " +               \
                                     cudaGetErrorString(e_));              \
   } while (0)
+
+// Host<->device copies on the context's stream, counted for r3d_transfer_bytes.
+static cudaError_t copy_h2d(r3d_ctx *c, void *dst, const void *src, size_t n,
+                            cudaStream_t s) {
+  c->h2d += n;
+  return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s);
+}
+static cudaError_t copy_d2h(r3d_ctx *c, void *dst, const void *src, size_t n,
+                            cudaStream_t s) {
+  c->d2h += n;
+  return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s);
+}
 
 static int dalloc(r3d_ctx *c, void **p, size_t bytes) {
   if (bytes == 0) bytes = 16;
@@ -338,7 +351,8 @@ extern "C" int r3d_set_closure(r3d_ctx *c, int clos, int pse_n) {
   if (c->initialized) {
     c->desc.clos = c->prob.clos;
     c->desc.pse_n = c->prob.pse_n;
-    CK(cudaMemcpy(c->ddesc, &c->desc, sizeof(Desc), cudaMemcpyHostToDevice));
+    CK(copy_h2d(c, c->ddesc, &c->desc, sizeof(Desc), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   }
   return R3D_OK;
 }
@@ -462,8 +476,8 @@ static int refresh(r3d_ctx *c, bool zero) {
   dr.ctl = ctl;
   int pf[8] = {0, g.tiles_x, 0, g.tiles_y, 0, g.tiles_z, 0, g.ix_ctas};
   CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
-  CK(cudaMemcpyAsync(dd, &dr, sizeof(Desc), cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(pre, pf, sizeof(pf), cudaMemcpyHostToDevice, s));
+  CK(copy_h2d(c, dd, &dr, sizeof(Desc), s));
+  CK(copy_h2d(c, pre, pf, sizeof(pf), s));
   kernels_set_smem(true, kSmemMax);
   launch_fwd_x<P64>(Batch{dd, pre, 1}, g.tiles_x, g.smx, s, 0, c64);
   launch_fft_y<P64>(Batch{dd, pre + 2, 1}, g.tiles_y, g.smy, s, -1, 0);
@@ -576,11 +590,11 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
       chi64[i] = st.chi[i] * sc;
       chi[i] = (R)chi64[i];
     }
-    CK(cudaMemcpyAsync(c->chi, chi.data(), chi.size() * sizeof(R), cudaMemcpyHostToDevice, s));
+    CK(copy_h2d(c, c->chi, chi.data(), chi.size() * sizeof(R), s));
     if (c->fp64)
       c->chi64 = c->chi;
     else
-      CK(cudaMemcpyAsync(c->chi64, chi64.data(), chi64.size() * 8, cudaMemcpyHostToDevice, s));
+      CK(copy_h2d(c, c->chi64, chi64.data(), chi64.size() * 8, s));
     CK(cudaStreamSynchronize(s));
   }
   // shell index of every half-spectrum point
@@ -588,8 +602,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     uint32_t *dtuple = nullptr;
     if (!st.cubic) {
       if ((rc = dalloc(c, (void **)&dtuple, st.tuple_idx.size() * 4))) return rc;
-      CK(cudaMemcpyAsync(dtuple, st.tuple_idx.data(), st.tuple_idx.size() * 4,
-                         cudaMemcpyHostToDevice, s));
+      CK(copy_h2d(c, dtuple, st.tuple_idx.data(), st.tuple_idx.size() * 4, s));
     }
     launch_kidx(d, dtuple, st.cubic ? 1 : 0, s);
     CK(cudaGetLastError());
@@ -615,15 +628,13 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     double *dx = dat, *dy = dat + natom, *dz = dat + 2 * natom, *dq = dat + 3 * natom;
     double *dsig = dat + 4 * natom, *deps = dsig + (size_t)n * natom;
     if (nu > 0) {
-      CK(cudaMemcpyAsync(dx, ax.data(), nu * 8, cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(dy, ay.data(), nu * 8, cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(dz, az.data(), nu * 8, cudaMemcpyHostToDevice, s));
-      CK(cudaMemcpyAsync(dq, p.q.data(), nu * 8, cudaMemcpyHostToDevice, s));
+      CK(copy_h2d(c, dx, ax.data(), nu * 8, s));
+      CK(copy_h2d(c, dy, ay.data(), nu * 8, s));
+      CK(copy_h2d(c, dz, az.data(), nu * 8, s));
+      CK(copy_h2d(c, dq, p.q.data(), nu * 8, s));
       for (int v = 0; v < n; ++v) {
-        CK(cudaMemcpyAsync(dsig + (size_t)v * natom, isig2.data() + (size_t)v * nu, nu * 8,
-                           cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(deps + (size_t)v * natom, eps4.data() + (size_t)v * nu, nu * 8,
-                           cudaMemcpyHostToDevice, s));
+        CK(copy_h2d(c, dsig + (size_t)v * natom, isig2.data() + (size_t)v * nu, nu * 8, s));
+        CK(copy_h2d(c, deps + (size_t)v * natom, eps4.data() + (size_t)v * nu, nu * 8, s));
       }
     }
     AtomTab at{dx, dy, dz, dq, dsig, deps, nu};
@@ -666,11 +677,11 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     h.maxstep = p.maxstep;
     h.tol = p.convergence;
     h.count_left = p.count;
-    CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(c->ddesc, &d, sizeof(Desc), cudaMemcpyHostToDevice, s));
+    CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
+    CK(copy_h2d(c, c->ddesc, &d, sizeof(Desc), s));
     int pre[16] = {0, c->tiles_x, 0, c->tiles_y, 0, c->tiles_z, 0, c->ix_ctas,
                    0, c->mix_ctas, c->ix_ctas, c->mix_ctas, 0, 0, 0, 0};
-    CK(cudaMemcpyAsync(c->dprefix, pre, sizeof(pre), cudaMemcpyHostToDevice, s));
+    CK(copy_h2d(c, c->dprefix, pre, sizeof(pre), s));
     CK(cudaStreamSynchronize(s));
   }
   // the attribute is a per-function limit shared by every context: always
@@ -756,13 +767,13 @@ static void enqueue(r3d_ctx *c, int stage) {
 }
 
 static int read_ctl(r3d_ctx *c, Ctl &h) {
-  CK(cudaMemcpyAsync(&h, c->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, c->stream));
+  CK(copy_d2h(c, &h, c->ctl, sizeof(Ctl), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return R3D_OK;
 }
 static int set_running(r3d_ctx *c) {
   int st = RUNNING;
-  CK(cudaMemcpyAsync(&c->ctl->status, &st, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(copy_h2d(c, &c->ctl->status, &st, sizeof(int), c->stream));
   return R3D_OK;
 }
 
@@ -798,6 +809,173 @@ extern "C" int r3d_anderson(r3d_ctx *c) {
   return R3D_OK;
 }
 
+// One iteration captured once as a CUDA graph (pointers never change).
+static int ensure_graph(r3d_ctx *c) {
+  if (c->gexec) return R3D_OK;
+  cudaStream_t s = c->stream;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  if (c->fp64)
+    enqueue<P64>(c, 0);
+  else
+    enqueue<PMix>(c, 0);
+  CK(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(&c->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return fail(c, R3D_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return R3D_OK;
+}
+
+static int reset_mixer(r3d_ctx *c) {
+  Ctl h{};
+  h.status = RUNNING;
+  h.maxstep = c->prob.maxstep;
+  h.tol = c->prob.convergence;
+  h.count_left = c->prob.count;
+  CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return R3D_OK;
+}
+
+extern "C" int r3d_step(r3d_ctx *c, int nsteps, double *ms) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "step before initialize");
+  if (nsteps < 0) return fail(c, R3D_EINVAL, "nsteps < 0");
+  CK(cudaSetDevice(c->opts.device));
+  int rc = ensure_graph(c);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(c->gexec, c->stream));
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms) *ms = t;
+  return R3D_OK;
+}
+
+template <typename P>
+static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
+                         double *bytes, int *nk) {
+  using R = typename P::R;
+  using T = typename P::T;
+  const Desc &d = c->desc;
+  cudaStream_t s = c->stream;
+  const int *pf = c->dprefix;
+  const double n = d.n, N = (double)d.N, rs = sizeof(R), ts = sizeof(T);
+  Batch bx{c->ddesc, pf + 0, 1}, by{c->ddesc, pf + 2, 1}, bz{c->ddesc, pf + 4, 1},
+      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1};
+  // keep t: the kernels below run out of sequence and overwrite it
+  void *tsave = nullptr;
+  const size_t tb = (size_t)d.n * d.N * sizeof(T);
+  CK(cudaMalloc(&tsave, tb));
+  CK(cudaMemcpyAsync(tsave, c->t, tb, cudaMemcpyDeviceToDevice, s));
+  Ctl h;
+  int rc = read_ctl(c, h);
+  if (rc) return rc;
+  const bool dots = c->mixer == MIX_AN2 && h.count_left <= 0;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int k = 0;
+  auto timed = [&](const char *name, double b, auto &&launch) -> int {
+    launch();  // warm
+    CK(cudaEventRecord(e0, s));
+    for (int i = 0; i < reps; ++i) launch();
+    CK(cudaEventRecord(e1, s));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (k < 16) {
+      ms[k] = t / reps;
+      bytes[k] = b;
+      names += (k ? "," : "") + std::string(name);
+    }
+    ++k;
+    return R3D_OK;
+  };
+  const double cref = d.cref ? rs : 0.0;
+  timed("fwd_x", n * N * (ts + rs + cref + rs),
+        [&] { launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 1, nullptr); });
+  timed("fft_y_fwd", n * N * 2 * rs,
+        [&] { launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 1); });
+  timed("zoz", n * N * 2 * rs + (double)d.Nh * 4,
+        [&] { launch_zoz<P>(bz, c->tiles_z, c->smz, s, 2, 1); });
+  timed("fft_y_inv", n * N * 2 * rs,
+        [&] { launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 1); });
+  timed("inv_x", n * N * (rs + ts + rs + rs + rs + (dots ? 2 * rs : 0)),
+        [&] { launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 1, nullptr, c->ix_per); });
+  if (c->mixer == MIX_AN2) {
+    timed("reduce", (double)c->ix_ctas * kPartials * 8,
+          [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
+    const bool picard = h.count_left > 0;
+    timed("mix_an2", picard ? n * N * (3 * ts + 2 * rs) : n * N * (5 * ts + 4 * rs),
+          [&] { launch_mix_an2<P>(bmx, c->mix_ctas, s); });
+  } else {
+    timed("anm_dots", n * N * rs * (h.hcount + 1),
+          [&] { launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 0); });
+    timed("reduce", (double)c->ix_ctas * kPartials * 8,
+          [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
+    timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 1); });
+    const int m = std::min(h.hcount, c->history);
+    timed("mix_anm", n * N * (rs + ts + m * ts + rs + ts + ts),
+          [&] { launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 2); });
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(c->t, tsave, tb, cudaMemcpyDeviceToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  cudaFree(tsave);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *nk = std::min(k, 16);
+  return reset_mixer(c);
+}
+
+extern "C" int r3d_profile_kernels(r3d_ctx *c, int reps, char *names, int len,
+                                   double *ms, double *bytes, int *nk) {
+  if (!c || !ms || !bytes || !nk || reps < 1) return fail(c, R3D_EINVAL, "bad arguments");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "profile before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  std::string nm;
+  int rc = c->fp64 ? profile_typed<P64>(c, reps, nm, ms, bytes, nk)
+                   : profile_typed<PMix>(c, reps, nm, ms, bytes, nk);
+  if (names && len > 0) {
+    std::strncpy(names, nm.c_str(), (size_t)len - 1);
+    names[len - 1] = 0;
+  }
+  return rc;
+}
+
+extern "C" int r3d_status(r3d_ctx *c, int *steps, double *rms, int *status) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "status before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  Ctl h;
+  int rc = read_ctl(c, h);
+  if (rc) return rc;
+  if (steps) *steps = h.step;
+  if (rms) *rms = h.rms;
+  if (status)
+    *status = h.status == RUNNING ? -1
+              : h.status == CONVERGED ? R3D_CONVERGED
+              : h.status == DIVERGED ? R3D_DIVERGED : R3D_MAXSTEP;
+  return R3D_OK;
+}
+
+extern "C" int r3d_transfer_bytes(const r3d_ctx *c, unsigned long long *h2d,
+                                  unsigned long long *d2h) {
+  if (!c) return R3D_EINVAL;
+  if (h2d) *h2d = c->h2d;
+  if (d2h) *d2h = c->d2h;
+  return R3D_OK;
+}
+
 extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
   if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
   if (!c->initialized) return fail(c, R3D_ESTATE, "iterate before initialize");
@@ -810,21 +988,10 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
     h.maxstep = c->prob.maxstep;
     h.tol = c->prob.convergence;
     h.count_left = c->prob.count;
-    CK(cudaMemcpyAsync(c->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
   }
-  if (!c->gexec) {
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    if (c->fp64)
-      enqueue<P64>(c, 0);
-    else
-      enqueue<PMix>(c, 0);
-    CK(cudaStreamEndCapture(s, &g));
-    cudaError_t e = cudaGraphInstantiate(&c->gexec, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess)
-      return fail(c, R3D_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-  }
+  int grc = ensure_graph(c);
+  if (grc) return grc;
   if (c->opts.verbose) std::printf("relaxing 3D UV RISM:\n");
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -846,7 +1013,8 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
     }
     if (c->opts.verbose && h.step > printed) {
       log.resize(h.step);
-      CK(cudaMemcpy(log.data(), c->desc.rmslog, sizeof(double) * h.step, cudaMemcpyDeviceToHost));
+      CK(copy_d2h(c, log.data(), c->desc.rmslog, sizeof(double) * h.step, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
       for (int i = printed; i < h.step; ++i)
         std::printf(" Step = %d Reside = %g\n", i + 1, log[i]);
       printed = h.step;
@@ -919,7 +1087,7 @@ extern "C" int r3d_thermo(r3d_ctx *c, double *xmu, double *xmu2, double *pmv,
     launch_thermo<PMix>(d, tg, c->scratch, ctas, c->stream);
   CK(cudaGetLastError());
   std::vector<double> part((size_t)ctas * d.n * 4);
-  CK(cudaMemcpyAsync(part.data(), c->scratch, part.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  CK(copy_d2h(c, part.data(), c->scratch, part.size() * 8, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   const Problem &p = c->prob;
   const double dv = p.box[0] * p.box[1] * p.box[2] / (double)d.N;
@@ -1013,7 +1181,7 @@ extern "C" int r3d_get_grid(r3d_ctx *c, int which, double *host) {
       return fail(c, R3D_EINVAL, "unknown grid");
   }
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(host, c->scratch, count * 8, cudaMemcpyDeviceToHost, s));
+  CK(copy_d2h(c, host, c->scratch, count * 8, s));
   CK(cudaStreamSynchronize(s));
   if (which == R3D_GRID_FK) {  // transform units -> physical beta phi_L(k)
     const Problem &p = c->prob;
@@ -1038,7 +1206,7 @@ extern "C" int r3d_set_t(r3d_ctx *c, const double *host) {
   const long long niv = (long long)c->desc.n * c->desc.N;
   int rc = ensure_scratch(c, niv * 8);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(c->scratch, host, niv * 8, cudaMemcpyHostToDevice, c->stream));
+  CK(copy_h2d(c, c->scratch, host, niv * 8, c->stream));
   if (c->fp64)
     launch_set_short<P64>(c->desc, c->scratch, c->t, c->stream);
   else
@@ -1100,9 +1268,9 @@ static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int 
   CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
   d.w = w;
   d.ctl = (Ctl *)ctl;
-  CK(cudaMemcpyAsync(ddesc, &d, sizeof(Desc), cudaMemcpyHostToDevice, s));
+  CK(copy_h2d(c, ddesc, &d, sizeof(Desc), s));
   int pf[16] = {0, c->tiles_x, 0, c->tiles_y, 0, c->tiles_z, 0, c->ix_ctas};
-  CK(cudaMemcpyAsync(pre, pf, sizeof(pf), cudaMemcpyHostToDevice, s));
+  CK(copy_h2d(c, pre, pf, sizeof(pf), s));
   const int *dp = (const int *)pre;
   Batch bx{(Desc *)ddesc, dp, 1}, by{(Desc *)ddesc, dp + 2, 1}, bz{(Desc *)ddesc, dp + 4, 1},
       bix{(Desc *)ddesc, dp + 6, 1};
@@ -1111,14 +1279,14 @@ static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int 
   const int par0 = ((nx + ny + nz) / 2) & 1;
   std::vector<double> tmp(std::max(N, 2 * Nh));
   if (dir < 0) {
-    CK(cudaMemcpyAsync(hbuf, in, N * 8, cudaMemcpyHostToDevice, s));
+    CK(copy_h2d(c, hbuf, in, N * 8, s));
     launch_from_double<P>((const double *)hbuf, src, N, 0, s);
     launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 0, src);
     launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 0);
     launch_zoz<P>(bz, c->tiles_z, c->smz, s, 0, 0);
     launch_to_double<P>(w, (double *)hbuf, 2 * Nh, 0, s);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, hbuf, 2 * Nh * 8, cudaMemcpyDeviceToHost, s));
+    CK(copy_d2h(c, out, hbuf, 2 * Nh * 8, s));
     CK(cudaStreamSynchronize(s));
     for (long long i = 0; i < Nh; ++i) {
       int pp = (int)(i % d.hx), y = (int)((i / d.hx) % ny), z = (int)(i / ((long long)d.hx * ny));
@@ -1136,14 +1304,14 @@ static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int 
       tmp[2 * i] = -b * sg / dv;
       tmp[2 * i + 1] = a * sg / dv;
     }
-    CK(cudaMemcpyAsync(hbuf, tmp.data(), 2 * Nh * 8, cudaMemcpyHostToDevice, s));
+    CK(copy_h2d(c, hbuf, tmp.data(), 2 * Nh * 8, s));
     launch_from_double<P>((const double *)hbuf, w, 2 * Nh, 0, s);
     launch_zoz<P>(bz, c->tiles_z, c->smz, s, 1, 0);
     launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 0);
     launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 0, src, c->ix_per);
     launch_to_double<P>(src, (double *)hbuf, N, 0, s);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, hbuf, N * 8, cudaMemcpyDeviceToHost, s));
+    CK(copy_d2h(c, out, hbuf, N * 8, s));
     CK(cudaStreamSynchronize(s));
     const double sc = 2.0 / (double)N;
     for (long long i = 0; i < N; ++i) out[i] *= sc;

@@ -30,7 +30,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_load_xvk", "r3d_set_problem", "r3d_set_closure", "r3d_set_mixer",
            "r3d_set_control", "r3d_initialize", "r3d_calculate", "r3d_anderson",
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
-           "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_fft3d"]
+           "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_step",
+           "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d"]
 
 
 class Opts(ctypes.Structure):
@@ -65,6 +66,11 @@ def _load():
         "r3d_info": [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong), ip],
         "r3d_device_bytes": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_iter_timing": [vp, dp, ip],
+        "r3d_step": [vp, ci, dp],
+        "r3d_profile_kernels": [vp, ci, ctypes.c_char_p, ci, dp, dp, ip],
+        "r3d_status": [vp, ip, dp, ip],
+        "r3d_transfer_bytes": [vp, ctypes.POINTER(ctypes.c_ulonglong),
+                               ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
     }
     for name, args in sig.items():
@@ -176,6 +182,34 @@ class RISM3D:
         ms, k = ctypes.c_double(), ctypes.c_int()
         self._check(lib.r3d_iter_timing(self.h, ctypes.byref(ms), ctypes.byref(k)))
         return ms.value, k.value
+
+    def step(self, nsteps):
+        """Advance exactly nsteps iterations; returns their device time (ms)."""
+        ms = ctypes.c_double()
+        self._check(lib.r3d_step(self.h, nsteps, ctypes.byref(ms)))
+        return ms.value
+
+    def profile_kernels(self, reps=10):
+        """[(kernel, ms per launch, algorithmic bytes per launch)]"""
+        names = ctypes.create_string_buffer(512)
+        ms, by = np.zeros(16), np.zeros(16)
+        nk = ctypes.c_int()
+        self._check(lib.r3d_profile_kernels(self.h, reps, names, 512, _dp(ms), _dp(by),
+                                            ctypes.byref(nk)))
+        nm = names.value.decode().split(",")
+        return [(nm[i], ms[i], by[i]) for i in range(nk.value)]
+
+    def status(self):
+        """(steps, rms, 'running'|'converged'|'maxstep'|'diverged')"""
+        st, rms, status = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        self._check(lib.r3d_status(self.h, ctypes.byref(st), ctypes.byref(rms),
+                                   ctypes.byref(status)))
+        return st.value, rms.value, STATUS.get(status.value, "running")
+
+    def transfer_bytes(self):
+        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        self._check(lib.r3d_transfer_bytes(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def thermo(self):
         n = self.info()["natv"]

@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 3D-RISM solver on the protein-sized configuration:
+
+  256^3 grid at 0.5 A (128 A cell), a seeded 2,000-atom globule (~0.05
+  atoms/A^3), 0.2 M NaCl in water (4 solvent sites), KH closure, the
+  reference's modified Anderson mixer (count 2, m 0.6, mp 0.2), RMS 1e-6.
+
+A step is one iteration of the solve (evaluate + RMS + mixing).  Printed as
+one JSON line on rank 0:
+  value        whole-job iterations/s with all state resident in HBM (each GPU
+               runs its own solve: weak scaling, no data-path collective)
+  e2e          iterations/s of complete solves through the C-ABI from host
+               files to host results (parse, upload, setup, iterate, thermo,
+               g(r) read-back), plus solves/s
+  roofline     the dominant kernel's algorithmic bytes / its CUDA-event time
+  cpu_baseline the FP64 CPU oracle on the same grid and solvent
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+                  [--impl b200|reference]
+`--impl reference` times the CPU restatement of the reference's solve (the
+reference ships no CPU path) on the host cores for the same workload.
+"""
+import argparse
+import gzip
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "3d-rism-cuda-mpi_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "ms/iter & solves/s at RMS<1e-6, mixed vs FP64, 1 B200; served p50/p99 latency"
+WORKLOAD = ("256^3 grid, 128 A cell, 2000-atom seeded globule, 0.2 M NaCl water "
+            "(4 sites), KH, AN2 (2 0.6 0.2), RMS 1e-6")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def make_deck(d, atoms=None):
+    import synthetic
+    with gzip.open(os.path.join(ROOT, "tests", "golden", "naclaq_vv.xvk.gz"), "rb") as fi, \
+            open(os.path.join(d, "naclaq_vv.xvk"), "wb") as fo:
+        shutil.copyfileobj(fi, fo)
+    if atoms is None:
+        return synthetic.config("c2", d), os.path.join(d, "naclaq_vv.xvk")
+    sol = synthetic.make_solute(2000, synthetic.SEEDS["c2"])
+    sub = {k: v[:atoms] for k, v in sol.items()}
+    p = synthetic.write_inp(os.path.join(d, "c2_sub.inp"), sub, (128.0,) * 3, (256,) * 3,
+                            "naclaq_vv.xvk")
+    return p, os.path.join(d, "naclaq_vv.xvk")
+
+
+# --------------------------------------------------------------- CPU oracle
+CPU_SAMPLE_ATOMS = 50
+CPU_SAMPLE_ITERS = 3
+
+
+def cpu_oracle_rate(iters, warm):
+    """Iterations/s of the FP64 CPU oracle on the 256^3 NaCl grid (all host
+    cores).  The per-iteration cost does not depend on the solute, so the
+    setup uses the first 50 atoms of the globule to keep it short."""
+    cores = os.cpu_count() or 1
+    code = r"""
+import sys, time, json
+sys.path.insert(0, %r)
+import oracle as O
+o = O.Oracle(%r, xvk=%r)
+o.initialize()
+for _ in range(%d):
+    o.calculate(); o.mix()
+t0 = time.perf_counter()
+for _ in range(%d):
+    o.calculate(); o.mix()
+dt = time.perf_counter() - t0
+print(json.dumps({"s_per_iter": dt / %d}))
+"""
+    with tempfile.TemporaryDirectory() as d:
+        inp, xvk = make_deck(d, atoms=CPU_SAMPLE_ATOMS)
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+        src = code % (os.path.join(ROOT, "oracle"), inp, xvk, warm, iters, iters)
+        out = subprocess.run([sys.executable, "-c", src], env=env, capture_output=True,
+                             text=True, timeout=900)
+        if out.returncode:
+            raise RuntimeError(out.stderr[-2000:])
+        s = json.loads(out.stdout.strip().splitlines()[-1])["s_per_iter"]
+    sample = (f"{iters} timed iterations (+{warm} warm-up) of the 256^3 NaCl-water solve "
+              f"(FP64 oracle, {cores} OpenMP threads; setup with a {CPU_SAMPLE_ATOMS}-atom "
+              "subset of the globule, which does not change the per-iteration cost)")
+    return 1.0 / s, cores, sample
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit())
+        mx = max(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        return json.load(open(p)).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+# -------------------------------------------------------------- GPU arm
+def run_gpu(args, rank, world, local):
+    import rism3d as R
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allmax(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    prec = args.precision
+    tmp = tempfile.mkdtemp(prefix=f"r3dbench{rank}_")
+    inp, xvk = make_deck(tmp)
+
+    # ---- end to end: one complete solve through the C-ABI ---------------
+    barrier()
+    t0 = time.perf_counter()
+    s = R.RISM3D(device=local, precision=prec)
+    s.initialize(inp, xvk=xvk)
+    steps, rms, status = s.iterate()
+    xmu_path = os.path.join(tmp, "c2.xmu")
+    s.output(xmu_path)
+    g = s.get("g")
+    e2e_s = time.perf_counter() - t0
+    h2d, d2h = s.transfer_bytes()
+    ms_loop, kpi = s.timing()
+    s.close()
+    e2e_s = allmax(e2e_s)
+    sfe_kcal = None
+    for ln in open(xmu_path):
+        if ln.startswith("SFE_SC="):
+            sfe_kcal = float(ln.split()[1]) / 4184.0
+    del g
+
+    # ---- device-resident iteration throughput --------------------------
+    s = R.RISM3D(device=local, precision=prec)
+    s.load(inp, xvk=xvk)
+    s.set_control(convergence=1e-300, maxstep=10 ** 8)
+    s.initialize()
+    s.step(args.warmup)
+    barrier()
+    with ClockSampler(local) as clk:
+        ms = s.step(args.steps)
+    ms = allmax(ms)
+    st = s.status()
+    if st[2] != "running":
+        raise RuntimeError(f"solve left the running state during timing: {st}")
+    prof = s.profile_kernels(reps=10)
+    ms_iter = ms / args.steps
+    value = world * args.steps / (ms * 1e-3)
+
+    # FP64 comparison on the same workload (a shorter timed run)
+    fp64 = None
+    if prec == "mixed" and not args.no_fp64:
+        s64 = R.RISM3D(device=local, precision="fp64")
+        s64.load(inp, xvk=xvk)
+        s64.set_control(convergence=1e-300, maxstep=10 ** 8)
+        s64.initialize()
+        s64.step(args.warmup)
+        k64 = max(10, args.steps // 4)
+        ms64 = allmax(s64.step(k64))
+        fp64 = {"ms_per_iter": ms64 / k64, "iter_per_s": world * k64 / (ms64 * 1e-3)}
+        s64.close()
+    s.close()
+
+    # dominant kernel roofline
+    name, kms, kbytes = max(prof, key=lambda x: x[1])
+    peak, peak_kind = peak_hbm()
+    achieved = kbytes / (kms * 1e-3) / 1e9
+    iter_bytes = sum(b for _, _, b in prof)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, sample = cpu_oracle_rate(CPU_SAMPLE_ITERS, 1)
+        cpu = {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_iter,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 grids+transforms, f64 state/reductions" if prec == "mixed" else "f64",
+            "data": "synthetic (seeded 2000-atom globule; shipped 0.2 M NaCl .xvk)",
+            "config": {"workload": WORKLOAD, "precision": prec, "grid": 256, "sites": 4,
+                       "atoms": 2000, "replicas": world,
+                       "l2": "inputs larger than L2 (>8 GB touched per iteration)"},
+            "ms_per_iter": ms_iter,
+            "iters_to_converge": steps, "solve_status": status, "final_rms": rms,
+            "solves_per_s": world / e2e_s, "sfe_sc_kcal_per_mol": sfe_kcal,
+            "e2e": {"value": world * steps / e2e_s, "unit": "iter/s",
+                    "h2d_bytes_per_step": h2d / max(steps, 1),
+                    "d2h_bytes_per_step": d2h / max(steps, 1),
+                    "solve_s": e2e_s, "solves_per_s": world / e2e_s},
+            "gpu_launches": kpi * args.steps,
+            "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": ncu_traffic(name), "algorithmic_bytes": kbytes,
+                         "launch_ms": kms,
+                         "iteration": {"algorithmic_bytes": iter_bytes,
+                                       "achieved_gbs": iter_bytes / (ms_iter * 1e-3) / 1e9,
+                                       "frac": iter_bytes / (ms_iter * 1e-3) / 1e9 / peak}},
+            "kernels": [{"name": n, "ms": m, "bytes": b, "gbs": b / (m * 1e-3) / 1e9}
+                        for n, m, b in prof],
+            "fp64": fp64,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    shutil.rmtree(tmp, ignore_errors=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    k = max(1, min(args.steps, CPU_SAMPLE_ITERS))
+    w = max(0, min(args.warmup, 1))
+    rate, cores, sample = cpu_oracle_rate(k, w)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate * 1.0, "unit": "iter/s",
+        "n_gpus": world, "steps": k, "warmup": w, "ms_per_step": 1e3 / rate,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 2000-atom globule; shipped 0.2 M NaCl .xvk)",
+        "config": {"workload": WORKLOAD, "precision": "fp64", "grid": 256, "sites": 4,
+                   "atoms": 2000},
+        "e2e": {"value": rate, "unit": "iter/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "note": "the reference ships no CPU implementation of the solve; this is the "
+                "project's FP64 restatement of it (oracle/), pinned to the reference's "
+                "own outputs",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

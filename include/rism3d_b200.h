@@ -154,6 +154,29 @@ int r3d_device_bytes(const r3d_ctx *ctx, unsigned long long *bytes);
 int r3d_iter_timing(const r3d_ctx *ctx, double *ms_per_iter,
                     int *kernels_per_iter);
 
+/* Advance the solve by exactly `nsteps` iterations (graph replays, no
+ * convergence polling; converged or diverged solves do no further work) and
+ * return their CUDA-event time in *ms.  No counterpart in the reference: the
+ * benchmark and batch loops use it to time iterations without host syncs. */
+int r3d_step(r3d_ctx *ctx, int nsteps, double *ms);
+
+/* Per-kernel CUDA-event timing of one iteration's kernels, each launched
+ * `reps` times in isolation: names (comma separated, <= len bytes), average
+ * ms per launch and algorithmic bytes per launch (compulsory reads + writes
+ * of the kernel's arrays).  Restores t afterwards and resets the mixer, so
+ * the next iterate() starts from the same t.  *nk receives the kernel count
+ * (arrays hold up to 16 entries). */
+int r3d_profile_kernels(r3d_ctx *ctx, int reps, char *names, int len,
+                        double *ms, double *bytes, int *nk);
+
+/* State of the solve: completed evaluations, last RMS, and R3D_CONVERGED /
+ * R3D_MAXSTEP / R3D_DIVERGED, or -1 while still running. */
+int r3d_status(r3d_ctx *ctx, int *steps, double *rms, int *status);
+
+/* Bytes copied host->device and device->host by this context so far. */
+int r3d_transfer_bytes(const r3d_ctx *ctx, unsigned long long *h2d,
+                       unsigned long long *d2h);
+
 /* FFT3D::execute (fft3d.cu:72-78), stand-alone test seam: the reference's
  * half-shifted 3D transform F(k) = dv sum_r f(r) e^{-i k.r} of a real grid.
  * dir -1: in = real [N], out = complex interleaved half spectrum [z][y][p]
