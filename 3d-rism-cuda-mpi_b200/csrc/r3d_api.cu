@@ -33,6 +33,22 @@ size_t smem_x(int hx, int n, int S, size_t csz);
 size_t smem_y(int ny, int P, size_t csz);
 size_t smem_z(int nz, int n, int P, size_t csz);
 void kernels_set_smem(bool fp64, size_t maxbytes);
+int dot_blocks_per_sm(bool fp64);
+int mix_chunk();
+void launch_twiddle(double2 *o64, float2 *o32, int count, double scale, cudaStream_t s);
+// compile-time-length passes (r3d_passes_ct.cu)
+size_t ct_smem_x(int L, int PC, size_t csz);
+size_t ct_smem_y(int L, int PC, size_t csz);
+size_t ct_smem_z(int L, int PC, int n, size_t csz);
+bool ct_length_ok(int L);
+template <typename P>
+bool ct_launch_fx(int, int, Batch, int, size_t, cudaStream_t, int, const void *);
+template <typename P>
+bool ct_launch_fy(int, int, Batch, int, size_t, cudaStream_t, int, int);
+template <typename P>
+bool ct_launch_zoz(int, int, Batch, int, size_t, cudaStream_t, int);
+template <typename P>
+bool ct_launch_ix(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
 template <typename P>
 void launch_fwd_x(Batch, int, size_t, cudaStream_t, int, const void *);
 template <typename P>
@@ -93,7 +109,8 @@ static std::string g_last_error;
 
 // Launch geometry of the five grid passes for one (grid, sites, precision).
 struct Geo {
-  int tiles_x = 0, tiles_y = 0, tiles_z = 0, ix_ctas = 0, ix_per = 1, mix_ctas = 0;
+  int tiles_x = 0, tiles_y = 0, tiles_z = 0, ix_ctas = 0, ix_per = 1, mix_ctas = 0,
+      dot_ctas = 0;
   size_t smx = 0, smy = 0, smz = 0;
 };
 
@@ -115,6 +132,7 @@ struct r3d_ctx {
        *fk = nullptr, *chi = nullptr, *lr = nullptr, *hist_a = nullptr,
        *hist_b = nullptr, *cref = nullptr, *chi64 = nullptr;
   double next_refresh = 0;  // mixed path: refresh when rms drops below this
+  void *tw64 = nullptr, *tw32 = nullptr;  // compile-time engine twiddles
   uint32_t *kidx = nullptr;
   double *partials = nullptr, *scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -123,10 +141,7 @@ struct r3d_ctx {
   int *dprefix = nullptr;  // [5][2]: prefix arrays of the passes + ix ctas
   Desc desc{};
   int nshell = 0;
-  // launch geometry
-  int tiles_x = 0, tiles_y = 0, tiles_z = 0, ix_ctas = 0, ix_per = 1,
-      mix_ctas = 0;
-  size_t smx = 0, smy = 0, smz = 0;
+  Geo geo;  // launch geometry of the iteration
   // graph of one iteration
   cudaGraphExec_t gexec = nullptr;
   double ms_per_iter = 0;
@@ -380,19 +395,7 @@ extern "C" int r3d_set_control(r3d_ctx *c, double convergence, int maxstep) {
 // ------------------------------------------------------------ geometry
 static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites);
 static int plan_geometry(r3d_ctx *c, Desc &d) {
-  Geo g;
-  int rc = plan_geo(c, d, g, c->fp64, c->prob.natv);
-  if (rc) return rc;
-  c->tiles_x = g.tiles_x;
-  c->tiles_y = g.tiles_y;
-  c->tiles_z = g.tiles_z;
-  c->ix_ctas = g.ix_ctas;
-  c->ix_per = g.ix_per;
-  c->mix_ctas = g.mix_ctas;
-  c->smx = g.smx;
-  c->smy = g.smy;
-  c->smz = g.smz;
-  return R3D_OK;
+  return plan_geo(c, d, c->geo, c->fp64, c->prob.natv);
 }
 
 static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
@@ -404,6 +407,8 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   d.hx = d.nx / 2;
   d.N = (long long)d.nx * d.ny * d.nz;
   d.Nh = (long long)d.hx * d.ny * d.nz;
+  d.Ns = d.N + 1536;   // 6 KB (FP32) / 12 KB (FP64) off a power of two
+  d.Nhs = d.Nh + 768;
   d.nrad_x = factor_length(d.hx, d.rad_x);
   d.nrad_y = factor_length(d.ny, d.rad_y);
   d.nrad_z = factor_length(d.nz, d.rad_z);
@@ -411,6 +416,16 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
     return fail(c, R3D_EINVAL, "grid sizes must factor into primes <= 13");
   const size_t cs = fp64 ? 16 : 8;
   const int rowsN = d.ny * d.nz;
+  // compile-time engine where the length and tile divide (else runtime engine)
+  const int pcx = fp64 ? 16 : 32;
+  d.ct_x = (ct_length_ok(d.hx) && rowsN % pcx == 0) ? pcx : 0;
+  int pcy = fp64 ? 8 : 16;
+  if (d.hx % pcy) pcy = 8;
+  d.ct_y = (ct_length_ok(d.ny) && d.hx % pcy == 0) ? pcy : 0;
+  int pcz = fp64 ? 4 : 8;
+  if (d.hx % pcz) pcz = 4;
+  d.ct_z = (ct_length_ok(d.nz) && d.hx % pcz == 0 &&
+            ct_smem_z(d.nz, pcz, d.n, cs) <= kSmemMax) ? pcz : 0;
   int S = 16;
   while (S > 1 && (rowsN % S || smem_x(d.hx, d.n, S, cs) > kSmemBudget)) S >>= 1;
   while (S > 1 && rowsN / S < 2 * kNumSM) S >>= 1;
@@ -424,20 +439,105 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   g.smx = smem_x(d.hx, d.n, S, cs);
   g.smy = smem_y(d.ny, Py, cs);
   g.smz = smem_z(d.nz, d.n, Pz, cs);
-  if (g.smx > kSmemMax || g.smy > kSmemMax || g.smz > kSmemMax)
-    return fail(c, R3D_EINVAL, "grid too large for one CTA's shared memory");
   d.tiles_x = rowsN / S;
   d.tiles_y = d.n * d.nz * (d.hx / Py);
   d.tiles_z = d.ny * (d.hx / Pz);
+  if (d.ct_x) {
+    d.tiles_x = d.n * (rowsN / d.ct_x);
+    g.smx = ct_smem_x(d.hx, d.ct_x, cs);
+  }
+  if (d.ct_y) {
+    d.tiles_y = d.n * d.nz * (d.hx / d.ct_y);
+    g.smy = ct_smem_y(d.ny, d.ct_y, cs);
+  }
+  if (d.ct_z) {  // the runtime engine serves the other z modes on the same tiles
+    d.zcols = d.ct_z;
+    d.tiles_z = d.ny * (d.hx / d.ct_z);
+    g.smz = std::max(ct_smem_z(d.nz, d.ct_z, d.n, cs), smem_z(d.nz, d.n, d.ct_z, cs));
+  }
+  if (g.smx > kSmemMax || g.smy > kSmemMax || g.smz > kSmemMax)
+    return fail(c, R3D_EINVAL, "grid too large for one CTA's shared memory");
   g.tiles_x = d.tiles_x;
   g.tiles_y = d.tiles_y;
   g.tiles_z = d.tiles_z;
   g.ix_ctas = std::min(d.tiles_x, 4 * kNumSM);
   g.ix_per = (d.tiles_x + g.ix_ctas - 1) / g.ix_ctas;
   g.ix_ctas = (d.tiles_x + g.ix_per - 1) / g.ix_per;
-  long long niv = (long long)d.n * d.N;
-  g.mix_ctas = (int)std::min<long long>((niv + kThreads - 1) / kThreads, 8 * kNumSM);
+  // mixers: one chunk of mix_chunk() elements per CTA; ANM dots: one full
+  // wave of a grid-stride reduction
+  const long long niv = (long long)d.n * d.Ns;
+  g.mix_ctas = (int)((niv + mix_chunk() - 1) / mix_chunk());
+  int nsm = kNumSM;
+  if (c->opts.device >= 0) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->opts.device);
+  const int bps = c->opts.device >= 0 ? dot_blocks_per_sm(fp64) : 4;
+  g.dot_ctas = (int)std::min<long long>((d.N + kThreads - 1) / kThreads, (long long)nsm * bps);
   return R3D_OK;
+}
+
+// ---------------------------------------------------------- pass dispatch
+// Each pass runs on the compile-time engine when plan_geo chose it for this
+// descriptor (d.ct_* != 0), else on the runtime-length engine.
+template <typename P>
+static void pass_fx(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode,
+                    const void *src) {
+  if (!(d.ct_x && ct_launch_fx<P>(d.hx, d.ct_x, b, g.tiles_x, g.smx, s, mode, src)))
+    launch_fwd_x<P>(b, g.tiles_x, g.smx, s, mode, src);
+}
+template <typename P>
+static void pass_fy(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int dir, int check) {
+  if (!(d.ct_y && ct_launch_fy<P>(d.ny, d.ct_y, b, g.tiles_y, g.smy, s, dir, check)))
+    launch_fft_y<P>(b, g.tiles_y, g.smy, s, dir, check);
+}
+template <typename P>
+static void pass_zoz(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode, int check) {
+  // the compile-time engine implements the fused mode (2) only
+  if (!(mode == 2 && d.ct_z && ct_launch_zoz<P>(d.nz, d.ct_z, b, g.tiles_z, g.smz, s, check)))
+    launch_zoz<P>(b, g.tiles_z, g.smz, s, mode, check);
+}
+template <typename P>
+static void pass_ix(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode, void *dst) {
+  if (!(d.ct_x && ct_launch_ix<P>(d.hx, d.ct_x, b, g.ix_ctas, g.smx, s, mode, dst, g.ix_per)))
+    launch_inv_x<P>(b, g.ix_ctas, g.smx, s, mode, dst, g.ix_per);
+}
+
+// Twiddle tables of the compile-time engine for one grid: [twx | pwx | twy |
+// pwy | twz | pwz]; FP64 always (refresh pipeline), FP32 as well for the
+// mixed path.  Sets the table pointers of d (grid type of the descriptor).
+static int make_twiddles(r3d_ctx *c, Desc &d, bool fp64_desc, void **t64, void **t32) {
+  const int L[6] = {d.hx, d.hx, d.ny, d.ny, d.nz, d.nz};
+  const double sc[6] = {-2.0 / d.hx, -1.0 / d.nx, -2.0 / d.ny, -1.0 / d.ny, -2.0 / d.nz,
+                        -1.0 / d.nz};
+  size_t tot = 0;
+  for (int i = 0; i < 6; ++i) tot += L[i];
+  int rc;
+  if (!*t64 && (rc = dalloc(c, t64, tot * sizeof(double2)))) return rc;
+  if (!fp64_desc && !*t32 && (rc = dalloc(c, t32, tot * sizeof(float2)))) return rc;
+  size_t off = 0;
+  const void *ptr[6];
+  for (int i = 0; i < 6; ++i) {
+    double2 *o64 = (double2 *)*t64 + off;
+    float2 *o32 = fp64_desc ? nullptr : (float2 *)*t32 + off;
+    launch_twiddle(o64, o32, L[i], sc[i], c->stream);
+    ptr[i] = fp64_desc ? (const void *)o64 : (const void *)o32;
+    off += L[i];
+  }
+  d.twx = ptr[0];
+  d.pwx = ptr[1];
+  d.twy = ptr[2];
+  d.pwy = ptr[3];
+  d.twz = ptr[4];
+  d.pwz = ptr[5];
+  CK(cudaGetLastError());
+  return R3D_OK;
+}
+static void set_twiddles64(const void *t64, Desc &d) {
+  const double2 *p = (const double2 *)t64;
+  d.twx = p;
+  d.pwx = p + d.hx;
+  d.twy = p + 2 * d.hx;
+  d.pwy = p + 2 * d.hx + d.ny;
+  d.twz = p + 2 * d.hx + 2 * d.ny;
+  d.pwz = p + 2 * d.hx + 2 * d.ny + d.nz;
 }
 
 // Refresh (also the setup's long-range term): freeze c_ref = c_s(t) (zero at
@@ -448,7 +548,7 @@ template <typename P>
 static int refresh(r3d_ctx *c, bool zero) {
   const Desc &d = c->desc;
   const int n = d.n;
-  const long long N = d.N, Nh = d.Nh;
+  const long long N = d.Ns, Nh = d.Nhs;  // padded site strides
   cudaStream_t s = c->stream;
   Desc dr{};
   Geo g;
@@ -474,16 +574,17 @@ static int refresh(r3d_ctx *c, bool zero) {
   dr.kidx = c->kidx;
   dr.fk = c->fk;
   dr.ctl = ctl;
+  set_twiddles64(c->tw64, dr);
   int pf[8] = {0, g.tiles_x, 0, g.tiles_y, 0, g.tiles_z, 0, g.ix_ctas};
   CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
   CK(copy_h2d(c, dd, &dr, sizeof(Desc), s));
   CK(copy_h2d(c, pre, pf, sizeof(pf), s));
   kernels_set_smem(true, kSmemMax);
-  launch_fwd_x<P64>(Batch{dd, pre, 1}, g.tiles_x, g.smx, s, 0, c64);
-  launch_fft_y<P64>(Batch{dd, pre + 2, 1}, g.tiles_y, g.smy, s, -1, 0);
-  launch_zoz<P64>(Batch{dd, pre + 4, 1}, g.tiles_z, g.smz, s, 2, 0);
-  launch_fft_y<P64>(Batch{dd, pre + 2, 1}, g.tiles_y, g.smy, s, 1, 0);
-  launch_inv_x<P64>(Batch{dd, pre + 6, 1}, g.ix_ctas, g.smx, s, 0, c64, g.ix_per);
+  pass_fx<P64>(dr, g, Batch{dd, pre, 1}, s, 0, c64);
+  pass_fy<P64>(dr, g, Batch{dd, pre + 2, 1}, s, -1, 0);
+  pass_zoz<P64>(dr, g, Batch{dd, pre + 4, 1}, s, 2, 0);
+  pass_fy<P64>(dr, g, Batch{dd, pre + 2, 1}, s, 1, 0);
+  pass_ix<P64>(dr, g, Batch{dd, pre + 6, 1}, s, 0, c64);
   launch_lr_update<P>(c64, c->lr, (long long)n * N, s);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
@@ -502,7 +603,7 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   b += (size_t)nshell * n * n * R;
   size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
   b += slots * n * N * (R + T);    // mixer history (residuals, states)
-  b += (size_t)std::max(c->ix_ctas, c->mix_ctas) * kPartials * 8;
+  b += (size_t)std::max(c->geo.ix_ctas, c->geo.dot_ctas) * kPartials * 8;
   b += (size_t)(c->prob.maxstep + 1) * 8 + sizeof(Ctl) + sizeof(Desc) + 4096;
   return b;
 }
@@ -515,7 +616,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   Desc &d = c->desc;
   cudaStream_t s = c->stream;
   const int n = d.n, nu = (int)p.q.size();
-  const long long N = d.N, Nh = d.Nh;
+  const long long N = d.Ns, Nh = d.Nhs;  // padded site strides
   int rc;
   // grids
   if ((rc = dalloc(c, &c->u, n * N * sizeof(R)))) return rc;
@@ -523,9 +624,9 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = dalloc(c, &c->res, n * N * sizeof(R)))) return rc;
   if ((rc = dalloc(c, &c->lr, n * N * sizeof(R)))) return rc;
   if ((rc = dalloc(c, &c->w, n * Nh * 2 * sizeof(R)))) return rc;
-  if ((rc = dalloc(c, &c->fr, N * sizeof(R)))) return rc;
-  if ((rc = dalloc(c, &c->fk, Nh * sizeof(double2)))) return rc;
-  if ((rc = dalloc(c, (void **)&c->kidx, Nh * 4))) return rc;
+  if ((rc = dalloc(c, &c->fr, d.N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->fk, d.Nh * sizeof(double2)))) return rc;
+  if ((rc = dalloc(c, (void **)&c->kidx, d.Nh * 4))) return rc;
   if ((rc = dalloc(c, &c->chi, (size_t)st.nshell * n * n * sizeof(R)))) return rc;
   // AN2: hist_a = t slots (T), hist_b = residual slots (R);
   // ANM: hist_a = residual ring (R), hist_b = z ring (T)
@@ -534,7 +635,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
   if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
   if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
-  const int npart = std::max(c->ix_ctas, c->mix_ctas);
+  const int npart = std::max(c->geo.ix_ctas, c->geo.dot_ctas);
   if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;
   double *rmslog;
   if ((rc = dalloc(c, (void **)&rmslog, (size_t)(p.maxstep + 1) * 8))) return rc;
@@ -544,8 +645,12 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   CK(cudaMemsetAsync(c->hist_a, 0, slots * n * N * ha, s));
   CK(cudaMemsetAsync(c->hist_b, 0, slots * n * N * hb, s));
   CK(cudaMemsetAsync(c->res, 0, n * N * sizeof(R), s));
-  CK(cudaMemsetAsync(c->fr, 0, N * sizeof(R), s));
-  CK(cudaMemsetAsync(c->fk, 0, Nh * sizeof(double2), s));
+  CK(cudaMemsetAsync(c->u, 0, n * N * sizeof(R), s));
+  CK(cudaMemsetAsync(c->t, 0, n * N * sizeof(T), s));
+  CK(cudaMemsetAsync(c->lr, 0, n * N * sizeof(R), s));
+  CK(cudaMemsetAsync(c->w, 0, n * Nh * 2 * sizeof(R), s));
+  CK(cudaMemsetAsync(c->fr, 0, d.N * sizeof(R), s));
+  CK(cudaMemsetAsync(c->fk, 0, d.Nh * sizeof(double2), s));
   if (!c->fp64) {
     if ((rc = dalloc(c, &c->cref, n * N * sizeof(R)))) return rc;
     if ((rc = dalloc(c, &c->chi64, (size_t)st.nshell * n * n * 8))) return rc;
@@ -578,6 +683,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   d.hist_b = c->hist_b;
   d.partials = c->partials;
   d.ctl = c->ctl;
+  if ((rc = make_twiddles(c, d, c->fp64, &c->tw64, &c->tw32))) return rc;
   d.partial_base = 0;
   d.rmslog = rmslog;
 
@@ -585,7 +691,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   std::vector<double> chi64(st.chi.size());
   {
     std::vector<R> chi(st.chi.size());
-    const double sc = 2.0 / (double)N;
+    const double sc = 2.0 / (double)d.N;
     for (size_t i = 0; i < chi.size(); ++i) {
       chi64[i] = st.chi[i] * sc;
       chi[i] = (R)chi64[i];
@@ -661,7 +767,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     if (coulomb && nu > 0) {
       double2 *ex = tabs, *ey = tabs + (size_t)nu * d.hx, *ez = ey + (size_t)nu * d.ny;
       launch_phase_tables(ex, ey, ez, dx, dy, dz, nu, d.nx, d.ny, d.nz, p.box, s);
-      const double dv = p.box[0] * p.box[1] * p.box[2] / (double)N;
+      const double dv = p.box[0] * p.box[1] * p.box[2] / (double)d.N;
       launch_fk(d, (double2 *)c->fk, ex, ey, ez, dq, nu, ubeta, p.box, dv, s);
       CK(cudaGetLastError());
     }
@@ -679,14 +785,16 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     h.count_left = p.count;
     CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
     CK(copy_h2d(c, c->ddesc, &d, sizeof(Desc), s));
-    int pre[16] = {0, c->tiles_x, 0, c->tiles_y, 0, c->tiles_z, 0, c->ix_ctas,
-                   0, c->mix_ctas, c->ix_ctas, c->mix_ctas, 0, 0, 0, 0};
+    // prefixes: x, y, z, ix, mix passes; ix / dot CTA counts; dot pass
+    int pre[16] = {0, c->geo.tiles_x, 0, c->geo.tiles_y, 0, c->geo.tiles_z, 0, c->geo.ix_ctas,
+                   0, c->geo.mix_ctas, c->geo.ix_ctas, c->geo.dot_ctas, 0, c->geo.dot_ctas, 0, 0};
     CK(copy_h2d(c, c->dprefix, pre, sizeof(pre), s));
     CK(cudaStreamSynchronize(s));
   }
   // the attribute is a per-function limit shared by every context: always
-  // allow the largest tile any context may choose
+  // allow the largest tile any context may choose (set before any capture)
   kernels_set_smem(c->fp64, kSmemMax);
+  kernels_set_smem(true, kSmemMax);
   CK(cudaGetLastError());
   return R3D_OK;
 }
@@ -734,17 +842,19 @@ static void enqueue(r3d_ctx *c, int stage) {
   cudaStream_t s = c->stream;
   const int *pf = c->dprefix;
   Batch bx{c->ddesc, pf + 0, 1}, by{c->ddesc, pf + 2, 1}, bz{c->ddesc, pf + 4, 1},
-      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1};
+      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1}, bdot{c->ddesc, pf + 12, 1};
   int k = 0;
   if (stage != 2) {
-    launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 1, nullptr);
-    launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 1);
-    launch_zoz<P>(bz, c->tiles_z, c->smz, s, 2, 1);
-    launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 1);
-    launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 1, nullptr, c->ix_per);
+    const Desc &d = c->desc;
+    const Geo &g = c->geo;
+    pass_fx<P>(d, g, bx, s, 1, nullptr);
+    pass_fy<P>(d, g, by, s, -1, 1);
+    pass_zoz<P>(d, g, bz, s, 2, 1);
+    pass_fy<P>(d, g, by, s, 1, 1);
+    pass_ix<P>(d, g, bix, s, 1, nullptr);
     k += 5;
     if (c->mixer == MIX_ANM) {
-      launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 0);
+      launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, pf + 11, 1, s, 0);
       ++k;
     }
     launch_reduce(c->ddesc, pf + 10, 1, stage == 0 ? 0 : 2, s);
@@ -755,11 +865,11 @@ static void enqueue(r3d_ctx *c, int stage) {
   }
   if (stage != 1) {
     if (c->mixer == MIX_AN2) {
-      launch_mix_an2<P>(bmx, c->mix_ctas, s);
+      launch_mix_an2<P>(bmx, c->geo.mix_ctas, s);
       ++k;
     } else {
-      launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 1);
-      launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 2);
+      launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 1);
+      launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 2);
       k += 2;
     }
   }
@@ -870,10 +980,10 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   const int *pf = c->dprefix;
   const double n = d.n, N = (double)d.N, rs = sizeof(R), ts = sizeof(T);
   Batch bx{c->ddesc, pf + 0, 1}, by{c->ddesc, pf + 2, 1}, bz{c->ddesc, pf + 4, 1},
-      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1};
+      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1}, bdot{c->ddesc, pf + 12, 1};
   // keep t: the kernels below run out of sequence and overwrite it
   void *tsave = nullptr;
-  const size_t tb = (size_t)d.n * d.N * sizeof(T);
+  const size_t tb = (size_t)d.n * d.Ns * sizeof(T);
   CK(cudaMalloc(&tsave, tb));
   CK(cudaMemcpyAsync(tsave, c->t, tb, cudaMemcpyDeviceToDevice, s));
   Ctl h;
@@ -902,30 +1012,30 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   };
   const double cref = d.cref ? rs : 0.0;
   timed("fwd_x", n * N * (ts + rs + cref + rs),
-        [&] { launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 1, nullptr); });
+        [&] { pass_fx<P>(d, c->geo, bx, s, 1, nullptr); });
   timed("fft_y_fwd", n * N * 2 * rs,
-        [&] { launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 1); });
+        [&] { pass_fy<P>(d, c->geo, by, s, -1, 1); });
   timed("zoz", n * N * 2 * rs + (double)d.Nh * 4,
-        [&] { launch_zoz<P>(bz, c->tiles_z, c->smz, s, 2, 1); });
+        [&] { pass_zoz<P>(d, c->geo, bz, s, 2, 1); });
   timed("fft_y_inv", n * N * 2 * rs,
-        [&] { launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 1); });
+        [&] { pass_fy<P>(d, c->geo, by, s, 1, 1); });
   timed("inv_x", n * N * (rs + ts + rs + rs + rs + (dots ? 2 * rs : 0)),
-        [&] { launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 1, nullptr, c->ix_per); });
+        [&] { pass_ix<P>(d, c->geo, bix, s, 1, nullptr); });
   if (c->mixer == MIX_AN2) {
-    timed("reduce", (double)c->ix_ctas * kPartials * 8,
+    timed("reduce", (double)c->geo.ix_ctas * kPartials * 8,
           [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
     const bool picard = h.count_left > 0;
     timed("mix_an2", picard ? n * N * (3 * ts + 2 * rs) : n * N * (5 * ts + 4 * rs),
-          [&] { launch_mix_an2<P>(bmx, c->mix_ctas, s); });
+          [&] { launch_mix_an2<P>(bmx, c->geo.mix_ctas, s); });
   } else {
     timed("anm_dots", n * N * rs * (h.hcount + 1),
-          [&] { launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 0); });
-    timed("reduce", (double)c->ix_ctas * kPartials * 8,
+          [&] { launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, pf + 11, 1, s, 0); });
+    timed("reduce", (double)c->geo.ix_ctas * kPartials * 8,
           [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
-    timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 1); });
+    timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 1); });
     const int m = std::min(h.hcount, c->history);
     timed("mix_anm", n * N * (rs + ts + m * ts + rs + ts + ts),
-          [&] { launch_anm<P>(bmx, c->mix_ctas, c->ddesc, pf + 11, 1, s, 2); });
+          [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 2); });
   }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->t, tsave, tb, cudaMemcpyDeviceToDevice, s));
@@ -1048,7 +1158,7 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
 // history slot (anderson_cuda.cu:11-22).
 static const void *t_of_residual(r3d_ctx *c, const Ctl &h) {
   if (h.status == MAXSTEP && h.mix_flag && c->mixer == MIX_AN2) {
-    size_t off = (size_t)h.coef[3] * c->desc.n * c->desc.N * sizeof(double);
+    size_t off = (size_t)h.coef[3] * c->desc.n * c->desc.Ns * sizeof(double);
     return (const char *)c->hist_a + off;
   }
   return c->t;
@@ -1149,14 +1259,22 @@ extern "C" int r3d_get_grid(r3d_ctx *c, int which, double *host) {
         launch_shift_qfr<PMix>(d, src, c->scratch, 1.0, x, s);
       break;
     }
-    case R3D_GRID_R: case R3D_GRID_FR: {
-      const void *src = which == R3D_GRID_R ? c->res : c->fr;
-      count = which == R3D_GRID_FR ? d.N : niv;
+    case R3D_GRID_R: {  // site-strided -> dense
+      count = niv;
       if ((rc = ensure_scratch(c, count * 8))) return rc;
       if (c->fp64)
-        launch_to_double<P64>(src, c->scratch, count, 0, s);
+        launch_shift_qfr<P64>(d, c->res, c->scratch, 0.0, 0, s);
       else
-        launch_to_double<PMix>(src, c->scratch, count, 0, s);
+        launch_shift_qfr<PMix>(d, c->res, c->scratch, 0.0, 0, s);
+      break;
+    }
+    case R3D_GRID_FR: {
+      count = d.N;
+      if ((rc = ensure_scratch(c, count * 8))) return rc;
+      if (c->fp64)
+        launch_to_double<P64>(c->fr, c->scratch, count, 0, s);
+      else
+        launch_to_double<PMix>(c->fr, c->scratch, count, 0, s);
       break;
     }
     case R3D_GRID_G: case R3D_GRID_H: {
@@ -1268,8 +1386,10 @@ static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int 
   CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), s));
   d.w = w;
   d.ctl = (Ctl *)ctl;
+  void *t64 = nullptr, *t32 = nullptr;
+  if ((rc = make_twiddles(c, d, c->fp64, &t64, &t32))) return rc;
   CK(copy_h2d(c, ddesc, &d, sizeof(Desc), s));
-  int pf[16] = {0, c->tiles_x, 0, c->tiles_y, 0, c->tiles_z, 0, c->ix_ctas};
+  int pf[16] = {0, c->geo.tiles_x, 0, c->geo.tiles_y, 0, c->geo.tiles_z, 0, c->geo.ix_ctas};
   CK(copy_h2d(c, pre, pf, sizeof(pf), s));
   const int *dp = (const int *)pre;
   Batch bx{(Desc *)ddesc, dp, 1}, by{(Desc *)ddesc, dp + 2, 1}, bz{(Desc *)ddesc, dp + 4, 1},
@@ -1281,9 +1401,9 @@ static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int 
   if (dir < 0) {
     CK(copy_h2d(c, hbuf, in, N * 8, s));
     launch_from_double<P>((const double *)hbuf, src, N, 0, s);
-    launch_fwd_x<P>(bx, c->tiles_x, c->smx, s, 0, src);
-    launch_fft_y<P>(by, c->tiles_y, c->smy, s, -1, 0);
-    launch_zoz<P>(bz, c->tiles_z, c->smz, s, 0, 0);
+    pass_fx<P>(d, c->geo, bx, s, 0, src);
+    pass_fy<P>(d, c->geo, by, s, -1, 0);
+    pass_zoz<P>(d, c->geo, bz, s, 0, 0);
     launch_to_double<P>(w, (double *)hbuf, 2 * Nh, 0, s);
     CK(cudaGetLastError());
     CK(copy_d2h(c, out, hbuf, 2 * Nh * 8, s));
@@ -1306,9 +1426,9 @@ static int fft_typed(r3d_ctx *c, int nx, int ny, int nz, const double *box, int 
     }
     CK(copy_h2d(c, hbuf, tmp.data(), 2 * Nh * 8, s));
     launch_from_double<P>((const double *)hbuf, w, 2 * Nh, 0, s);
-    launch_zoz<P>(bz, c->tiles_z, c->smz, s, 1, 0);
-    launch_fft_y<P>(by, c->tiles_y, c->smy, s, 1, 0);
-    launch_inv_x<P>(bix, c->ix_ctas, c->smx, s, 0, src, c->ix_per);
+    pass_zoz<P>(d, c->geo, bz, s, 1, 0);
+    pass_fy<P>(d, c->geo, by, s, 1, 0);
+    pass_ix<P>(d, c->geo, bix, s, 0, src);
     launch_to_double<P>(src, (double *)hbuf, N, 0, s);
     CK(cudaGetLastError());
     CK(copy_d2h(c, out, hbuf, N * 8, s));

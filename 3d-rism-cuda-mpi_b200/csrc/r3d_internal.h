@@ -108,6 +108,10 @@ struct Desc {
   int nx, ny, nz, n;  // grid and unique solvent sites
   int hx;             // nx / 2 (length of the packed x transform)
   long long N, Nh;    // voxels, half-spectrum points (hx*ny*nz)
+  // site / slot strides of the per-site arrays (elements): N and Nh padded
+  // off powers of two so that the many streams of one kernel do not all
+  // land on the same DRAM channels
+  long long Ns, Nhs;
   int clos, pse_n;
   int mixer, history;
   double beta;        // ANM damping
@@ -123,6 +127,11 @@ struct Desc {
   // FFT plans (radices outermost first)
   int8_t rad_x[kMaxRadices], rad_y[kMaxRadices], rad_z[kMaxRadices];
   int nrad_x, nrad_y, nrad_z;
+  // compile-time-engine passes: columns per tile, 0 = runtime-length engine
+  int ct_x, ct_y, ct_z;
+  // twiddle tables of the compile-time engine (complex, grid type):
+  // tw* = e^{-2 pi i e / L}, pw* = half-sample e^{-i pi a / n} of each pass
+  const void *twx, *pwx, *twy, *pwy, *twz, *pwz;
   // buffers (typed by the kernel's real type)
   // u = beta u - q_v beta phi_L(r) and t = t - q_v beta phi_L(r) (the
   // short-range parts); cref = frozen c_s of the last refresh (or null);

@@ -38,81 +38,9 @@
 #include <math.h>
 #include <stdint.h>
 
-#include "r3d_fft.cuh"
-#include "r3d_internal.h"
+#include "r3d_common.cuh"
 
 namespace r3d {
-
-// ------------------------------------------------------------------ helpers
-struct Batch {
-  const Desc *d;       // [ns]
-  const int *prefix;   // [ns + 1] CTA prefix of this pass
-  int ns;
-};
-
-__device__ __forceinline__ int find_solve(const Batch &b, int cta) {
-  int lo = 0, hi = b.ns - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (b.prefix[mid] <= cta)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
-
-template <typename R>
-__device__ __forceinline__ R closure_g(int clos, int pse_n, R earg) {
-  // calculate_cuda.cu:1-16 (KH, HNC); PSE-n: sum_{i<=n} t*^i / i! for t* > 0.
-  if (clos == HNC) return exp(earg);
-  if (earg >= (R)0) {
-    if (clos == KH || pse_n == 1) return (R)1 + earg;
-    R term = (R)1, sum = (R)1;
-    for (int i = 1; i <= pse_n; ++i) {
-      term *= earg / (R)i;
-      sum += term;
-    }
-    return sum;
-  }
-  return exp(earg);
-}
-
-template <typename R>
-__device__ __forceinline__ bool solve_running(const Desc &d) {
-  return d.ctl->status == RUNNING;
-}
-
-// Shared-memory carve-up: twiddles, digit-reversal table, pack twiddles, data.
-template <typename C>
-struct Smem {
-  C *tw;
-  int16_t *perm;
-  C *ptw;  // half-sample twiddles e^{-i pi a / n}
-  C *buf;
-};
-template <typename C>
-__device__ __forceinline__ Smem<C> carve(char *sm, int L, int Lp) {
-  Smem<C> s;
-  s.tw = (C *)sm;
-  size_t off = sizeof(C) * L;
-  s.ptw = (C *)(sm + off);
-  off += sizeof(C) * Lp;
-  s.perm = (int16_t *)(sm + off);
-  off += ((sizeof(int16_t) * L + 15) / 16) * 16;
-  s.buf = (C *)(sm + off);
-  return s;
-}
-// e^{-i pi a / n} for a in [0, L)
-template <typename C>
-__device__ void half_twiddles(C *ptw, int L, int n) {
-  for (int a = threadIdx.x; a < L; a += blockDim.x) {
-    double s, c;
-    sincospi(-(double)a / (double)n, &s, &c);
-    ptw[a].x = c;
-    ptw[a].y = s;
-  }
-}
 
 // ======================================================================
 // FX: forward x pass.  MODE 0: plain real input `src` ([n][N]);
@@ -145,7 +73,7 @@ __global__ void __launch_bounds__(kThreads)
     int m = e % hx, sr = e / hx, r = sr % S, v = sr / S;
     long long row = row0 + r;
     int y = (int)(row % ny), z = (int)(row / ny);
-    long long base = (long long)v * d.N + row * nx;
+    long long base = (long long)v * d.Ns + row * nx;
     R f0, f1;
     if (MODE == 0) {
       f0 = src[base + m];
@@ -174,7 +102,7 @@ __global__ void __launch_bounds__(kThreads)
   C *w = (C *)d.w;
   for (int e = threadIdx.x; e < total; e += blockDim.x) {
     int p = e % hx, sr = e / hx, r = sr % S, v = sr / S;
-    w[(long long)v * d.Nh + (row0 + r) * hx + p] = sm.buf[sr * hx + p];
+    w[(long long)v * d.Nhs + (row0 + r) * hx + p] = sm.buf[sr * hx + p];
   }
 }
 
@@ -202,7 +130,7 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   SPlan<C> pl{ny, d.nrad_y, {}, sm.tw, sm.perm};
   for (int k = 0; k < d.nrad_y; ++k) pl.rad[k] = d.rad_y[k];
-  C *w = (C *)d.w + (long long)v * d.Nh + (long long)z * ny * hx + pt * PC;
+  C *w = (C *)d.w + (long long)v * d.Nhs + (long long)z * ny * hx + pt * PC;
   const int total = ny * PC;
   if (DIR < 0) {
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
@@ -297,21 +225,21 @@ __global__ void __launch_bounds__(kThreads)
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
       sm.buf[(v * nz + sm.perm[z]) * PC + p] =
-          cmul(w[(long long)v * d.Nh + z * zs + p], sm.ptw[z]);
+          cmul(w[(long long)v * d.Nhs + z * zs + p], sm.ptw[z]);
     }
     __syncthreads();
     fft_dit<-1>(sm.buf, n * PC, PC, sA, 1, PC, pl);
   } else {
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
-      sm.buf[(v * nz + z) * PC + p] = w[(long long)v * d.Nh + z * zs + p];
+      sm.buf[(v * nz + z) * PC + p] = w[(long long)v * d.Nhs + z * zs + p];
     }
     __syncthreads();
   }
   if (MODE == 0) {
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
-      w[(long long)v * d.Nh + z * zs + p] = sm.buf[(v * nz + z) * PC + p];
+      w[(long long)v * d.Nhs + z * zs + p] = sm.buf[(v * nz + z) * PC + p];
     }
     return;
   }
@@ -338,7 +266,7 @@ __global__ void __launch_bounds__(kThreads)
   fft_dif<1>(sm.buf, n * PC, PC, sA, 1, PC, pl);
   for (int e = threadIdx.x; e < total; e += blockDim.x) {
     int p = e % PC, vz = e / PC, z = vz % nz, v = vz / nz;
-    w[(long long)v * d.Nh + z * zs + p] =
+    w[(long long)v * d.Nhs + z * zs + p] =
         cmul(sm.buf[(v * nz + sm.perm[z]) * PC + p], cconj(sm.ptw[z]));
   }
 }
@@ -349,19 +277,6 @@ __global__ void __launch_bounds__(kThreads)
 // of R^2 (cal_rms.cu) and, when AN2 is past its Picard warm-up, the five
 // theta dots per site (anderson_cuda.cu:25-67).  A CTA handles `per` tiles.
 // ======================================================================
-template <typename R>
-__device__ __forceinline__ double block_sum(double v, double *red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  double s = 0;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
-  return s;  // valid in thread 0
-}
-
 template <typename P, int MODE>
 __global__ void __launch_bounds__(kThreads)
     k_inv_x(Batch b, typename P::R *dst, int per) {
@@ -387,7 +302,7 @@ __global__ void __launch_bounds__(kThreads)
   const R *u = (const R *)d.u, *lr = (const R *)d.lr;
   R *res = (R *)d.res;
   const R *rp = (const R *)d.hist_b;
-  const long long niv = (long long)n * d.N;
+  const long long niv = (long long)n * d.Ns;
   double acc_ss = 0;
   double acc[kMaxSites][5];
   for (int v = 0; v < kMaxSites; ++v)
@@ -403,7 +318,7 @@ __global__ void __launch_bounds__(kThreads)
     __syncthreads();
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
       int p = e % hx, sr = e / hx, r = sr % S, v = sr / S;
-      sm.buf[sr * hx + p] = w[(long long)v * d.Nh + (row0 + r) * hx + p];
+      sm.buf[sr * hx + p] = w[(long long)v * d.Nhs + (row0 + r) * hx + p];
     }
     __syncthreads();
     fft_dif<1>(sm.buf, n * S, 1 << 30, 0, hx, 1, pl);
@@ -419,7 +334,7 @@ __global__ void __launch_bounds__(kThreads)
         R h0 = zc.x, h1 = -zc.y;
         if ((m + y + z) & 1) h0 = -h0;
         if ((m + hx + y + z) & 1) h1 = -h1;
-        long long base = (long long)v * d.N + row * nx;
+        long long base = (long long)v * d.Ns + row * nx;
         if (MODE == 0) {
           dst[base + m] = h0;
           dst[base + m + hx] = h1;
@@ -458,12 +373,12 @@ __global__ void __launch_bounds__(kThreads)
   }
   if (MODE == 0) return;
   double *part = d.partials + (size_t)cta * kPartials;
-  double s = block_sum<R>(acc_ss, red);
+  double s = block_sum(acc_ss, red);
   if (threadIdx.x == 0) part[0] = s;
   if (dots) {
     for (int v = 0; v < n; ++v)
       for (int k = 0; k < 5; ++k) {
-        double x = block_sum<R>(acc[v][k], red);
+        double x = block_sum(acc[v][k], red);
         if (threadIdx.x == 0) part[1 + 5 * v + k] = x;
       }
   }
@@ -544,7 +459,7 @@ __global__ void __launch_bounds__(kThreads)
     double v = 0;
     for (int i = threadIdx.x; i < nct; i += blockDim.x)
       v += d.partials[(size_t)i * kPartials + k];
-    double s = block_sum<double>(v, red);
+    double s = block_sum(v, red);
     if (threadIdx.x == 0) sums[k] = s;
   }
   __syncthreads();
@@ -602,6 +517,12 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // AN2 mix: newdt0 / newdt (anderson_cuda.cu:1-22), all sites in one launch.
+// Each CTA owns one chunk of kMixChunk consecutive elements of the [site][x]
+// arrays; every thread loads its kMixPer elements of all six streams before
+// it stores anything, so each thread keeps 6 * kMixPer loads in flight.
+constexpr int kMixPer = 4;
+constexpr int kMixChunk = kThreads * kMixPer;
+
 template <typename P>
 __global__ void __launch_bounds__(kThreads)
     k_mix_an2(Batch b) {
@@ -611,32 +532,61 @@ __global__ void __launch_bounds__(kThreads)
   const Desc &d = b.d[si];
   const Ctl *c = d.ctl;
   if (!c->mix_flag) return;
-  const long long niv = (long long)d.n * d.N;
-  const int cta = blockIdx.x - b.prefix[si];
-  const int nct = b.prefix[si + 1] - b.prefix[si];
-  T *t = (T *)d.t;
-  const R *r = (const R *)d.res;
-  T *tp = (T *)d.hist_a;
-  R *rp = (R *)d.hist_b;
+  const long long niv = (long long)d.n * d.Ns;
+  const long long i0 = (long long)(blockIdx.x - b.prefix[si]) * kMixChunk + threadIdx.x;
+  T *__restrict__ t = (T *)d.t;
+  const R *__restrict__ r = (const R *)d.res;
+  T *__restrict__ tp = (T *)d.hist_a;
+  R *__restrict__ rp = (R *)d.hist_b;
   const bool picard = c->coef[2] < 0;
   const long long boff = (long long)c->coef[3] * niv;
   const double s1 = c->coef[0], s2 = c->coef[1], m = d.m;
-  for (long long i = (long long)cta * blockDim.x + threadIdx.x; i < niv;
-       i += (long long)nct * blockDim.x) {
-    T ti = t[i];
-    R ri = r[i];
-    if (picard) {
-      tp[boff + i] = ti;
-      rp[boff + i] = ri;
-      t[i] = ti + (T)ri;
-    } else {
-      double tt = ti, rr = ri;
-      double tp0 = tp[i], tp1 = tp[i + niv];
-      double rp0 = rp[i], rp1 = rp[i + niv];
-      double uu = tt + s1 * (tp0 - tt) + s2 * (tp1 - tt);
-      double vv = tt + rr + s1 * (tp0 + rp0 - tt - rr) + s2 * (tp1 + rp1 - tt - rr);
-      tp[boff + i] = ti;
-      rp[boff + i] = ri;
+  T tv[kMixPer];
+  R rv[kMixPer];
+  if (picard) {
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) {
+        tv[k] = t[i];
+        rv[k] = r[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) {
+        tp[boff + i] = tv[k];
+        rp[boff + i] = rv[k];
+        t[i] = tv[k] + (T)rv[k];
+      }
+    }
+    return;
+  }
+  T a0[kMixPer], a1[kMixPer];
+  R b0[kMixPer], b1[kMixPer];
+#pragma unroll
+  for (int k = 0; k < kMixPer; ++k) {
+    const long long i = i0 + k * kThreads;
+    if (i < niv) {
+      tv[k] = t[i];
+      rv[k] = r[i];
+      a0[k] = tp[i];
+      a1[k] = tp[i + niv];
+      b0[k] = rp[i];
+      b1[k] = rp[i + niv];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMixPer; ++k) {
+    const long long i = i0 + k * kThreads;
+    if (i < niv) {
+      const double tt = tv[k], rr = rv[k];
+      const double tp0 = a0[k], tp1 = a1[k], rp0 = b0[k], rp1 = b1[k];
+      const double uu = tt + s1 * (tp0 - tt) + s2 * (tp1 - tt);
+      const double vv = tt + rr + s1 * (tp0 + rp0 - tt - rr) + s2 * (tp1 + rp1 - tt - rr);
+      tp[boff + i] = tv[k];
+      rp[boff + i] = rv[k];
       t[i] = (T)(uu + m * (vv - uu));
     }
   }
@@ -656,7 +606,7 @@ __global__ void __launch_bounds__(kThreads)
   const int cta = blockIdx.x - b.prefix[si];
   const int nct = b.prefix[si + 1] - b.prefix[si];
   const int H1 = d.history + 1;
-  const long long niv = (long long)d.n * d.N;
+  const long long niv = (long long)d.n * d.Ns;
   const R *f = (const R *)d.hist_a;
   const R *res = (const R *)d.res;
   double *part = d.partials + (size_t)cta * kPartials;
@@ -667,13 +617,13 @@ __global__ void __launch_bounds__(kThreads)
     double acc = 0;
     for (int v = 0; v < d.n; ++v) {
       double sv = 0;
-      const R *a = res + (long long)v * d.N, *bq = fi + (long long)v * d.N;
+      const R *a = res + (long long)v * d.Ns, *bq = fi + (long long)v * d.Ns;
       for (long long x = (long long)cta * blockDim.x + threadIdx.x; x < d.N;
            x += (long long)nct * blockDim.x)
         sv += (double)a[x] * (double)bq[x];
       acc += sv * d.irho[v];
     }
-    double s = block_sum<double>(acc, red);
+    double s = block_sum(acc, red);
     if (threadIdx.x == 0) part[1 + i] = s;
   }
 }
@@ -730,6 +680,7 @@ __global__ void k_anm_coef(const Desc *descs, const int *ctas, int force) {
 
 // ANM mix: t_{k+1} = w_k (t_k + beta R_k) + sum_i alpha_i z_i ; the newest
 // pair (R_k, z_k = t_k + beta R_k) is written into the ring under `head`.
+// Chunked like k_mix_an2.
 template <typename P>
 __global__ void __launch_bounds__(kThreads)
     k_mix_anm(Batch b) {
@@ -739,25 +690,41 @@ __global__ void __launch_bounds__(kThreads)
   const Desc &d = b.d[si];
   const Ctl *c = d.ctl;
   if (!c->mix_flag) return;
-  const long long niv = (long long)d.n * d.N;
-  const int cta = blockIdx.x - b.prefix[si];
-  const int nct = b.prefix[si + 1] - b.prefix[si];
+  const long long niv = (long long)d.n * d.Ns;
+  const long long i0 = (long long)(blockIdx.x - b.prefix[si]) * kMixChunk + threadIdx.x;
   const int head = c->mix_head, m = c->mix_m;
-  T *t = (T *)d.t;
-  const R *res = (const R *)d.res;
-  R *f = (R *)d.hist_a;
-  T *zr = (T *)d.hist_b;
+  T *__restrict__ t = (T *)d.t;
+  const R *__restrict__ res = (const R *)d.res;
+  R *__restrict__ f = (R *)d.hist_a;
+  T *__restrict__ zr = (T *)d.hist_b;
   const double beta = d.beta, w0 = c->coef[0];
-  for (long long i = (long long)cta * blockDim.x + threadIdx.x; i < niv;
-       i += (long long)nct * blockDim.x) {
-    double rk = res[i];
-    double zk = (double)t[i] + beta * rk;
-    double acc = w0 * zk;
-    for (int j = 0; j < m; ++j)
-      acc += c->coef[1 + j] * (double)zr[(long long)c->mix_slots[j] * niv + i];
-    f[(long long)head * niv + i] = (R)rk;
-    zr[(long long)head * niv + i] = (T)zk;
-    t[i] = (T)acc;
+  double acc[kMixPer], rk[kMixPer], zk[kMixPer];
+#pragma unroll
+  for (int k = 0; k < kMixPer; ++k) {
+    const long long i = i0 + k * kThreads;
+    if (i < niv) {
+      rk[k] = res[i];
+      zk[k] = (double)t[i] + beta * rk[k];
+      acc[k] = w0 * zk[k];
+    }
+  }
+  for (int j = 0; j < m; ++j) {
+    const T *__restrict__ zj = zr + (long long)c->mix_slots[j] * niv;
+    const double cj = c->coef[1 + j];
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) acc[k] += cj * (double)zj[i];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMixPer; ++k) {
+    const long long i = i0 + k * kThreads;
+    if (i < niv) {
+      f[(long long)head * niv + i] = (R)rk[k];
+      zr[(long long)head * niv + i] = (T)zk[k];
+      t[i] = (T)acc[k];
+    }
   }
 }
 
@@ -849,8 +816,8 @@ __global__ void __launch_bounds__(kThreads)
     if (NS > 0 || v < n) {
       // set_du, minus the long-range part; init_tuv's t0 = q_v fr is
       // t_s = 0 on the short-range side
-      u[(long long)v * d.N + ip] = (R)(lj[v] * ikbt + d.qv[v] * bde - d.qv[v] * bfr);
-      t[(long long)v * d.N + ip] = (T)0;
+      u[(long long)v * d.Ns + ip] = (R)(lj[v] * ikbt + d.qv[v] * bde - d.qv[v] * bfr);
+      t[(long long)v * d.Ns + ip] = (T)0;
     }
   }
 }
@@ -951,7 +918,7 @@ template <typename P>
 __global__ void k_cref(Desc d, double *c64) {
   using R = typename P::R;
   using T = typename P::T;
-  const long long niv = (long long)d.n * d.N;
+  const long long niv = (long long)d.n * d.Ns;
   const T *t = (const T *)d.t;
   const R *u = (const R *)d.u;
   R *cref = (R *)d.cref;
@@ -1012,7 +979,7 @@ __global__ void __launch_bounds__(kThreads)
     double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
     for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < d.N;
          x += (long long)gridDim.x * blockDim.x) {
-      long long i = (long long)v * d.N + x;
+      long long i = (long long)v * d.Ns + x;
       // physical t = t_s + q_v beta phi_L(r); t* = t - beta u = t_s - u_s
       double tt = (double)t[i] + d.qv[v] * (double)fr[x];
       double ts = -(double)u[i] + (double)tg[i];
@@ -1040,10 +1007,10 @@ __global__ void __launch_bounds__(kThreads)
       a2 += egf;
       a3 += c;
     }
-    double s0 = block_sum<double>(a0, red);
-    double s1 = block_sum<double>(a1, red);
-    double s2 = block_sum<double>(a2, red);
-    double s3 = block_sum<double>(a3, red);
+    double s0 = block_sum(a0, red);
+    double s1 = block_sum(a1, red);
+    double s2 = block_sum(a2, red);
+    double s3 = block_sum(a3, red);
     if (threadIdx.x == 0) {
       double *o = out + ((size_t)blockIdx.x * d.n + v) * 4;
       o[0] = s0;
@@ -1058,13 +1025,14 @@ __global__ void __launch_bounds__(kThreads)
 template <typename P>
 __global__ void k_gh(Desc d, const typename P::T *tg, double *g, double *h) {
   using R = typename P::R;
-  const long long niv = (long long)d.n * d.N;
+  const long long niv = (long long)d.n * d.N;  // dense output [site][N]
   const R *u = (const R *)d.u, *res = (const R *)d.res;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
-       i += (long long)gridDim.x * blockDim.x) {
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < niv;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long i = (j / d.N) * d.Ns + j % d.N;
     double gv = closure_g<double>(d.clos, d.pse_n, -(double)u[i] + (double)tg[i]);
-    if (g) g[i] = gv;
-    if (h) h[i] = (double)res[i] - 1.0 + gv;
+    if (g) g[j] = gv;
+    if (h) h[j] = (double)res[i] - 1.0 + gv;
   }
 }
 
@@ -1084,12 +1052,14 @@ __global__ void k_from_double(const double *src, R *dst, long long n) {
 template <typename P, typename X>
 __global__ void k_shift_qfr(Desc d, const X *src, double *dst, double sign) {
   using R = typename P::R;
-  const long long niv = (long long)d.n * d.N;
+  const long long niv = (long long)d.n * d.N;  // dense output [site][N]
   const R *fr = (const R *)d.fr;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
-       i += (long long)gridDim.x * blockDim.x) {
-    int v = (int)(i / d.N);
-    dst[i] = (double)src[i] + sign * d.qv[v] * (double)fr[i % d.N];
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < niv;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(j / d.N);
+    const long long x = j % d.N;
+    const double f = sign != 0.0 ? sign * d.qv[v] * (double)fr[x] : 0.0;
+    dst[j] = (double)src[(long long)v * d.Ns + x] + f;
   }
 }
 // physical -> short-range: dst = src - q_v fr
@@ -1097,12 +1067,23 @@ template <typename P>
 __global__ void k_set_short(Desc d, const double *src, typename P::T *dst) {
   using R = typename P::R;
   using T = typename P::T;
-  const long long niv = (long long)d.n * d.N;
+  const long long niv = (long long)d.n * d.N;  // dense input [site][N]
   const R *fr = (const R *)d.fr;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < niv;
-       i += (long long)gridDim.x * blockDim.x) {
-    int v = (int)(i / d.N);
-    dst[i] = (T)(src[i] - d.qv[v] * (double)fr[i % d.N]);
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < niv;
+       j += (long long)gridDim.x * blockDim.x) {
+    const int v = (int)(j / d.N);
+    const long long x = j % d.N;
+    dst[(long long)v * d.Ns + x] = (T)(src[j] - d.qv[v] * (double)fr[x]);
+  }
+}
+
+// Twiddle table entries e^{i pi scale e} for e in [0, count).
+__global__ void k_twiddle(double2 *o64, float2 *o32, int count, double scale) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < count; e += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(scale * (double)e, &s, &c);
+    if (o64) o64[e] = make_double2(c, s);
+    if (o32) o32[e] = make_float2((float)c, (float)s);
   }
 }
 
@@ -1134,11 +1115,38 @@ static void set_smem_attrs(size_t maxbytes) {
   cudaFuncSetAttribute(k_inv_x<P, 1>, a, mb);
 }
 
+// Resident CTAs per SM of the grid-stride streaming kernels (mixers), so
+// that their grids are exactly one wave.
+int dot_blocks_per_sm(bool fp64) {
+  int b = 0;
+  if (fp64)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_anm_dots<P64>, kThreads, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_anm_dots<PMix>, kThreads, 0);
+  return b > 0 ? b : 1;
+}
+int mix_chunk() { return kMixChunk; }
+
+void launch_twiddle(double2 *o64, float2 *o32, int count, double scale, cudaStream_t s) {
+  k_twiddle<<<(count + kThreads - 1) / kThreads, kThreads, 0, s>>>(o64, o32, count, scale);
+}
+
+template <typename P>
+void ct_allow_smem_all();
+
 void kernels_set_smem(bool fp64, size_t maxbytes) {
+  static bool ct_done[2] = {false, false};
   if (fp64)
     set_smem_attrs<P64>(maxbytes);
   else
     set_smem_attrs<PMix>(maxbytes);
+  if (!ct_done[fp64]) {  // compile-time-engine passes, once per process
+    if (fp64)
+      ct_allow_smem_all<P64>();
+    else
+      ct_allow_smem_all<PMix>();
+    ct_done[fp64] = true;
+  }
 }
 
 // Pass launchers.  `grid` = total CTAs of the pass over all solves in the

@@ -1,0 +1,444 @@
+// r3d_passes_ct.cu -- the five grid passes on the compile-time FFT engine
+// (r3d_fft_ct.cuh).  Compiled once per precision: R3D_CT_FP64 = 1 builds the
+// FP64 instantiations, 0 the mixed-precision ones.  The passes compute the
+// same quantities as the runtime-length passes in r3d_kernels.cu (which stay
+// as the fallback for lengths outside kCtLengths); see that file for the
+// algorithm and the reference lines each step follows.
+#include "r3d_common.cuh"
+#include "r3d_fft_ct.cuh"
+
+#ifndef R3D_CT_FP64
+#define R3D_CT_FP64 1
+#endif
+
+namespace r3d {
+
+#if R3D_CT_FP64
+using PCT = P64;
+#else
+using PCT = PMix;
+#endif
+
+// ------------------------------------------------------------------ FX
+// tile = PC consecutive rows (row = y + ny z) of one site; smem [L][PC+1].
+template <typename P, int L, int PC, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_fx_ct(Batch b, const typename P::R *src) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  constexpr int LD = PC + 1;
+  extern __shared__ __align__(16) char smem[];
+  C *buf = (C *)smem;
+  __shared__ int par[PC];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (MODE == 1 && d.ctl->status != RUNNING) return;
+  const int tile = blockIdx.x - b.prefix[si];
+  const int tps = (d.ny * d.nz) / PC;  // tiles per site
+  const int v = tile / tps;
+  const long long row0 = (long long)(tile % tps) * PC;
+  const int nx = d.nx, ny = d.ny;
+  if (threadIdx.x < PC) {
+    long long row = row0 + threadIdx.x;
+    par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
+  }
+  __syncthreads();
+  const C *pw = (const C *)d.pwx;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *cref = (const R *)d.cref;
+  for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+    const int r = e / L, m = e % L;
+    const long long base = (long long)v * d.Ns + (row0 + r) * nx;
+    R f0, f1;
+    if (MODE == 0) {
+      f0 = src[base + m];
+      f1 = src[base + m + L];
+    } else {
+      // trm1mt on the short-range parts (calculate_cuda.cu:18-24)
+      const double t0 = t[base + m], t1 = t[base + m + L];
+      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
+      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + L] + t1);
+      double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
+      if (cref) {
+        c0 -= (double)cref[base + m];
+        c1 -= (double)cref[base + m + L];
+      }
+      f0 = (R)c0;
+      f1 = (R)c1;
+    }
+    if ((m + par[r]) & 1) f0 = -f0;
+    if ((m + L + par[r]) & 1) f1 = -f1;
+    buf[digit_rev<L>(m) * LD + r] = cmul(C{f0, -f1}, pw[m]);
+  }
+  __syncthreads();
+  ct_fft_dit<L, PC, LD, -1>(buf, (const C *)d.twx);
+  C *w = (C *)d.w + (long long)v * d.Nhs + row0 * L;
+  for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+    const int r = e / L, p = e % L;
+    w[(long long)r * L + p] = buf[p * LD + r];
+  }
+}
+
+// ------------------------------------------------------------------ FY
+// tile = PC x-columns of one (site, z) plane; smem [L = ny][PC].
+template <typename P, int L, int PC, int DIR>
+__global__ void __launch_bounds__(kThreads)
+    k_fy_ct(Batch b, int check) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) char smem[];
+  C *buf = (C *)smem;
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (check && d.ctl->status != RUNNING) return;
+  int tile = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, ptiles = hx / PC;
+  const int pt = tile % ptiles;
+  tile /= ptiles;
+  const int z = tile % d.nz, v = tile / d.nz;
+  const C *pw = (const C *)d.pwy;
+  C *w = (C *)d.w + (long long)v * d.Nhs + (long long)z * L * hx + pt * PC;
+  if (DIR < 0) {
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int p = e % PC, y = e / PC;
+      buf[digit_rev<L>(y) * PC + p] = cmul(w[(long long)y * hx + p], pw[y]);
+    }
+    __syncthreads();
+    ct_fft_dit<L, PC, PC, -1>(buf, (const C *)d.twy);
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int p = e % PC, y = e / PC;
+      w[(long long)y * hx + p] = buf[y * PC + p];
+    }
+  } else {
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int p = e % PC, y = e / PC;
+      buf[y * PC + p] = w[(long long)y * hx + p];
+    }
+    __syncthreads();
+    ct_fft_dif<L, PC, PC, 1>(buf, (const C *)d.twy);
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int p = e % PC, y = e / PC;
+      w[(long long)y * hx + p] = cmul(buf[digit_rev<L>(y) * PC + p], cconj(pw[y]));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ ZOZ
+// tile = PC x-columns at one y, all n sites; smem [site][L = nz][PC].
+// Forward z, (mqvfk when d.fk is set), Ornstein-Zernike, inverse z.
+template <typename P, int L, int PC, int NS>
+__device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const Desc &d,
+                                      int y, int pt) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  constexpr int M = NS > 0 ? NS : kMaxSites;
+  const int n = NS > 0 ? NS : d.n;
+  const long long zs = (long long)d.ny * d.hx;
+  const long long off = (long long)y * d.hx + pt * PC;
+  const R *chi = (const R *)d.chi;
+  const double2 *fk = (const double2 *)d.fk;
+  for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+    const int p = e % PC, z = e / PC;
+    const long long gi = z * zs + off + p;
+    const R *ch = chi + (size_t)d.kidx[gi] * n * n;
+    C c[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q)
+      if (q < n) c[q] = buf[(q * L + z) * PC + p];
+    if (fk) {  // mqvfk (refresh pipeline only)
+      const double2 f = fk[gi];
+#pragma unroll
+      for (int q = 0; q < M; ++q)
+        if (q < n) {
+          c[q].x -= (R)(d.qv[q] * f.x);
+          c[q].y -= (R)(d.qv[q] * f.y);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < M; ++a) {
+      if (a < n) {
+        R hr = 0, hi = 0;
+#pragma unroll
+        for (int q = 0; q < M; ++q) {
+          if (q < n) {
+            const R x = ch[a * n + q];
+            hr += c[q].x * x;
+            hi += c[q].y * x;
+          }
+        }
+        buf[(a * L + z) * PC + p] = C{hr, hi};
+      }
+    }
+  }
+}
+
+template <typename P, int L, int PC>
+__global__ void __launch_bounds__(kThreads)
+    k_zoz_ct(Batch b, int check) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  extern __shared__ __align__(16) char smem[];
+  C *buf = (C *)smem;
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (check && d.ctl->status != RUNNING) return;
+  const int tile = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, n = d.n, ptiles = hx / PC;
+  const int pt = tile % ptiles, y = tile / ptiles;
+  const long long zs = (long long)d.ny * hx;
+  const C *pw = (const C *)d.pwz, *tw = (const C *)d.twz;
+  C *w = (C *)d.w + (long long)y * hx + pt * PC;
+  for (int e = threadIdx.x; e < n * PC * L; e += kThreads) {
+    const int p = e % PC, z = (e / PC) % L, v = e / (PC * L);
+    buf[(v * L + digit_rev<L>(z)) * PC + p] = cmul(w[(long long)v * d.Nhs + z * zs + p], pw[z]);
+  }
+  __syncthreads();
+  for (int v = 0; v < n; ++v) ct_fft_dit<L, PC, PC, -1>(buf + v * L * PC, tw);
+  switch (n) {
+    case 1: ct_oz<P, L, PC, 1>(buf, d, y, pt); break;
+    case 2: ct_oz<P, L, PC, 2>(buf, d, y, pt); break;
+    case 3: ct_oz<P, L, PC, 3>(buf, d, y, pt); break;
+    case 4: ct_oz<P, L, PC, 4>(buf, d, y, pt); break;
+    default: ct_oz<P, L, PC, 0>(buf, d, y, pt); break;
+  }
+  __syncthreads();
+  for (int v = 0; v < n; ++v) ct_fft_dif<L, PC, PC, 1>(buf + v * L * PC, tw);
+  for (int e = threadIdx.x; e < n * PC * L; e += kThreads) {
+    const int p = e % PC, z = (e / PC) % L, v = e / (PC * L);
+    w[(long long)v * d.Nhs + z * zs + p] =
+        cmul(buf[(v * L + digit_rev<L>(z)) * PC + p], cconj(pw[z]));
+  }
+}
+
+// ------------------------------------------------------------------ IX
+// tiles as FX; a CTA handles `per` consecutive tiles.  MODE 0 writes the
+// real grid to dst; MODE 1 forms g, R = h + 1 - g (calculate_cuda.cu:54-60),
+// sum R^2 (cal_rms.cu) and, past AN2's Picard warm-up, the five theta dots
+// per site (anderson_cuda.cu:25-67) into this CTA's partials.
+template <typename P, int L, int PC, int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_ix_ct(Batch b, typename P::R *dst, int per) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  constexpr int LD = PC + 1;
+  extern __shared__ __align__(16) char smem[];
+  C *buf = (C *)smem;
+  __shared__ int par[PC];
+  __shared__ double red[kThreads / 32];
+  __shared__ double sums[kPartials];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (MODE == 1 && d.ctl->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int nx = d.nx, ny = d.ny;
+  const int tps = (d.ny * d.nz) / PC;
+  const int ntile = d.n * tps;
+  const bool dots = MODE == 1 && d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
+  const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *lr = (const R *)d.lr;
+  R *res = (R *)d.res;
+  const R *rp = (const R *)d.hist_b;
+  const long long niv = (long long)d.n * d.Ns;
+  if (MODE == 1)
+    for (int k = threadIdx.x; k < kPartials; k += kThreads) sums[k] = 0;
+  double a_ss = 0, a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0;
+  int cur_v = -1;
+  auto flush = [&]() {
+    if (cur_v < 0) return;
+    double x;
+    x = block_sum(a_ss, red);
+    if (threadIdx.x == 0) sums[0] += x;
+    if (dots) {
+      double q[5] = {a0, a1, a2, a3, a4};
+      for (int k = 0; k < 5; ++k) {
+        x = block_sum(q[k], red);
+        if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
+      }
+    }
+    a_ss = a0 = a1 = a2 = a3 = a4 = 0;
+  };
+  for (int it = 0; it < per; ++it) {
+    const int tile = cta * per + it;
+    if (tile >= ntile) break;
+    const int v = tile / tps;
+    const long long row0 = (long long)(tile % tps) * PC;
+    if (MODE == 1 && v != cur_v) {
+      flush();
+      cur_v = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < PC) {
+      long long row = row0 + threadIdx.x;
+      par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
+    }
+    const C *w = (const C *)d.w + (long long)v * d.Nhs + row0 * L;
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, p = e % L;
+      buf[p * LD + r] = w[(long long)r * L + p];
+    }
+    __syncthreads();
+    ct_fft_dif<L, PC, LD, 1>(buf, tw);
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, m = e % L;
+      const C zc = cmul(buf[digit_rev<L>(m) * LD + r], cconj(pw[m]));
+      R h0 = zc.x, h1 = -zc.y;
+      if ((m + par[r]) & 1) h0 = -h0;
+      if ((m + L + par[r]) & 1) h1 = -h1;
+      const long long base = (long long)v * d.Ns + (row0 + r) * nx;
+      if (MODE == 0) {
+        dst[base + m] = h0;
+        dst[base + m + L] = h1;
+      } else {
+        const double t0 = t[base + m], t1 = t[base + m + L];
+        const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
+        const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + L] + t1);
+        const R r0 = (R)((double)h0 + (double)lr[base + m] - g0);
+        const R r1 = (R)((double)h1 + (double)lr[base + m + L] - g1);
+        res[base + m] = r0;
+        res[base + m + L] = r1;
+        a_ss += (double)r0 * r0 + (double)r1 * r1;
+        if (dots) {
+          const double p0 = rp[base + m], p1 = rp[base + m + L];
+          const double q0 = rp[niv + base + m], q1 = rp[niv + base + m + L];
+          const double t10 = (double)r0 - p0, t20 = (double)r0 - q0;
+          const double t11 = (double)r1 - p1, t21 = (double)r1 - q1;
+          a0 += r0 * t10 + r1 * t11;
+          a1 += r0 * t20 + r1 * t21;
+          a2 += t10 * t10 + t11 * t11;
+          a3 += t10 * t20 + t11 * t21;
+          a4 += t20 * t20 + t21 * t21;
+        }
+      }
+    }
+  }
+  if (MODE == 0) return;
+  flush();
+  __syncthreads();
+  double *part = d.partials + (size_t)cta * kPartials;
+  for (int k = threadIdx.x; k < kPartials; k += kThreads) part[k] = sums[k];
+}
+
+// ------------------------------------------------------------ launchers
+#define R3D_CT_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
+
+#if R3D_CT_FP64
+size_t ct_smem_x(int L, int PC, size_t csz) { return csz * (size_t)L * (PC + 1); }
+size_t ct_smem_y(int L, int PC, size_t csz) { return csz * (size_t)L * PC; }
+size_t ct_smem_z(int L, int PC, int n, size_t csz) { return csz * (size_t)L * PC * n; }
+bool ct_length_ok(int L) {
+#define R3D_OK_L(LL) if (L == LL) return true;
+  R3D_CT_LENGTHS(R3D_OK_L)
+#undef R3D_OK_L
+  return false;
+}
+#endif
+
+// Every instantiation is opted into large dynamic shared memory by
+// ct_allow_smem (called at context setup: the attribute cannot be set while a
+// stream is being captured into a graph).
+template <typename K>
+static void allow_smem(K kern) {
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+}
+
+// Returns false when (L, PC) has no compile-time instantiation.
+template <typename P>
+bool ct_launch_fx(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s, int mode,
+                  const void *src) {
+  using R = typename P::R;
+#define R3D_FX(LL)                                                                 \
+  if (L == LL && PC == (sizeof(R) == 4 ? 32 : 16)) {                              \
+    constexpr int PCC = sizeof(R) == 4 ? 32 : 16;                                  \
+    if (mode == 0) {                                                               \
+      k_fx_ct<P, LL, PCC, 0><<<grid, kThreads, smem, s>>>(b, (const R *)src);      \
+    } else {                                                                       \
+      k_fx_ct<P, LL, PCC, 1><<<grid, kThreads, smem, s>>>(b, nullptr);             \
+    }                                                                              \
+    return true;                                                                   \
+  }
+  R3D_CT_LENGTHS(R3D_FX)
+#undef R3D_FX
+  return false;
+}
+
+template <typename P>
+bool ct_launch_fy(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s, int dir,
+                  int check) {
+#define R3D_FY_PC(LL, PCC)                                                  \
+  if (L == LL && PC == PCC) {                                               \
+    if (dir < 0) {                                                          \
+      k_fy_ct<P, LL, PCC, -1><<<grid, kThreads, smem, s>>>(b, check);       \
+    } else {                                                                \
+      k_fy_ct<P, LL, PCC, 1><<<grid, kThreads, smem, s>>>(b, check);        \
+    }                                                                       \
+    return true;                                                            \
+  }
+#define R3D_FY(LL) R3D_FY_PC(LL, 8) R3D_FY_PC(LL, 16)
+  R3D_CT_LENGTHS(R3D_FY)
+#undef R3D_FY
+#undef R3D_FY_PC
+  return false;
+}
+
+template <typename P>
+bool ct_launch_zoz(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s, int check) {
+#define R3D_Z_PC(LL, PCC)                                                 \
+  if (L == LL && PC == PCC) {                                             \
+    k_zoz_ct<P, LL, PCC><<<grid, kThreads, smem, s>>>(b, check);          \
+    return true;                                                          \
+  }
+#define R3D_Z(LL) R3D_Z_PC(LL, 4) R3D_Z_PC(LL, 8)
+  R3D_CT_LENGTHS(R3D_Z)
+#undef R3D_Z
+#undef R3D_Z_PC
+  return false;
+}
+
+template <typename P>
+bool ct_launch_ix(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s, int mode,
+                  void *dst, int per) {
+  using R = typename P::R;
+#define R3D_IX(LL)                                                                   \
+  if (L == LL && PC == (sizeof(R) == 4 ? 32 : 16)) {                                \
+    constexpr int PCC = sizeof(R) == 4 ? 32 : 16;                                    \
+    if (mode == 0) {                                                                 \
+      k_ix_ct<P, LL, PCC, 0><<<grid, kThreads, smem, s>>>(b, (R *)dst, per);         \
+    } else {                                                                         \
+      k_ix_ct<P, LL, PCC, 1><<<grid, kThreads, smem, s>>>(b, nullptr, per);          \
+    }                                                                                \
+    return true;                                                                     \
+  }
+  R3D_CT_LENGTHS(R3D_IX)
+#undef R3D_IX
+  return false;
+}
+
+template <typename P>
+void ct_allow_smem_all() {
+  using R = typename P::R;
+  constexpr int PX = sizeof(R) == 4 ? 32 : 16;
+#define R3D_ATTR(LL)                                                      \
+  allow_smem(k_fx_ct<P, LL, PX, 0>);                                      \
+  allow_smem(k_fx_ct<P, LL, PX, 1>);                                      \
+  allow_smem(k_ix_ct<P, LL, PX, 0>);                                      \
+  allow_smem(k_ix_ct<P, LL, PX, 1>);                                      \
+  allow_smem(k_fy_ct<P, LL, 8, -1>);                                      \
+  allow_smem(k_fy_ct<P, LL, 8, 1>);                                       \
+  allow_smem(k_fy_ct<P, LL, 16, -1>);                                     \
+  allow_smem(k_fy_ct<P, LL, 16, 1>);                                      \
+  allow_smem(k_zoz_ct<P, LL, 4>);                                         \
+  allow_smem(k_zoz_ct<P, LL, 8>);
+  R3D_CT_LENGTHS(R3D_ATTR)
+#undef R3D_ATTR
+}
+template void ct_allow_smem_all<PCT>();
+
+template bool ct_launch_fx<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, const void *);
+template bool ct_launch_fy<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, int);
+template bool ct_launch_zoz<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
+template bool ct_launch_ix<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
+
+}  // namespace r3d

@@ -41,16 +41,18 @@ WORKLOAD = ("256^3 grid, 128 A cell, 2000-atom seeded globule, 0.2 M NaCl water 
 FALLBACK_HBM_GBS = 6650.0
 
 
-def make_deck(d, atoms=None):
+def make_deck(d, atoms=None, grid=256):
+    """The 256^3 deck (default), or for profiling a smaller grid at the same
+    0.5 A spacing and/or the first `atoms` atoms of the same globule."""
     import synthetic
     with gzip.open(os.path.join(ROOT, "tests", "golden", "naclaq_vv.xvk.gz"), "rb") as fi, \
             open(os.path.join(d, "naclaq_vv.xvk"), "wb") as fo:
         shutil.copyfileobj(fi, fo)
-    if atoms is None:
+    if atoms is None and grid == 256:
         return synthetic.config("c2", d), os.path.join(d, "naclaq_vv.xvk")
     sol = synthetic.make_solute(2000, synthetic.SEEDS["c2"])
-    sub = {k: v[:atoms] for k, v in sol.items()}
-    p = synthetic.write_inp(os.path.join(d, "c2_sub.inp"), sub, (128.0,) * 3, (256,) * 3,
+    sub = {k: v[:atoms or 2000] for k, v in sol.items()}
+    p = synthetic.write_inp(os.path.join(d, "c2_sub.inp"), sub, (grid * 0.5,) * 3, (grid,) * 3,
                             "naclaq_vv.xvk")
     return p, os.path.join(d, "naclaq_vv.xvk")
 
@@ -183,7 +185,8 @@ def run_gpu(args, rank, world, local):
 
     prec = args.precision
     tmp = tempfile.mkdtemp(prefix=f"r3dbench{rank}_")
-    inp, xvk = make_deck(tmp)
+    custom = args.grid != 256 or args.atoms != 2000
+    inp, xvk = make_deck(tmp, atoms=args.atoms if custom else None, grid=args.grid)
 
     # ---- end to end: one complete solve through the C-ABI ---------------
     barrier()
@@ -243,7 +246,7 @@ def run_gpu(args, rank, world, local):
     iter_bytes = sum(b for _, _, b in prof)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not custom:
         rate, cores, sample = cpu_oracle_rate(CPU_SAMPLE_ITERS, 1)
         cpu = {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port", "sample": sample}
 
@@ -254,8 +257,11 @@ def run_gpu(args, rank, world, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 grids+transforms, f64 state/reductions" if prec == "mixed" else "f64",
             "data": "synthetic (seeded 2000-atom globule; shipped 0.2 M NaCl .xvk)",
-            "config": {"workload": WORKLOAD, "precision": prec, "grid": 256, "sites": 4,
-                       "atoms": 2000, "replicas": world,
+            "config": {"workload": WORKLOAD if not custom else
+                       f"PROFILING CASE (not the headline): {args.grid}^3 grid, "
+                       f"{args.atoms} atoms, NaCl water, KH, AN2",
+                       "precision": prec, "grid": args.grid, "sites": 4,
+                       "atoms": args.atoms, "replicas": world,
                        "l2": "inputs larger than L2 (>8 GB touched per iteration)"},
             "ms_per_iter": ms_iter,
             "iters_to_converge": steps, "solve_status": status, "final_rms": rms,
@@ -316,6 +322,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--grid", type=int, default=256, help="profiling only: grid size")
+    ap.add_argument("--atoms", type=int, default=2000, help="profiling only: solute atoms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
     args = ap.parse_args()
