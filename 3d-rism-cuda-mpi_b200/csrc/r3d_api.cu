@@ -106,6 +106,9 @@ constexpr int kNumSM = 148;
 using namespace r3d;
 
 static std::string g_last_error;
+namespace r3d {
+void set_last_error(const std::string &m) { g_last_error = m; }
+}  // namespace r3d
 
 // Launch geometry of the five grid passes for one (grid, sites, precision).
 struct Geo {

@@ -31,7 +31,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_set_control", "r3d_initialize", "r3d_calculate", "r3d_anderson",
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
            "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_step",
-           "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d"]
+           "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
+           "r3d_fft3d_noalloc"]
 
 
 class Opts(ctypes.Structure):
@@ -72,6 +73,7 @@ def _load():
         "r3d_transfer_bytes": [vp, ctypes.POINTER(ctypes.c_ulonglong),
                                ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
+        "r3d_fft3d_noalloc": [ci, ci, ci, ci, dp, ci, vp, vp, vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)

@@ -186,6 +186,24 @@ int r3d_transfer_bytes(const r3d_ctx *ctx, unsigned long long *h2d,
 int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
               const double *box, int dir, const double *in, double *out);
 
+/* No counterpart in the reference.  r3d_fft3d (FP64) for callers that
+ * cannot allocate device memory: code running while another framework owns
+ * the device's memory pool, real-time loops that must not enter the
+ * allocator, or work recorded once and replayed.  d_in / d_out are the
+ * caller's device buffers, in the layouts of r3d_fft3d; the only working
+ * storage is one fixed array of R3D_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading this library holds until the process exits.  Grids with
+ * nx/2*ny*nz above (R3D_NOALLOC_SCRATCH_BYTES - 16384) / 16 points (about
+ * 2.1 million: 160^3) are rejected with R3D_EBUDGET.  All calls on a device share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  The
+ * first call on each device looks up the array's address; make it before
+ * any stream capture.  stream may be NULL (the default stream); the call
+ * returns after its work on that stream has finished.  Errors are reported
+ * by r3d_last_error(NULL). */
+#define R3D_NOALLOC_SCRATCH_BYTES (32u << 20)
+int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
+                      int dir, const double *d_in, double *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
