@@ -50,6 +50,9 @@ bool ct_launch_zoz(int, int, Batch, int, size_t, cudaStream_t, int);
 template <typename P>
 bool ct_launch_ix(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
 template <typename P>
+bool ct_launch_ixb(int, int, Batch, int, size_t, cudaStream_t, int);
+size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz);
+template <typename P>
 void launch_fwd_x(Batch, int, size_t, cudaStream_t, int, const void *);
 template <typename P>
 void launch_fft_y(Batch, int, size_t, cudaStream_t, int, int);
@@ -114,6 +117,10 @@ void set_last_error(const std::string &m) { g_last_error = m; }
 struct Geo {
   int tiles_x = 0, tiles_y = 0, tiles_z = 0, ix_ctas = 0, ix_per = 1, mix_ctas = 0,
       dot_ctas = 0;
+  // the iteration's IX with bulk-staged inputs (ixb_pc = 0: not used): rows
+  // per tile, CTAs, tiles per CTA, shared memory
+  int ixb_pc = 0, ixb_ctas = 0, ixb_per = 1;
+  size_t smixb = 0;
   size_t smx = 0, smy = 0, smz = 0;
 };
 
@@ -466,6 +473,20 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   g.ix_ctas = std::min(d.tiles_x, 4 * kNumSM);
   g.ix_per = (d.tiles_x + g.ix_ctas - 1) / g.ix_ctas;
   g.ix_ctas = (d.tiles_x + g.ix_per - 1) / g.ix_per;
+  g.ixb_pc = 0;
+  if (d.ct_x && !getenv("R3D_NO_IXB")) {  // bulk-staged IX: as many CTAs as stay resident
+    const int pcb = fp64 ? 4 : 8;
+    const size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+    if (rowsN % pcb == 0 && sm <= kSmemMax) {
+      const int tiles = d.n * (rowsN / pcb);
+      const int per_sm = std::max(1, (int)((228 * 1024) / (sm + 2048)));
+      g.ixb_pc = pcb;
+      g.smixb = sm;
+      g.ixb_ctas = std::min(tiles, kNumSM * per_sm);
+      g.ixb_per = (tiles + g.ixb_ctas - 1) / g.ixb_ctas;
+      g.ixb_ctas = (tiles + g.ixb_per - 1) / g.ixb_per;
+    }
+  }
   // mixers: one chunk of mix_chunk() elements per CTA; ANM dots: one full
   // wave of a grid-stride reduction
   const long long niv = (long long)d.n * d.Ns;
@@ -499,9 +520,14 @@ static void pass_zoz(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int m
 }
 template <typename P>
 static void pass_ix(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode, void *dst) {
+  if (mode == 1 && g.ixb_pc &&
+      ct_launch_ixb<P>(d.hx, g.ixb_pc, b, g.ixb_ctas, g.smixb, s, g.ixb_per))
+    return;
   if (!(d.ct_x && ct_launch_ix<P>(d.hx, d.ct_x, b, g.ix_ctas, g.smx, s, mode, dst, g.ix_per)))
     launch_inv_x<P>(b, g.ix_ctas, g.smx, s, mode, dst, g.ix_per);
 }
+// CTAs of the iteration's IX (each writes one row of the partials k_reduce sums)
+static int iter_ix_ctas(const Geo &g) { return g.ixb_pc ? g.ixb_ctas : g.ix_ctas; }
 
 // Twiddle tables of the compile-time engine for one grid: [twx | pwx | twy |
 // pwy | twz | pwz]; FP64 always (refresh pipeline), FP32 as well for the
@@ -574,6 +600,8 @@ static int refresh(r3d_ctx *c, bool zero) {
   dr.pse_n = d.pse_n;
   dr.w = w64;
   dr.chi = c->chi64;
+  dr.chis = d.chis;
+  dr.cubic = d.cubic;
   dr.kidx = c->kidx;
   dr.fk = c->fk;
   dr.ctl = ctl;
@@ -606,7 +634,8 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   b += (size_t)nshell * n * n * R;
   size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
   b += slots * n * N * (R + T);    // mixer history (residuals, states)
-  b += (size_t)std::max(c->geo.ix_ctas, c->geo.dot_ctas) * kPartials * 8;
+  b += (size_t)std::max(std::max(c->geo.ix_ctas, iter_ix_ctas(c->geo)), c->geo.dot_ctas) *
+       kPartials * 8;
   b += (size_t)(c->prob.maxstep + 1) * 8 + sizeof(Ctl) + sizeof(Desc) + 4096;
   return b;
 }
@@ -630,7 +659,8 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = dalloc(c, &c->fr, d.N * sizeof(R)))) return rc;
   if ((rc = dalloc(c, &c->fk, d.Nh * sizeof(double2)))) return rc;
   if ((rc = dalloc(c, (void **)&c->kidx, d.Nh * 4))) return rc;
-  if ((rc = dalloc(c, &c->chi, (size_t)st.nshell * n * n * sizeof(R)))) return rc;
+  const int chis = (n * n + 3) / 4 * 4;  // padded rows: aligned vector loads
+  if ((rc = dalloc(c, &c->chi, (size_t)st.nshell * chis * sizeof(R)))) return rc;
   // AN2: hist_a = t slots (T), hist_b = residual slots (R);
   // ANM: hist_a = residual ring (R), hist_b = z ring (T)
   const size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
@@ -638,7 +668,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
   if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
   if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
-  const int npart = std::max(c->geo.ix_ctas, c->geo.dot_ctas);
+  const int npart = std::max(std::max(c->geo.ix_ctas, iter_ix_ctas(c->geo)), c->geo.dot_ctas);
   if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;
   double *rmslog;
   if ((rc = dalloc(c, (void **)&rmslog, (size_t)(p.maxstep + 1) * 8))) return rc;
@@ -656,7 +686,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   CK(cudaMemsetAsync(c->fk, 0, d.Nh * sizeof(double2), s));
   if (!c->fp64) {
     if ((rc = dalloc(c, &c->cref, n * N * sizeof(R)))) return rc;
-    if ((rc = dalloc(c, &c->chi64, (size_t)st.nshell * n * n * 8))) return rc;
+    if ((rc = dalloc(c, &c->chi64, (size_t)st.nshell * ((n * n + 3) / 4 * 4) * 8))) return rc;
     CK(cudaMemsetAsync(c->cref, 0, n * N * sizeof(R), s));
   }
   CK(cudaMemsetAsync(c->partials, 0, (size_t)npart * kPartials * 8, s));
@@ -691,14 +721,18 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   d.rmslog = rmslog;
 
   // chi shell table, scaled by 2/N (the unnormalised transforms' factor)
-  std::vector<double> chi64(st.chi.size());
+  d.cubic = st.cubic ? 1 : 0;
+  d.chis = chis;
+  std::vector<double> chi64((size_t)st.nshell * chis, 0.0);
   {
-    std::vector<R> chi(st.chi.size());
+    std::vector<R> chi(chi64.size(), (R)0);
     const double sc = 2.0 / (double)d.N;
-    for (size_t i = 0; i < chi.size(); ++i) {
-      chi64[i] = st.chi[i] * sc;
-      chi[i] = (R)chi64[i];
-    }
+    for (int sh = 0; sh < st.nshell; ++sh)
+      for (int q = 0; q < n * n; ++q) {
+        const size_t i = (size_t)sh * chis + q;
+        chi64[i] = st.chi[(size_t)sh * n * n + q] * sc;
+        chi[i] = (R)chi64[i];
+      }
     CK(copy_h2d(c, c->chi, chi.data(), chi.size() * sizeof(R), s));
     if (c->fp64)
       c->chi64 = c->chi;
@@ -789,8 +823,9 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
     CK(copy_h2d(c, c->ddesc, &d, sizeof(Desc), s));
     // prefixes: x, y, z, ix, mix passes; ix / dot CTA counts; dot pass
-    int pre[16] = {0, c->geo.tiles_x, 0, c->geo.tiles_y, 0, c->geo.tiles_z, 0, c->geo.ix_ctas,
-                   0, c->geo.mix_ctas, c->geo.ix_ctas, c->geo.dot_ctas, 0, c->geo.dot_ctas, 0, 0};
+    const int ixc = iter_ix_ctas(c->geo);
+    int pre[16] = {0, c->geo.tiles_x, 0, c->geo.tiles_y, 0, c->geo.tiles_z, 0, ixc,
+                   0, c->geo.mix_ctas, ixc, c->geo.dot_ctas, 0, c->geo.dot_ctas, 0, 0};
     CK(copy_h2d(c, c->dprefix, pre, sizeof(pre), s));
     CK(cudaStreamSynchronize(s));
   }
@@ -882,6 +917,7 @@ static void enqueue(r3d_ctx *c, int stage) {
 static int read_ctl(r3d_ctx *c, Ctl &h) {
   CK(copy_d2h(c, &h, c->ctl, sizeof(Ctl), c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (h.err) return fail(c, R3D_ECUDA, "a kernel's bounded wait for a staged copy ran out");
   return R3D_OK;
 }
 static int set_running(r3d_ctx *c) {
@@ -1025,7 +1061,7 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   timed("inv_x", n * N * (rs + ts + rs + rs + rs + (dots ? 2 * rs : 0)),
         [&] { pass_ix<P>(d, c->geo, bix, s, 1, nullptr); });
   if (c->mixer == MIX_AN2) {
-    timed("reduce", (double)c->geo.ix_ctas * kPartials * 8,
+    timed("reduce", (double)iter_ix_ctas(c->geo) * kPartials * 8,
           [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
     const bool picard = h.count_left > 0;
     timed("mix_an2", picard ? n * N * (3 * ts + 2 * rs) : n * N * (5 * ts + 4 * rs),
@@ -1033,7 +1069,7 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   } else {
     timed("anm_dots", n * N * rs * (h.hcount + 1),
           [&] { launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, pf + 11, 1, s, 0); });
-    timed("reduce", (double)c->geo.ix_ctas * kPartials * 8,
+    timed("reduce", (double)iter_ix_ctas(c->geo) * kPartials * 8,
           [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
     timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 1); });
     const int m = std::min(h.hcount, c->history);

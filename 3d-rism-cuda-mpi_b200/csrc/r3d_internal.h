@@ -129,6 +129,8 @@ struct Desc {
   int nrad_x, nrad_y, nrad_z;
   // compile-time-engine passes: columns per tile, 0 = runtime-length engine
   int ct_x, ct_y, ct_z;
+  int cubic;  // nx = ny = nz and a cubic cell: shell index computed, no kidx
+  int chis;   // chi row stride (elements): n*n rounded up to a multiple of 4
   // twiddle tables of the compile-time engine (complex, grid type):
   // tw* = e^{-2 pi i e / L}, pw* = half-sample e^{-i pi a / n} of each pass
   const void *twx, *pwx, *twy, *pwy, *twz, *pwz;

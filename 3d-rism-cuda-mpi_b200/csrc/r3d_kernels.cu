@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kThreads)
     const int nn = n * n;
     for (int e = threadIdx.x; e < nz * PC; e += blockDim.x) {
       int p = e % PC, z = e / PC;
-      const R *ch = chi + (size_t)kidx[z * zs + p] * nn;
+      const R *ch = chi + (size_t)kidx[z * zs + p] * d.chis;
       const double2 *f = fk ? fk + z * zs + p : nullptr;
       C *bp = sm.buf + z * PC + p;
       switch (n) {
@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(kThreads)
     c->rms = sqrt(sums[0] / ((double)d.N * d.n));
     c->step += 1;
     if (c->step <= c->maxstep) d.rmslog[c->step - 1] = c->rms;
-    if (!isfinite(c->rms)) {
+    if (!isfinite(c->rms) || c->err) {  // err: a kernel's bounded wait ran out
       c->status = DIVERGED;
       c->mix_flag = 0;
       return;

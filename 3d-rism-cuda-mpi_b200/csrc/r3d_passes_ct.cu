@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kThreads)
   const C *pw = (const C *)d.pwx;
   const T *t = (const T *)d.t;
   const R *u = (const R *)d.u, *cref = (const R *)d.cref;
+#pragma unroll 4
   for (int e = threadIdx.x; e < PC * L; e += kThreads) {
     const int r = e / L, m = e % L;
     const long long base = (long long)v * d.Ns + (row0 + r) * nx;
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   ct_fft_dit<L, PC, LD, -1>(buf, (const C *)d.twx);
   C *w = (C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll
   for (int e = threadIdx.x; e < PC * L; e += kThreads) {
     const int r = e / L, p = e % L;
     w[(long long)r * L + p] = buf[p * LD + r];
@@ -100,23 +102,27 @@ __global__ void __launch_bounds__(kThreads)
   const C *pw = (const C *)d.pwy;
   C *w = (C *)d.w + (long long)v * d.Nhs + (long long)z * L * hx + pt * PC;
   if (DIR < 0) {
+#pragma unroll
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int p = e % PC, y = e / PC;
       buf[digit_rev<L>(y) * PC + p] = cmul(w[(long long)y * hx + p], pw[y]);
     }
     __syncthreads();
     ct_fft_dit<L, PC, PC, -1>(buf, (const C *)d.twy);
+#pragma unroll
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int p = e % PC, y = e / PC;
       w[(long long)y * hx + p] = buf[y * PC + p];
     }
   } else {
+#pragma unroll
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int p = e % PC, y = e / PC;
       buf[y * PC + p] = w[(long long)y * hx + p];
     }
     __syncthreads();
     ct_fft_dif<L, PC, PC, 1>(buf, (const C *)d.twy);
+#pragma unroll
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int p = e % PC, y = e / PC;
       w[(long long)y * hx + p] = cmul(buf[digit_rev<L>(y) * PC + p], cconj(pw[y]));
@@ -138,10 +144,43 @@ __device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const 
   const long long off = (long long)y * d.hx + pt * PC;
   const R *chi = (const R *)d.chi;
   const double2 *fk = (const double2 *)d.fk;
+  // shell of |k|: cubic cells use s = ax^2 + ay^2 + az^2 over the odd
+  // integers a = 2j - n + 1 (shell (s - 3) / 8), others the kidx table
+  const long long ay = 2 * y - d.ny + 1;
+#pragma unroll 2
   for (int e = threadIdx.x; e < PC * L; e += kThreads) {
     const int p = e % PC, z = e / PC;
     const long long gi = z * zs + off + p;
-    const R *ch = chi + (size_t)d.kidx[gi] * n * n;
+    size_t shell;
+    if (d.cubic) {
+      const long long ax = 4 * (pt * PC + p) - d.nx + 1, az = 2 * z - d.nz + 1;
+      shell = (size_t)((ax * ax + ay * ay + az * az - 3) / 8);
+    } else {
+      shell = d.kidx[gi];
+    }
+    const R *ch = chi + shell * d.chis;
+    R x[M * M];
+    if constexpr (NS > 0 && (NS * NS) % 4 == 0 && sizeof(R) == 4) {  // 16-byte rows
+#pragma unroll
+      for (int q = 0; q < NS * NS / 4; ++q) {
+        const float4 v4 = reinterpret_cast<const float4 *>(ch)[q];
+        x[4 * q] = v4.x;
+        x[4 * q + 1] = v4.y;
+        x[4 * q + 2] = v4.z;
+        x[4 * q + 3] = v4.w;
+      }
+    } else if constexpr (NS > 0 && (NS * NS) % 2 == 0 && sizeof(R) == 8) {
+#pragma unroll
+      for (int q = 0; q < NS * NS / 2; ++q) {
+        const double2 v2 = reinterpret_cast<const double2 *>(ch)[q];
+        x[2 * q] = v2.x;
+        x[2 * q + 1] = v2.y;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < M * M; ++q)
+        if (q < n * n) x[q] = ch[q];
+    }
     C c[M];
 #pragma unroll
     for (int q = 0; q < M; ++q)
@@ -162,9 +201,9 @@ __device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const 
 #pragma unroll
         for (int q = 0; q < M; ++q) {
           if (q < n) {
-            const R x = ch[a * n + q];
-            hr += c[q].x * x;
-            hi += c[q].y * x;
+            const R xq = x[a * n + q];
+            hr += c[q].x * xq;
+            hi += c[q].y * xq;
           }
         }
         buf[(a * L + z) * PC + p] = C{hr, hi};
@@ -189,9 +228,14 @@ __global__ void __launch_bounds__(kThreads)
   const long long zs = (long long)d.ny * hx;
   const C *pw = (const C *)d.pwz, *tw = (const C *)d.twz;
   C *w = (C *)d.w + (long long)y * hx + pt * PC;
-  for (int e = threadIdx.x; e < n * PC * L; e += kThreads) {
-    const int p = e % PC, z = (e / PC) % L, v = e / (PC * L);
-    buf[(v * L + digit_rev<L>(z)) * PC + p] = cmul(w[(long long)v * d.Nhs + z * zs + p], pw[z]);
+  for (int v = 0; v < n; ++v) {
+    const C *wv = w + (long long)v * d.Nhs;
+    C *bv = buf + v * L * PC;
+#pragma unroll
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int p = e % PC, z = e / PC;
+      bv[digit_rev<L>(z) * PC + p] = cmul(wv[z * zs + p], pw[z]);
+    }
   }
   __syncthreads();
   for (int v = 0; v < n; ++v) ct_fft_dit<L, PC, PC, -1>(buf + v * L * PC, tw);
@@ -204,10 +248,14 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
   for (int v = 0; v < n; ++v) ct_fft_dif<L, PC, PC, 1>(buf + v * L * PC, tw);
-  for (int e = threadIdx.x; e < n * PC * L; e += kThreads) {
-    const int p = e % PC, z = (e / PC) % L, v = e / (PC * L);
-    w[(long long)v * d.Nhs + z * zs + p] =
-        cmul(buf[(v * L + digit_rev<L>(z)) * PC + p], cconj(pw[z]));
+  for (int v = 0; v < n; ++v) {
+    C *wv = w + (long long)v * d.Nhs;
+    const C *bv = buf + v * L * PC;
+#pragma unroll
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int p = e % PC, z = e / PC;
+      wv[z * zs + p] = cmul(bv[digit_rev<L>(z) * PC + p], cconj(pw[z]));
+    }
   }
 }
 
@@ -216,8 +264,17 @@ __global__ void __launch_bounds__(kThreads)
 // real grid to dst; MODE 1 forms g, R = h + 1 - g (calculate_cuda.cu:54-60),
 // sum R^2 (cal_rms.cu) and, past AN2's Picard warm-up, the five theta dots
 // per site (anderson_cuda.cu:25-67) into this CTA's partials.
+#ifndef R3D_IX_MINB
+#define R3D_IX_MINB 2
+#endif
+#ifndef R3D_IX_UNROLL
+#define R3D_IX_UNROLL 1
+#endif
+#define R3D_PRAGMA(x) _Pragma(#x)
+#define R3D_UNROLL_N(n) R3D_PRAGMA(unroll n)
+#define R3D_UNROLL(n) R3D_UNROLL_N(n)
 template <typename P, int L, int PC, int MODE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
     k_ix_ct(Batch b, typename P::R *dst, int per) {
   using R = typename P::R;
   using T = typename P::T;
@@ -275,12 +332,14 @@ __global__ void __launch_bounds__(kThreads)
       par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
     }
     const C *w = (const C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int r = e / L, p = e % L;
       buf[p * LD + r] = w[(long long)r * L + p];
     }
     __syncthreads();
     ct_fft_dif<L, PC, LD, 1>(buf, tw);
+    R3D_UNROLL(R3D_IX_UNROLL)
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int r = e / L, m = e % L;
       const C zc = cmul(buf[digit_rev<L>(m) * LD + r], cconj(pw[m]));
@@ -316,6 +375,219 @@ __global__ void __launch_bounds__(kThreads)
   }
   if (MODE == 0) return;
   flush();
+  __syncthreads();
+  double *part = d.partials + (size_t)cta * kPartials;
+  for (int k = threadIdx.x; k < kPartials; k += kThreads) part[k] = sums[k];
+}
+
+// ------------------------------------------------- IX with bulk staging
+// The iteration's IX (MODE 1) with the per-voxel inputs staged by the bulk
+// copy engine: a tile's PC rows of one site are one contiguous block in each
+// of t, u, lr and the two AN2 residual slots, so one cp.async.bulk per array
+// brings the next tile into shared memory while the current one is being
+// transformed and reduced (two stages, one mbarrier each).
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Bounded wait for phase `parity` of `bar`; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <typename P, int L, int PC>
+struct IxStage {  // byte layout of one stage of staged inputs
+  static constexpr int NX = 2 * L;
+  static constexpr size_t t = 0;
+  static constexpr size_t u = t + (size_t)PC * NX * sizeof(typename P::T);
+  static constexpr size_t lr = u + (size_t)PC * NX * sizeof(typename P::R);
+  static constexpr size_t r0 = lr + (size_t)PC * NX * sizeof(typename P::R);
+  static constexpr size_t r1 = r0 + (size_t)PC * NX * sizeof(typename P::R);
+  static constexpr size_t bytes = r1 + (size_t)PC * NX * sizeof(typename P::R);
+};
+#if R3D_CT_FP64
+size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz) {
+  const size_t buf = ((csz * (size_t)L * (PC + 1) + 127) / 128) * 128;
+  const size_t stage = (size_t)PC * 2 * L * (tsz + 4 * rsz);
+  return buf + 2 * stage;
+}
+#endif
+
+template <typename P, int L, int PC>
+__global__ void __launch_bounds__(kThreads)
+    k_ix_bulk(Batch b, int per) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  using St = IxStage<P, L, PC>;
+  constexpr int LD = PC + 1, NX = 2 * L;
+  constexpr size_t BUF = ((sizeof(C) * (size_t)L * LD + 127) / 128) * 128;
+  extern __shared__ __align__(128) char smem[];
+  C *buf = (C *)smem;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int par[PC];
+  __shared__ double red[kThreads / 32];
+  __shared__ double sums[kPartials];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (d.ctl->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int ny = d.ny;
+  const int tps = (d.ny * d.nz) / PC;
+  const int ntile = d.n * tps;
+  const int first = cta * per;
+  const int count = min(per, ntile - first);
+  if (count <= 0) return;
+  const bool dots = d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
+  const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
+  R *res = (R *)d.res;
+  const long long niv = (long long)d.n * d.Ns;
+  const uint32_t tbytes = PC * NX * sizeof(T), rbytes = PC * NX * sizeof(R);
+  const uint32_t stage_tx = tbytes + 2 * rbytes + (dots ? 2 * rbytes : 0);
+  auto issue = [&](int tile, int st) {  // thread 0: copies of one tile
+    const int v = tile / tps;
+    const long long base = (long long)v * d.Ns + (long long)(tile % tps) * PC * NX;
+    char *sb = smem + BUF + st * St::bytes;
+    uint64_t *br = &bar[st];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(br, stage_tx);
+    bulk_g2s(sb + St::t, (const T *)d.t + base, tbytes, br);
+    bulk_g2s(sb + St::u, (const R *)d.u + base, rbytes, br);
+    bulk_g2s(sb + St::lr, (const R *)d.lr + base, rbytes, br);
+    if (dots) {
+      bulk_g2s(sb + St::r0, (const R *)d.hist_b + base, rbytes, br);
+      bulk_g2s(sb + St::r1, (const R *)d.hist_b + niv + base, rbytes, br);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int k = threadIdx.x; k < kPartials; k += kThreads) sums[k] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) issue(first, 0);
+  double a_ss = 0, a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0;
+  int cur_v = -1;
+  uint32_t phase = 0;  // bit st: parity of the next wait on stage st
+  bool failed = false;
+  int stop = -1;  // iteration at which a staged copy's wait ran out
+  for (int it = 0; it < count; ++it) {
+    const int tile = first + it, st = it & 1;
+    const int v = tile / tps;
+    const long long row0 = (long long)(tile % tps) * PC;
+    if (v != cur_v) {  // uniform: flush the previous site's sums
+      if (cur_v >= 0) {
+        double x = block_sum(a_ss, red);
+        if (threadIdx.x == 0) sums[0] += x;
+        if (dots) {
+          const double q[5] = {a0, a1, a2, a3, a4};
+#pragma unroll
+          for (int k = 0; k < 5; ++k) {
+            x = block_sum(q[k], red);
+            if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
+          }
+        }
+        a_ss = a0 = a1 = a2 = a3 = a4 = 0;
+      }
+      cur_v = v;
+    }
+    // the other stage is free (its readers passed the barrier at the end of
+    // the previous iteration): prefetch the next tile into it
+    if (threadIdx.x == 0 && it + 1 < count) issue(tile + 1, st ^ 1);
+    if (threadIdx.x < PC) {
+      const long long row = row0 + threadIdx.x;
+      par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
+    }
+    const C *w = (const C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, p = e % L;
+      buf[p * LD + r] = w[(long long)r * L + p];
+    }
+    __syncthreads();
+    ct_fft_dif<L, PC, LD, 1>(buf, tw);
+    if (!mbar_wait(&bar[st], (phase >> st) & 1)) failed = true;
+    phase ^= 1u << st;
+    const char *sb = smem + BUF + st * St::bytes;
+    const T *ts = (const T *)(sb + St::t);
+    const R *us = (const R *)(sb + St::u), *ls = (const R *)(sb + St::lr);
+    const R *q0s = (const R *)(sb + St::r0), *q1s = (const R *)(sb + St::r1);
+    const long long gbase = (long long)v * d.Ns + row0 * NX;
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, m = e % L;
+      const C zc = cmul(buf[digit_rev<L>(m) * LD + r], cconj(pw[m]));
+      R h0 = zc.x, h1 = -zc.y;
+      if ((m + par[r]) & 1) h0 = -h0;
+      if ((m + L + par[r]) & 1) h1 = -h1;
+      const int i0 = r * NX + m, i1 = i0 + L;
+      const double t0 = ts[i0], t1 = ts[i1];
+      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)us[i0] + t0);
+      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)us[i1] + t1);
+      const R r0 = (R)((double)h0 + (double)ls[i0] - g0);
+      const R r1 = (R)((double)h1 + (double)ls[i1] - g1);
+      res[gbase + i0] = r0;
+      res[gbase + i1] = r1;
+      a_ss += (double)r0 * r0 + (double)r1 * r1;
+      if (dots) {
+        const double t10 = (double)r0 - q0s[i0], t20 = (double)r0 - q1s[i0];
+        const double t11 = (double)r1 - q0s[i1], t21 = (double)r1 - q1s[i1];
+        a0 += r0 * t10 + r1 * t11;
+        a1 += r0 * t20 + r1 * t21;
+        a2 += t10 * t10 + t11 * t11;
+        a3 += t10 * t20 + t11 * t21;
+        a4 += t20 * t20 + t21 * t21;
+      }
+    }
+    if (__syncthreads_or(failed)) {  // buf, par and this stage are free again
+      stop = it;
+      break;
+    }
+  }
+  if (stop >= 0) {  // flag the solve, wait (bounded) for the copies in flight, give up
+    if (threadIdx.x == 0) atomicExch(&d.ctl->err, 1);
+    const int st = stop & 1;
+    mbar_wait(&bar[st], ((phase >> st) & 1) ^ 1);
+    if (stop + 1 < count) mbar_wait(&bar[st ^ 1], (phase >> (st ^ 1)) & 1);
+    return;
+  }
+  {
+    double x = block_sum(a_ss, red);
+    if (threadIdx.x == 0) sums[0] += x;
+    if (dots) {
+      const double q[5] = {a0, a1, a2, a3, a4};
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        x = block_sum(q[k], red);
+        if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
+      }
+    }
+  }
   __syncthreads();
   double *part = d.partials + (size_t)cta * kPartials;
   for (int k = threadIdx.x; k < kPartials; k += kThreads) part[k] = sums[k];
@@ -417,6 +689,19 @@ bool ct_launch_ix(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s,
 }
 
 template <typename P>
+bool ct_launch_ixb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s, int per) {
+#define R3D_IXB(LL)                                                             \
+  if (L == LL && PC == (sizeof(typename P::R) == 4 ? 8 : 4)) {                 \
+    constexpr int PCC = sizeof(typename P::R) == 4 ? 8 : 4;                     \
+    k_ix_bulk<P, LL, PCC><<<grid, kThreads, smem, s>>>(b, per);                \
+    return true;                                                                \
+  }
+  R3D_CT_LENGTHS(R3D_IXB)
+#undef R3D_IXB
+  return false;
+}
+
+template <typename P>
 void ct_allow_smem_all() {
   using R = typename P::R;
   constexpr int PX = sizeof(R) == 4 ? 32 : 16;
@@ -430,7 +715,8 @@ void ct_allow_smem_all() {
   allow_smem(k_fy_ct<P, LL, 16, -1>);                                     \
   allow_smem(k_fy_ct<P, LL, 16, 1>);                                      \
   allow_smem(k_zoz_ct<P, LL, 4>);                                         \
-  allow_smem(k_zoz_ct<P, LL, 8>);
+  allow_smem(k_zoz_ct<P, LL, 8>);                                         \
+  allow_smem(k_ix_bulk<P, LL, (sizeof(typename P::R) == 4 ? 8 : 4)>);
   R3D_CT_LENGTHS(R3D_ATTR)
 #undef R3D_ATTR
 }
@@ -440,5 +726,6 @@ template bool ct_launch_fx<PCT>(int, int, Batch, int, size_t, cudaStream_t, int,
 template bool ct_launch_fy<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, int);
 template bool ct_launch_zoz<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
 template bool ct_launch_ix<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
+template bool ct_launch_ixb<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
 
 }  // namespace r3d
