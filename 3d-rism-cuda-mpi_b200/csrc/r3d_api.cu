@@ -26,7 +26,7 @@ struct Batch {
 };
 struct AtomTab {
   const double *x, *y, *z, *q;
-  const double *isig2, *eps4;
+  const double *sig2, *eps4;
   int nu;
 };
 size_t smem_x(int hx, int n, int S, size_t csz);
@@ -753,7 +753,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   // potentials: atom tables (cal_LJ.cu:33-40 mixing rules)
   {
     const double lambda1 = p.adswitch == 1 ? p.lambda : 1.0;
-    std::vector<double> ax(nu), ay(nu), az(nu), isig2((size_t)n * nu), eps4((size_t)n * nu);
+    std::vector<double> ax(nu), ay(nu), az(nu), sig2((size_t)n * nu), eps4((size_t)n * nu);
     for (int iu = 0; iu < nu; ++iu) {
       ax[iu] = p.r[3 * iu];
       ay[iu] = p.r[3 * iu + 1];
@@ -762,7 +762,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     for (int v = 0; v < n; ++v)
       for (int iu = 0; iu < nu; ++iu) {
         double sg = (p.sig[iu] + p.sigv[v]) * 0.5 * lambda1;
-        isig2[(size_t)v * nu + iu] = 1.0 / (sg * sg);
+        sig2[(size_t)v * nu + iu] = sg * sg;
         eps4[(size_t)v * nu + iu] = std::sqrt(p.eps[iu] * p.epsv[v]) * 4.0;
       }
     double *dat;
@@ -776,12 +776,12 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
       CK(copy_h2d(c, dz, az.data(), nu * 8, s));
       CK(copy_h2d(c, dq, p.q.data(), nu * 8, s));
       for (int v = 0; v < n; ++v) {
-        CK(copy_h2d(c, dsig + (size_t)v * natom, isig2.data() + (size_t)v * nu, nu * 8, s));
+        CK(copy_h2d(c, dsig + (size_t)v * natom, sig2.data() + (size_t)v * nu, nu * 8, s));
         CK(copy_h2d(c, deps + (size_t)v * natom, eps4.data() + (size_t)v * nu, nu * 8, s));
       }
     }
     AtomTab at{dx, dy, dz, dq, dsig, deps, nu};
-    // the kernel indexes isig2/eps4 as [v * nu + i]; pass nu as the stride
+    // the kernel indexes sig2/eps4 as [v * nu + i]; pass nu as the stride
     const double ikbt = 1.0 / (phys::avogadro * phys::boltzmann * p.temper);
     const int coulomb = p.adswitch != 1;
     const double lambda2 = p.adswitch == 2 ? p.lambda : 1.0;

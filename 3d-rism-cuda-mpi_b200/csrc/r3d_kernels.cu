@@ -734,14 +734,27 @@ __global__ void __launch_bounds__(kThreads)
 // ======================================================================
 struct AtomTab {
   const double *x, *y, *z, *q;  // [nu]
-  const double *isig2, *eps4;   // [n][nu]: 1/sigma_uv^2, 4 eps_uv
+  const double *sig2, *eps4;    // [n][nu]: sigma_uv^2, 4 eps_uv
   int nu;
 };
 
 constexpr int kAtomTile = 128;
+constexpr int kPotVox = 2;  // voxels per thread, adjacent in x (nx is even)
 
-// One thread per voxel: LJ for every site, Coulomb real space; writes
-// u[v] = beta u_LJ + q_v beta phi(r), fr = beta phi_L(r), t0[v] = q_v fr.
+// Grid potentials, all sites per voxel: LJ (cal_LJ.cu:56-81), Coulomb in real
+// space (cal_Coulomb.cu:40-62); writes u[v] = beta u_LJ + q_v beta (phi -
+// phi_L), fr = beta phi_L(r), t0[v] = 0 (the short-range side of init_tuv's
+// t0 = q_v fr).
+//
+// The pair sums are the reference's, arranged so that one atom-voxel pair
+// costs one FP64 reciprocal square root and no division:
+//   1/r = rsqrt(r^2);  (sigma/r)^2 = sigma^2 (1/r)^2, clamped at 1/cut^2,
+//   which is the reference's clamp of (r/sigma)^2 from below at cut^2;
+//   e^{-r} of the long-range kernel (1 - e^{-r})/r is evaluated only for
+//   r <= 38 A: beyond, 1 - e^{-r} rounds to 1 in FP64, as it does in the
+//   reference, and most pairs of a protein-sized grid are that far apart.
+// Each thread owns kPotVox voxels, which share an atom's y/z distance terms
+// and its shared-memory loads.
 template <typename P, int NS>
 __global__ void __launch_bounds__(kThreads)
     k_potential(Desc d, AtomTab at, double ikbt, double ubeta, double dx,
@@ -749,58 +762,71 @@ __global__ void __launch_bounds__(kThreads)
   using R = typename P::R;
   using T = typename P::T;
   constexpr int M = NS > 0 ? NS : kMaxSites;
-  __shared__ double sx[kAtomTile], sy[kAtomTile], sz[kAtomTile], sq[kAtomTile];
-  __shared__ double ss[kMaxSites][kAtomTile], se[kMaxSites][kAtomTile];
-  const long long ip = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = ip < d.N;
+  constexpr int V = kPotVox;
+  __shared__ double2 sxy[kAtomTile], szq[kAtomTile];
+  __shared__ double2 sse[M][kAtomTile];  // (sigma^2, 4 eps) per site
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = it * V < d.N;
+  const long long ip = live ? it * V : 0;
   const int n = d.n;
-  int x = 0, y = 0, z = 0;
-  if (live) {
-    x = (int)(ip % d.nx);
-    y = (int)((ip / d.nx) % d.ny);
-    z = (int)(ip / ((long long)d.nx * d.ny));
-  }
+  const int x = (int)(ip % d.nx), y = (int)((ip / d.nx) % d.ny),
+            z = (int)(ip / ((long long)d.nx * d.ny));
   const double rx = (x - d.nx / 2) * dx, ry = (y - d.ny / 2) * dy,
                rz = (z - d.nz / 2) * dz;
-  double lj[M];
+  double lj[V][M], e[V], f[V];
 #pragma unroll
-  for (int v = 0; v < M; ++v) lj[v] = 0;
-  double e = 0, f = 0;
-  const double cut2 = 2.0e-3 * 2.0e-3;
+  for (int j = 0; j < V; ++j) {
+    e[j] = f[j] = 0;
+#pragma unroll
+    for (int v = 0; v < M; ++v) lj[j][v] = 0;
+  }
+  const double smax = 1.0 / (2.0e-3 * 2.0e-3);  // cal_LJ.cu:11
   for (int a0 = 0; a0 < at.nu; a0 += kAtomTile) {
     const int na = min(kAtomTile, at.nu - a0);
     __syncthreads();
     for (int i = threadIdx.x; i < na; i += blockDim.x) {
-      sx[i] = at.x[a0 + i];
-      sy[i] = at.y[a0 + i];
-      sz[i] = at.z[a0 + i];
-      sq[i] = at.q[a0 + i];
-      for (int v = 0; v < n; ++v) {
-        ss[v][i] = at.isig2[v * at.nu + a0 + i];
-        se[v][i] = at.eps4[v * at.nu + a0 + i];
-      }
+      sxy[i] = make_double2(at.x[a0 + i], at.y[a0 + i]);
+      szq[i] = make_double2(at.z[a0 + i], at.q[a0 + i]);
+      for (int v = 0; v < n; ++v)
+        sse[v][i] = make_double2(at.sig2[v * at.nu + a0 + i], at.eps4[v * at.nu + a0 + i]);
     }
     __syncthreads();
     for (int i = 0; i < na; ++i) {
-      double ddx = rx - sx[i], ddy = ry - sy[i], ddz = rz - sz[i];
-      double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      const double2 axy = sxy[i], azq = szq[i];
+      const double ddy = ry - axy.y, ddz = rz - azq.x;
+      const double yz2 = fma(ddy, ddy, ddz * ddz);
+      double r2[V], ir[V], ir2[V];
 #pragma unroll
-      for (int v = 0; v < M; ++v) {  // LJ, cal_LJ.cu:56-81
+      for (int j = 0; j < V; ++j) {
+        const double ddx = rx + j * dx - axy.x;
+        r2[j] = fma(ddx, ddx, yz2);
+        ir[j] = rsqrt(r2[j]);
+        ir2[j] = ir[j] * ir[j];
+      }
+#pragma unroll
+      for (int v = 0; v < M; ++v) {
         if (NS > 0 || v < n) {
-          double rs2 = r2 * ss[v][i];
-          if (rs2 < cut2) rs2 = cut2;
-          double irs6 = 1.0 / (rs2 * rs2 * rs2);
-          lj[v] += se[v][i] * irs6 * (irs6 - 1.0);
+          const double2 se = sse[v][i];
+#pragma unroll
+          for (int j = 0; j < V; ++j) {
+            const double s2 = fmin(se.x * ir2[j], smax);
+            const double s6 = s2 * s2 * s2;
+            lj[j][v] = fma(se.y, fma(s6, s6, -s6), lj[j][v]);
+          }
         }
       }
-      if (coulomb) {  // coulomb, cal_Coulomb.cu:40-62
-        double ra = sqrt(r2);
-        if (ra >= 1.0e-5) {
-          double qr = sq[i] / ra;
-          e += qr;
-          f += qr * (1 - exp(-ra));
-        } else {
-          f += sq[i];
+      if (coulomb) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          if (r2[j] >= 1.0e-10) {  // r >= 1e-5 A
+            const double qr = azq.y * ir[j];
+            const double ra = r2[j] * ir[j];
+            const double em = ra <= 38.0 ? exp(-ra) : 0.0;
+            e[j] += qr;
+            f[j] = fma(qr, 1.0 - em, f[j]);
+          } else {
+            f[j] += azq.y;
+          }
         }
       }
     }
@@ -808,16 +834,18 @@ __global__ void __launch_bounds__(kThreads)
   if (!live) return;
   R *u = (R *)d.u, *fr = (R *)d.fr;
   T *t = (T *)d.t;
-  const double bfr = f * ubeta, bde = e * ubeta;  // betar
-  fr[ip] = (R)bfr;
-  if (fr64) fr64[ip] = bfr;
 #pragma unroll
-  for (int v = 0; v < M; ++v) {
-    if (NS > 0 || v < n) {
-      // set_du, minus the long-range part; init_tuv's t0 = q_v fr is
-      // t_s = 0 on the short-range side
-      u[(long long)v * d.Ns + ip] = (R)(lj[v] * ikbt + d.qv[v] * bde - d.qv[v] * bfr);
-      t[(long long)v * d.Ns + ip] = (T)0;
+  for (int j = 0; j < V; ++j) {
+    const long long q = ip + j;
+    const double bfr = f[j] * ubeta, bde = e[j] * ubeta;  // betar
+    fr[q] = (R)bfr;
+    if (fr64) fr64[q] = bfr;
+#pragma unroll
+    for (int v = 0; v < M; ++v) {
+      if (NS > 0 || v < n) {
+        u[(long long)v * d.Ns + q] = (R)(lj[j][v] * ikbt + d.qv[v] * bde - d.qv[v] * bfr);
+        t[(long long)v * d.Ns + q] = (T)0;
+      }
     }
   }
 }
@@ -1209,7 +1237,8 @@ template <typename P>
 void launch_potential(const Desc &d, const AtomTab &at, double ikbt,
                       double ubeta, const double *dr, int coulomb,
                       double *fr64, cudaStream_t s) {
-  int grid = (int)((d.N + kThreads - 1) / kThreads);
+  const long long thr = (d.N + kPotVox - 1) / kPotVox;
+  int grid = (int)((thr + kThreads - 1) / kThreads);
 #define R3D_POT(NS)                                                        \
   k_potential<P, NS><<<grid, kThreads, 0, s>>>(d, at, ikbt, ubeta, dr[0], \
                                                dr[1], dr[2], coulomb, fr64)

@@ -26,6 +26,12 @@
 #include <omp.h>
 #endif
 
+/* Deterministic parallel sums: the index range is cut into kSumBlocks
+ * fixed blocks, each summed in order, and the block sums are added in block
+ * order, so results do not depend on the thread count or on scheduling. */
+enum { kSumBlocks = 64 };
+static long blk_lo(long n, int b) { return (long)((double)n * b / kSumBlocks); }
+
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
 #endif
@@ -1011,12 +1017,18 @@ double orc_calculate(orc_solver *s) {
     cplx *hu = s->huv + iv * n, *gu = s->guv + iv * n;
     double *tr = s->tr + iv * n;
     fft3_backward(hu, s->grid, s->dkf, s->dir, s->dik, 1.0 / s->volume);
-#pragma omp parallel for schedule(static) reduction(+ : ss)
-    for (long ip = 0; ip < n; ++ip) { /* tr, calculate_cuda.cu:54-60 */
-      gu[ip].re = tr[ip];
-      tr[ip] = hu[ip].re + 1.0 - gu[ip].re;
-      ss += tr[ip] * tr[ip];
+    double part[kSumBlocks];
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < kSumBlocks; ++b) {
+      double acc = 0.0;
+      for (long ip = blk_lo(n, b); ip < blk_lo(n, b + 1); ++ip) { /* tr, calculate_cuda.cu:54-60 */
+        gu[ip].re = tr[ip];
+        tr[ip] = hu[ip].re + 1.0 - gu[ip].re;
+        acc += tr[ip] * tr[ip];
+      }
+      part[b] = acc;
     }
+    for (int b = 0; b < kSumBlocks; ++b) ss += part[b];
   }
   return sqrt(ss / ((double)n * natv));
 }
@@ -1067,15 +1079,31 @@ static void mix_an2(orc_solver *s) {
       double s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
       const double *tr = s->tr + iv * n, *r0 = s->rp + iv * n,
                    *r1 = s->rp + niv + iv * n;
-#pragma omp parallel for schedule(static) reduction(+ : s0, s1, s2, s3, s4)
-      for (long ip = 0; ip < n; ++ip) {
-        double t1 = tr[ip] - r0[ip];
-        double t2 = tr[ip] - r1[ip];
-        s0 += tr[ip] * t1;
-        s1 += tr[ip] * t2;
-        s2 += t1 * t1;
-        s3 += t1 * t2;
-        s4 += t2 * t2;
+      double part[kSumBlocks][5];
+#pragma omp parallel for schedule(static)
+      for (int b = 0; b < kSumBlocks; ++b) {
+        double q0 = 0, q1 = 0, q2 = 0, q3 = 0, q4 = 0;
+        for (long ip = blk_lo(n, b); ip < blk_lo(n, b + 1); ++ip) {
+          double t1 = tr[ip] - r0[ip];
+          double t2 = tr[ip] - r1[ip];
+          q0 += tr[ip] * t1;
+          q1 += tr[ip] * t2;
+          q2 += t1 * t1;
+          q3 += t1 * t2;
+          q4 += t2 * t2;
+        }
+        part[b][0] = q0;
+        part[b][1] = q1;
+        part[b][2] = q2;
+        part[b][3] = q3;
+        part[b][4] = q4;
+      }
+      for (int b = 0; b < kSumBlocks; ++b) {
+        s0 += part[b][0];
+        s1 += part[b][1];
+        s2 += part[b][2];
+        s3 += part[b][3];
+        s4 += part[b][4];
       }
       double irho = 1.0 / s->rhov[iv];
       c[0] += s0 * irho;
@@ -1168,16 +1196,27 @@ static void mix_anm(orc_solver *s) {
       const double *fk = s->tr + iv * n;
       for (int i = 0; i < m; ++i) {
         const double *fi = s->hf + (long)slot[i] * niv + iv * n;
-        double ci = 0;
-#pragma omp parallel for schedule(static) reduction(+ : ci)
-        for (long ip = 0; ip < n; ++ip) ci += fk[ip] * (fk[ip] - fi[ip]);
+        double ci = 0, part[kSumBlocks];
+#pragma omp parallel for schedule(static)
+        for (int b = 0; b < kSumBlocks; ++b) {
+          double acc = 0.0;
+          for (long ip = blk_lo(n, b); ip < blk_lo(n, b + 1); ++ip)
+            acc += fk[ip] * (fk[ip] - fi[ip]);
+          part[b] = acc;
+        }
+        for (int b = 0; b < kSumBlocks; ++b) ci += part[b];
         c[i] += ci * irho;
         for (int j = 0; j <= i; ++j) {
           const double *fj = s->hf + (long)slot[j] * niv + iv * n;
           double aij = 0;
-#pragma omp parallel for schedule(static) reduction(+ : aij)
-          for (long ip = 0; ip < n; ++ip)
-            aij += (fk[ip] - fi[ip]) * (fk[ip] - fj[ip]);
+#pragma omp parallel for schedule(static)
+          for (int b = 0; b < kSumBlocks; ++b) {
+            double acc = 0.0;
+            for (long ip = blk_lo(n, b); ip < blk_lo(n, b + 1); ++ip)
+              acc += (fk[ip] - fi[ip]) * (fk[ip] - fj[ip]);
+            part[b] = acc;
+          }
+          for (int b = 0; b < kSumBlocks; ++b) aij += part[b];
           A[i * m + j] += aij * irho;
         }
       }

@@ -1,0 +1,84 @@
+"""Golden fixtures for the two solver features the reference does not have --
+the history-m Anderson mixer and the PSE-n closure -- produced by the FP64 CPU
+oracle (the oracle's AN2/KH/HNC path is pinned to the reference's own outputs
+by tests/test_oracle.py; these extensions share that path and are pinned only
+to the oracle itself):
+
+    tests/golden/oracle/<case>.json      deck, closure, mixer, steps, status
+    tests/golden/oracle/<case>.xmu       the oracle's .xmu
+    tests/golden/oracle/<case>_guv.npz   g at 4096 seeded voxels per site,
+                                         plus per-site sum g and sum g^2
+
+    python tests/golden/make_oracle_fixtures.py
+"""
+import gzip
+import json
+import os
+import shutil
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+
+KH, HNC, PSE = 0, 1, 2
+AN2, ANM = 0, 1
+
+# case -> (reference deck, closure, pse_n, mixer, history, damping)
+CASES = {
+    "c1_anm10": ("c1", KH, 1, ANM, 10, 0.3),
+    "c1_pse2_anm10": ("c1", PSE, 2, ANM, 10, 0.3),
+    "s_rect_pse3_anm10": ("s_rect", PSE, 3, ANM, 10, 0.3),
+    "s64kh_pse2": ("s64kh", PSE, 2, AN2, 2, -1.0),
+    "s64nacl_anm10": ("s64nacl", KH, 1, ANM, 10, 0.3),
+}
+SOLVENTS = ["h2o_vv", "naclaq_vv", "kclaq_vv", "ctip3p"]
+
+
+def materialise(deck, d):
+    inp = shutil.copyfile(os.path.join(HERE, "ref", deck + ".inp"), os.path.join(d, deck + ".inp"))
+    txt = open(inp).read()
+    for k in SOLVENTS:
+        if k + ".xvk" in txt:
+            xvk = os.path.join(d, k + ".xvk")
+            with gzip.open(os.path.join(HERE, k + ".xvk.gz"), "rb") as fi, open(xvk, "wb") as fo:
+                shutil.copyfileobj(fi, fo)
+            return inp, xvk
+    raise KeyError(deck)
+
+
+def main(only=None):
+    import oracle as O
+    dst = os.path.join(HERE, "oracle")
+    os.makedirs(dst, exist_ok=True)
+    tmp = tempfile.mkdtemp()
+    for case, (deck, clos, pse_n, mixer, hist, damp) in CASES.items():
+        if only and case not in only:
+            continue
+        inp, xvk = materialise(deck, tmp)
+        o = O.Oracle(inp, xvk=xvk)
+        o.set_closure(clos, pse_n)
+        if mixer == ANM:
+            o.set_mixer(mixer, hist, damp)  # AN2 keeps the deck's (count, m, mp)
+        o.initialize()
+        steps, rms, status = o.iterate()
+        xmu = os.path.join(dst, case + ".xmu")
+        o.write_xmu(xmu)
+        meta = dict(case=case, deck=deck, closure=clos, pse_n=pse_n, mixer=mixer,
+                    history=hist, damping=damp, steps=steps, rms=rms, status=status)
+        json.dump(meta, open(os.path.join(dst, case + ".json"), "w"), indent=1)
+        g = o.get("g")
+        flat = g.reshape(g.shape[0], -1)
+        rng = np.random.default_rng(12345)
+        idx = np.sort(rng.choice(flat.shape[1], size=min(4096, flat.shape[1]), replace=False))
+        np.savez_compressed(os.path.join(dst, case + "_guv.npz"), shape=np.array(g.shape),
+                            idx=idx, g=flat[:, idx], sum=flat.sum(axis=1),
+                            sum2=(flat * flat).sum(axis=1))
+        print(case, status, steps, rms, flush=True)
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or None)

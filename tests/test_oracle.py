@@ -95,3 +95,20 @@ def test_oracle_fft_is_the_shifted_transform(shape):
     back = O.fft3d(F, box, +1)
     np.testing.assert_allclose(back.real, f, atol=1e-12)
     np.testing.assert_allclose(back.imag, 0, atol=1e-12)
+
+
+def test_oracle_reproduces_extension_fixture(refcase, tmp_path):
+    """The oracle's sums are order-fixed (thread-count independent), so it
+    reproduces its own PSE-3 / history-10 fixture exactly."""
+    gold = os.path.join(os.path.dirname(__file__), "golden", "oracle")
+    meta = json.load(open(os.path.join(gold, "s_rect_pse3_anm10.json")))
+    inp, xvk = refcase(meta["deck"])
+    o = O.Oracle(inp, xvk=xvk)
+    o.set_closure(meta["closure"], meta["pse_n"])
+    o.set_mixer(meta["mixer"], meta["history"], meta["damping"])
+    o.initialize()
+    steps, rms, status = o.iterate()
+    assert (steps, status) == (meta["steps"], meta["status"])
+    out = tmp_path / "o.xmu"
+    o.write_xmu(str(out))
+    assert out.read_text() == open(os.path.join(gold, "s_rect_pse3_anm10.xmu")).read()
