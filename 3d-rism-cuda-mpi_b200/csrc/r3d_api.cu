@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -61,6 +62,7 @@ void launch_zoz(Batch, int, size_t, cudaStream_t, int, int);
 template <typename P>
 void launch_inv_x(Batch, int, size_t, cudaStream_t, int, void *, int);
 void launch_reduce(const Desc *, const int *, int, int, cudaStream_t);
+void launch_ctl_gather(const Desc *, int, double *, cudaStream_t);
 template <typename P>
 void launch_mix_an2(Batch, int, cudaStream_t);
 template <typename P>
@@ -529,6 +531,39 @@ static void pass_ix(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mo
 // CTAs of the iteration's IX (each writes one row of the partials k_reduce sums)
 static int iter_ix_ctas(const Geo &g) { return g.ixb_pc ? g.ixb_ctas : g.ix_ctas; }
 
+// Launch prefixes of ns solves that share one geometry (a device int block):
+// the CTA prefixes of the x, y, z, IX, mix and ANM-dot passes (ns + 1 entries
+// each: solve i owns CTAs [p[i], p[i+1]) of the launch), then every solve's
+// IX CTA count (rows of partials k_reduce sums) and ANM dot CTA count.
+enum { PF_X, PF_Y, PF_Z, PF_IX, PF_MIX, PF_DOT, PF_IXC, PF_DOTC };
+static int pf_off(int ns, int k) {
+  return k <= PF_IXC ? k * (ns + 1) : PF_IXC * (ns + 1) + ns;
+}
+static int pf_len(int ns) { return PF_IXC * (ns + 1) + 2 * ns; }
+static std::vector<int> make_prefix(const Geo &g, int ns) {
+  std::vector<int> v(pf_len(ns));
+  const int per[6] = {g.tiles_x, g.tiles_y, g.tiles_z, iter_ix_ctas(g), g.mix_ctas, g.dot_ctas};
+  for (int k = 0; k < 6; ++k)
+    for (int i = 0; i <= ns; ++i) v[pf_off(ns, k) + i] = i * per[k];
+  for (int i = 0; i < ns; ++i) {
+    v[pf_off(ns, PF_IXC) + i] = iter_ix_ctas(g);
+    v[pf_off(ns, PF_DOTC) + i] = g.dot_ctas;
+  }
+  return v;
+}
+// Grid sizes of one launch over ns solves of geometry g.
+static Geo scaled(const Geo &g, int ns) {
+  Geo s = g;
+  s.tiles_x *= ns;
+  s.tiles_y *= ns;
+  s.tiles_z *= ns;
+  s.ix_ctas *= ns;
+  s.ixb_ctas *= ns;
+  s.mix_ctas *= ns;
+  s.dot_ctas *= ns;
+  return s;
+}
+
 // Twiddle tables of the compile-time engine for one grid: [twx | pwx | twy |
 // pwy | twz | pwz]; FP64 always (refresh pipeline), FP32 as well for the
 // mixed path.  Sets the table pointers of d (grid type of the descriptor).
@@ -674,7 +709,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = dalloc(c, (void **)&rmslog, (size_t)(p.maxstep + 1) * 8))) return rc;
   if ((rc = dalloc(c, (void **)&c->ctl, sizeof(Ctl)))) return rc;
   if ((rc = dalloc(c, (void **)&c->ddesc, sizeof(Desc)))) return rc;
-  if ((rc = dalloc(c, (void **)&c->dprefix, 16 * sizeof(int)))) return rc;
+  if ((rc = dalloc(c, (void **)&c->dprefix, pf_len(1) * sizeof(int)))) return rc;
   CK(cudaMemsetAsync(c->hist_a, 0, slots * n * N * ha, s));
   CK(cudaMemsetAsync(c->hist_b, 0, slots * n * N * hb, s));
   CK(cudaMemsetAsync(c->res, 0, n * N * sizeof(R), s));
@@ -822,11 +857,8 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     h.count_left = p.count;
     CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
     CK(copy_h2d(c, c->ddesc, &d, sizeof(Desc), s));
-    // prefixes: x, y, z, ix, mix passes; ix / dot CTA counts; dot pass
-    const int ixc = iter_ix_ctas(c->geo);
-    int pre[16] = {0, c->geo.tiles_x, 0, c->geo.tiles_y, 0, c->geo.tiles_z, 0, ixc,
-                   0, c->geo.mix_ctas, ixc, c->geo.dot_ctas, 0, c->geo.dot_ctas, 0, 0};
-    CK(copy_h2d(c, c->dprefix, pre, sizeof(pre), s));
+    const std::vector<int> pre = make_prefix(c->geo, 1);
+    CK(copy_h2d(c, c->dprefix, pre.data(), pre.size() * sizeof(int), s));
     CK(cudaStreamSynchronize(s));
   }
   // the attribute is a per-function limit shared by every context: always
@@ -873,44 +905,61 @@ extern "C" int r3d_initialize(r3d_ctx *c) {
 }
 
 // --------------------------------------------------------------- iterate
+// Solves of one geometry whose iteration kernels are launched together.
+struct Group {
+  Desc rep;          // host descriptor of the first solve (shape fields)
+  Geo geo;           // geometry of one solve
+  const Desc *ddescs;  // device descriptors [ns]
+  const int *dpf;    // device prefix block (make_prefix)
+  int ns;
+  int mixer;
+};
+static Group single_group(const r3d_ctx *c) {
+  return Group{c->desc, c->geo, c->ddesc, c->dprefix, 1, c->mixer};
+}
+
 // stage: 0 = full iteration (evaluate, decide, mix), 1 = evaluate only
-// (calculate), 2 = mix only (anderson)
+// (calculate), 2 = mix only (anderson).  Returns the kernels launched.
 template <typename P>
-static void enqueue(r3d_ctx *c, int stage) {
-  cudaStream_t s = c->stream;
-  const int *pf = c->dprefix;
-  Batch bx{c->ddesc, pf + 0, 1}, by{c->ddesc, pf + 2, 1}, bz{c->ddesc, pf + 4, 1},
-      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1}, bdot{c->ddesc, pf + 12, 1};
+static int enqueue_group(const Group &G, cudaStream_t s, int stage) {
+  const int ns = G.ns;
+  const Geo g = scaled(G.geo, ns);
+  const Desc &d = G.rep;
+  auto B = [&](int k) { return Batch{G.ddescs, G.dpf + pf_off(ns, k), ns}; };
+  const int *ixc = G.dpf + pf_off(ns, PF_IXC), *dotc = G.dpf + pf_off(ns, PF_DOTC);
   int k = 0;
   if (stage != 2) {
-    const Desc &d = c->desc;
-    const Geo &g = c->geo;
-    pass_fx<P>(d, g, bx, s, 1, nullptr);
-    pass_fy<P>(d, g, by, s, -1, 1);
-    pass_zoz<P>(d, g, bz, s, 2, 1);
-    pass_fy<P>(d, g, by, s, 1, 1);
-    pass_ix<P>(d, g, bix, s, 1, nullptr);
+    pass_fx<P>(d, g, B(PF_X), s, 1, nullptr);
+    pass_fy<P>(d, g, B(PF_Y), s, -1, 1);
+    pass_zoz<P>(d, g, B(PF_Z), s, 2, 1);
+    pass_fy<P>(d, g, B(PF_Y), s, 1, 1);
+    pass_ix<P>(d, g, B(PF_IX), s, 1, nullptr);
     k += 5;
-    if (c->mixer == MIX_ANM) {
-      launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, pf + 11, 1, s, 0);
+    if (G.mixer == MIX_ANM) {
+      launch_anm<P>(B(PF_DOT), g.dot_ctas, G.ddescs, dotc, ns, s, 0);
       ++k;
     }
-    launch_reduce(c->ddesc, pf + 10, 1, stage == 0 ? 0 : 2, s);
+    launch_reduce(G.ddescs, ixc, ns, stage == 0 ? 0 : 2, s);
     ++k;
   } else {
-    launch_reduce(c->ddesc, pf + 10, 1, 1, s);
+    launch_reduce(G.ddescs, ixc, ns, 1, s);
     ++k;
   }
   if (stage != 1) {
-    if (c->mixer == MIX_AN2) {
-      launch_mix_an2<P>(bmx, c->geo.mix_ctas, s);
+    if (G.mixer == MIX_AN2) {
+      launch_mix_an2<P>(B(PF_MIX), g.mix_ctas, s);
       ++k;
     } else {
-      launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 1);
-      launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 2);
+      launch_anm<P>(B(PF_MIX), g.mix_ctas, G.ddescs, dotc, ns, s, 1);
+      launch_anm<P>(B(PF_MIX), g.mix_ctas, G.ddescs, dotc, ns, s, 2);
       k += 2;
     }
   }
+  return k;
+}
+template <typename P>
+static void enqueue(r3d_ctx *c, int stage) {
+  const int k = enqueue_group<P>(single_group(c), c->stream, stage);
   if (stage == 0) c->kernels_per_iter = k;
 }
 
@@ -1018,8 +1067,10 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   cudaStream_t s = c->stream;
   const int *pf = c->dprefix;
   const double n = d.n, N = (double)d.N, rs = sizeof(R), ts = sizeof(T);
-  Batch bx{c->ddesc, pf + 0, 1}, by{c->ddesc, pf + 2, 1}, bz{c->ddesc, pf + 4, 1},
-      bix{c->ddesc, pf + 6, 1}, bmx{c->ddesc, pf + 8, 1}, bdot{c->ddesc, pf + 12, 1};
+  Batch bx{c->ddesc, pf + pf_off(1, PF_X), 1}, by{c->ddesc, pf + pf_off(1, PF_Y), 1},
+      bz{c->ddesc, pf + pf_off(1, PF_Z), 1}, bix{c->ddesc, pf + pf_off(1, PF_IX), 1},
+      bmx{c->ddesc, pf + pf_off(1, PF_MIX), 1}, bdot{c->ddesc, pf + pf_off(1, PF_DOT), 1};
+  const int *ixc = pf + pf_off(1, PF_IXC), *dotc = pf + pf_off(1, PF_DOTC);
   // keep t: the kernels below run out of sequence and overwrite it
   void *tsave = nullptr;
   const size_t tb = (size_t)d.n * d.Ns * sizeof(T);
@@ -1062,19 +1113,19 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
         [&] { pass_ix<P>(d, c->geo, bix, s, 1, nullptr); });
   if (c->mixer == MIX_AN2) {
     timed("reduce", (double)iter_ix_ctas(c->geo) * kPartials * 8,
-          [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
+          [&] { launch_reduce(c->ddesc, ixc, 1, 1, s); });
     const bool picard = h.count_left > 0;
     timed("mix_an2", picard ? n * N * (3 * ts + 2 * rs) : n * N * (5 * ts + 4 * rs),
           [&] { launch_mix_an2<P>(bmx, c->geo.mix_ctas, s); });
   } else {
     timed("anm_dots", n * N * rs * (h.hcount + 1),
-          [&] { launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, pf + 11, 1, s, 0); });
+          [&] { launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, dotc, 1, s, 0); });
     timed("reduce", (double)iter_ix_ctas(c->geo) * kPartials * 8,
-          [&] { launch_reduce(c->ddesc, pf + 10, 1, 1, s); });
-    timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 1); });
+          [&] { launch_reduce(c->ddesc, ixc, 1, 1, s); });
+    timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, dotc, 1, s, 1); });
     const int m = std::min(h.hcount, c->history);
     timed("mix_anm", n * N * (rs + ts + m * ts + rs + ts + ts),
-          [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, pf + 11, 1, s, 2); });
+          [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, dotc, 1, s, 2); });
   }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->t, tsave, tb, cudaMemcpyDeviceToDevice, s));
@@ -1506,4 +1557,215 @@ extern "C" int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
   if (rc) g_last_error = c->err;
   r3d_destroy(c);
   return rc;
+}
+
+// ----------------------------------------------------------------- batches
+// Independent solves iterated together: the solves of one geometry (grid,
+// sites, mixer) form a group, each kernel of an iteration covers every solve
+// of its group (a CTA finds its solve in the group's prefix block), and one
+// CUDA graph holds one iteration of all groups.  Solves that have converged,
+// diverged or hit maxstep are skipped by every kernel while the others run.
+struct r3d_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<r3d_ctx *> ctxs;
+  std::vector<Group> groups;
+  std::vector<void *> gmem;    // device blocks of the groups
+  std::vector<int> order;      // gathered index -> ctxs index
+  double *dsum = nullptr, *hsum = nullptr;  // gathered control words
+  cudaGraphExec_t gexec = nullptr;
+  bool dirty = true;
+  int kernels_per_iter = 0;
+};
+
+static int bfail(int code, const std::string &m) {
+  g_last_error = "batch: " + m;
+  return code;
+}
+#define BCK(x)                                                              \
+  do {                                                                      \
+    cudaError_t e_ = (x);                                                   \
+    if (e_ != cudaSuccess) return bfail(R3D_ECUDA, cudaGetErrorString(e_)); \
+  } while (0)
+
+static void batch_release(r3d_batch *b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  b->gexec = nullptr;
+  for (void *p : b->gmem) cudaFree(p);
+  b->gmem.clear();
+  b->groups.clear();
+  if (b->dsum) cudaFree(b->dsum);
+  if (b->hsum) cudaFreeHost(b->hsum);
+  b->dsum = b->hsum = nullptr;
+}
+
+extern "C" int r3d_batch_create(int device, r3d_batch **out) {
+  if (!out) return bfail(R3D_EINVAL, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return bfail(R3D_EINVAL, "no such device");
+  BCK(cudaSetDevice(device));
+  r3d_batch *b = new r3d_batch;
+  b->device = device;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return bfail(R3D_ECUDA, "stream");
+  }
+  *out = b;
+  return R3D_OK;
+}
+
+extern "C" int r3d_batch_add(r3d_batch *b, r3d_ctx *c) {
+  if (!b || !c) return bfail(R3D_EINVAL, "NULL argument");
+  if (!c->initialized) return bfail(R3D_ESTATE, "context not initialized");
+  if (c->opts.device != b->device) return bfail(R3D_EINVAL, "context on another device");
+  if (!b->ctxs.empty() && b->ctxs[0]->fp64 != c->fp64)
+    return bfail(R3D_EINVAL, "contexts of one batch must share the precision");
+  if (std::find(b->ctxs.begin(), b->ctxs.end(), c) != b->ctxs.end())
+    return bfail(R3D_EINVAL, "context already in the batch");
+  b->ctxs.push_back(c);
+  b->dirty = true;
+  return R3D_OK;
+}
+
+extern "C" int r3d_batch_destroy(r3d_batch *b) {
+  if (!b) return R3D_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_release(b);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return R3D_OK;
+}
+
+// Groups, their device blocks and the graph of one iteration.
+template <typename P>
+static int batch_build(r3d_batch *b) {
+  batch_release(b);
+  std::vector<std::vector<int>> members;
+  std::vector<std::array<long long, 6>> keys;
+  for (int i = 0; i < (int)b->ctxs.size(); ++i) {
+    const r3d_ctx *c = b->ctxs[i];
+    const std::array<long long, 6> key{c->desc.nx, c->desc.ny, c->desc.nz, c->desc.n,
+                                       c->mixer, c->mixer == MIX_ANM ? c->history : 0};
+    size_t g = std::find(keys.begin(), keys.end(), key) - keys.begin();
+    if (g == keys.size()) {
+      keys.push_back(key);
+      members.emplace_back();
+    }
+    members[g].push_back(i);
+  }
+  cudaStream_t s = b->stream;
+  b->order.clear();
+  for (auto &m : members) {
+    const int ns = (int)m.size();
+    const r3d_ctx *c0 = b->ctxs[m[0]];
+    std::vector<Desc> ds(ns);
+    for (int i = 0; i < ns; ++i) ds[i] = b->ctxs[m[i]]->desc;
+    const std::vector<int> pre = make_prefix(c0->geo, ns);
+    const size_t db = ((ns * sizeof(Desc) + 255) / 256) * 256;
+    void *mem = nullptr;
+    BCK(cudaMalloc(&mem, db + pre.size() * sizeof(int)));
+    b->gmem.push_back(mem);
+    BCK(cudaMemcpyAsync(mem, ds.data(), ns * sizeof(Desc), cudaMemcpyHostToDevice, s));
+    BCK(cudaMemcpyAsync((char *)mem + db, pre.data(), pre.size() * sizeof(int),
+                        cudaMemcpyHostToDevice, s));
+    b->groups.push_back(Group{c0->desc, c0->geo, (const Desc *)mem,
+                              (const int *)((char *)mem + db), ns, c0->mixer});
+    for (int i : m) b->order.push_back(i);
+  }
+  const size_t nsol = b->ctxs.size();
+  BCK(cudaMalloc((void **)&b->dsum, nsol * 4 * sizeof(double)));
+  BCK(cudaMallocHost((void **)&b->hsum, nsol * 4 * sizeof(double)));
+  BCK(cudaStreamSynchronize(s));
+  cudaGraph_t g;
+  BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int k = 0;
+  for (const Group &G : b->groups) k += enqueue_group<P>(G, s, 0);
+  BCK(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(&b->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return bfail(R3D_ECUDA, std::string("graph: ") + cudaGetErrorString(e));
+  b->kernels_per_iter = k;
+  b->dirty = false;
+  return R3D_OK;
+}
+
+template <typename P>
+static int batch_run(r3d_batch *b, int *iterations, double *ms_out) {
+  cudaStream_t s = b->stream;
+  // fresh mixer state of every solve (AN2::initialize inside iterate)
+  for (r3d_ctx *c : b->ctxs) {
+    int rc = reset_mixer(c);
+    if (rc) return bfail(rc, c->err);
+    c->next_refresh = 1e-3;
+  }
+  if (b->dirty) {
+    int rc = batch_build<P>(b);
+    if (rc) return rc;
+  }
+  const int nsol = (int)b->ctxs.size();
+  int maxstep = 0;
+  for (r3d_ctx *c : b->ctxs) maxstep = std::max(maxstep, c->prob.maxstep);
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  BCK(cudaEventRecord(e0, s));
+  const int chunk = 8;
+  int iters = 0;
+  for (;;) {
+    for (int i = 0; i < chunk; ++i) BCK(cudaGraphLaunch(b->gexec, s));
+    iters += chunk;
+    int off = 0;
+    for (const Group &G : b->groups) {
+      launch_ctl_gather(G.ddescs, G.ns, b->dsum + 4 * off, s);
+      off += G.ns;
+    }
+    BCK(cudaMemcpyAsync(b->hsum, b->dsum, nsol * 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BCK(cudaStreamSynchronize(s));
+    bool running = false;
+    for (int j = 0; j < nsol; ++j) {
+      r3d_ctx *c = b->ctxs[b->order[j]];
+      const double *w = b->hsum + 4 * j;
+      if (w[3] != 0) return bfail(R3D_ECUDA, "a kernel's bounded wait for a staged copy ran out");
+      if ((int)w[0] != RUNNING) continue;
+      running = true;
+      if (!c->fp64 && w[2] < c->next_refresh) {
+        // mixed path: move the converged part of c into the FP64 reference
+        int rc = refresh<PMix>(c, false);
+        if (rc) return bfail(rc, c->err);
+        c->next_refresh *= 1e-2;
+      }
+    }
+    if (!running || iters > maxstep + chunk) break;
+  }
+  BCK(cudaEventRecord(e1, s));
+  BCK(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int most = 0;
+  for (int j = 0; j < nsol; ++j) most = std::max(most, (int)b->hsum[4 * j + 1]);
+  for (r3d_ctx *c : b->ctxs) c->ms_per_iter = most > 0 ? ms / most : 0;
+  if (iterations) *iterations = most;
+  if (ms_out) *ms_out = ms;
+  return R3D_OK;
+}
+
+extern "C" int r3d_batch_iterate(r3d_batch *b, int *iterations, double *ms) {
+  if (!b) return bfail(R3D_EINVAL, "batch is NULL");
+  if (b->ctxs.empty()) return bfail(R3D_ESTATE, "empty batch");
+  BCK(cudaSetDevice(b->device));
+  for (r3d_ctx *c : b->ctxs) BCK(cudaStreamSynchronize(c->stream));
+  return b->ctxs[0]->fp64 ? batch_run<P64>(b, iterations, ms) : batch_run<PMix>(b, iterations, ms);
+}
+
+extern "C" int r3d_batch_info(const r3d_batch *b, int *solves, int *groups, int *kernels_per_iter) {
+  if (!b) return bfail(R3D_EINVAL, "batch is NULL");
+  if (solves) *solves = (int)b->ctxs.size();
+  if (groups) *groups = (int)b->groups.size();
+  if (kernels_per_iter) *kernels_per_iter = b->kernels_per_iter;
+  return R3D_OK;
 }

@@ -1219,6 +1219,20 @@ void launch_reduce(const Desc *d, const int *ctas, int ns, int force,
                    cudaStream_t s) {
   k_reduce<<<ns, kThreads, 0, s>>>(d, ctas, force);
 }
+// Control words of ns solves, gathered for one read-back:
+// out[4 i ..] = status, completed steps, rms, error word.
+__global__ void k_ctl_gather(const Desc *descs, int ns, double *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+    const Ctl *c = descs[i].ctl;
+    out[4 * i + 0] = c->status;
+    out[4 * i + 1] = c->step;
+    out[4 * i + 2] = c->rms;
+    out[4 * i + 3] = c->err;
+  }
+}
+void launch_ctl_gather(const Desc *d, int ns, double *out, cudaStream_t s) {
+  k_ctl_gather<<<(ns + kThreads - 1) / kThreads, kThreads, 0, s>>>(d, ns, out);
+}
 template <typename P>
 void launch_mix_an2(Batch b, int grid, cudaStream_t s) {
   k_mix_an2<P><<<grid, kThreads, 0, s>>>(b);

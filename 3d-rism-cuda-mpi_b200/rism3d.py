@@ -32,7 +32,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
            "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
-           "r3d_fft3d_noalloc"]
+           "r3d_fft3d_noalloc", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
+           "r3d_batch_info", "r3d_batch_destroy"]
 
 
 class Opts(ctypes.Structure):
@@ -74,6 +75,11 @@ def _load():
                                ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
         "r3d_fft3d_noalloc": [ci, ci, ci, ci, dp, ci, vp, vp, vp],
+        "r3d_batch_create": [ci, ctypes.POINTER(vp)],
+        "r3d_batch_add": [vp, vp],
+        "r3d_batch_iterate": [vp, ip, dp],
+        "r3d_batch_info": [vp, ip, ip, ip],
+        "r3d_batch_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -260,3 +266,43 @@ def fft3d(data, box, direction, precision="fp64", device=0):
     if rc:
         raise R3DError(rc, lib.r3d_last_error(None).decode())
     return out.reshape(nz, ny, nx)
+
+
+class Batch:
+    """Many initialized RISM3D solves iterated together (r3d_batch_*): every
+    kernel of an iteration covers all solves of one geometry.  Results are
+    read from the RISM3D objects as usual."""
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        rc = lib.r3d_batch_create(device, ctypes.byref(h))
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+        self.h = h
+        self.solves = []
+
+    def _check(self, rc):
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+
+    def add(self, solve):
+        self._check(lib.r3d_batch_add(self.h, solve.h))
+        self.solves.append(solve)
+
+    def iterate(self):
+        """-> (largest step count, device ms of the whole loop)"""
+        it, ms = ctypes.c_int(), ctypes.c_double()
+        self._check(lib.r3d_batch_iterate(self.h, ctypes.byref(it), ctypes.byref(ms)))
+        return it.value, ms.value
+
+    def info(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(lib.r3d_batch_info(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return {"solves": a.value, "groups": b.value, "kernels_per_iter": c.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.r3d_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close

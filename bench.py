@@ -297,6 +297,7 @@ def run_gpu(args, rank, world, local):
                     "d2h_bytes_per_step": d2h / max(steps, 1),
                     "solve_s": e2e_s, "solves_per_s": world / e2e_s,
                     "solves_timed": len(warm), "cold_solve_s": cold_s,
+                    "warm_solves_s": [w[0] for w in warm],
                     "phases_s": phases},
             "gpu_launches": kpi * args.steps,
             "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
@@ -352,7 +353,7 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--grid", type=int, default=256, help="profiling only: grid size")
     ap.add_argument("--atoms", type=int, default=2000, help="profiling only: solute atoms")
-    ap.add_argument("--e2e-reps", type=int, default=2, help="warm end-to-end solves timed")
+    ap.add_argument("--e2e-reps", type=int, default=3, help="warm end-to-end solves timed")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
     args = ap.parse_args()

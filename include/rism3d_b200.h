@@ -204,6 +204,33 @@ int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
 int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
                       int dir, const double *d_in, double *d_out, void *stream);
 
+/* ---- batches of independent solves --------------------------------------
+ * The reference runs one solve per process (main.cu:63-65).  A batch iterates
+ * many initialized contexts together: the solves of one geometry (grid,
+ * solvent sites, mixer) share every kernel launch of an iteration, which is
+ * what makes many small solves (48^3-128^3 grids, a few ms of work each) use
+ * the whole GPU.  Each solve keeps its own closure, tolerance, maxstep and
+ * mixer parameters and stops on its own; results are read per context
+ * (r3d_status, r3d_thermo, r3d_write_xmu, r3d_get_grid).  All contexts of a
+ * batch share the device and the precision; a context belongs to at most one
+ * batch at a time and must not be used on its own during r3d_batch_iterate.
+ * Errors are reported by r3d_last_error(NULL). */
+typedef struct r3d_batch r3d_batch;
+int r3d_batch_create(int device, r3d_batch **out);
+/* Adds an initialized context (not owned: destroy it yourself, after the
+ * batch). */
+int r3d_batch_add(r3d_batch *b, r3d_ctx *ctx);
+/* RISM3D::iterate (iterate.cu:6-107) for every solve of the batch at once:
+ * fresh mixer state, iterations until every solve has converged, diverged
+ * or reached its maxstep.  iterations: the largest step count of any solve;
+ * ms: device time of the whole loop. */
+int r3d_batch_iterate(r3d_batch *b, int *iterations, double *ms);
+/* solves, geometry groups (launches per kernel of an iteration), kernels per
+ * iteration of the batch's graph (after the first r3d_batch_iterate). */
+int r3d_batch_info(const r3d_batch *b, int *solves, int *groups, int *kernels_per_iter);
+/* Frees the batch's own buffers; its contexts stay valid. */
+int r3d_batch_destroy(r3d_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,86 @@
+"""Batches of independent solves (r3d_batch_*): every solve of a batch ends
+exactly where it ends alone -- same step count, byte-identical .xmu, identical
+g -- because a batched launch runs each solve's tiles with the solve's own
+geometry and reductions.  Mixed geometries, closures, mixers and a diverging
+solve share one batch."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# (reference deck, closure, pse_n, mixer, history, damping); None = the deck's own
+SOLVES = [("s64kh", None), ("c1", None), ("s64nacl", None), ("s_rect", None),
+          ("c1", (2, 2, 1, 10, 0.3)), ("s64kh", (2, 2, 0, 0, 0)), ("s64hnc", None),
+          ("c1", (0, 1, 1, 10, 0.3))]
+
+
+def _make(R, refcase, deck, over, prec):
+    inp, xvk = refcase(deck)
+    s = R.RISM3D(precision=prec)
+    s.load(inp, xvk=xvk)
+    if over:
+        clos, n, mixer, hist, damp = over
+        s.set_closure(clos, n)
+        if mixer == R.MIX_ANM:
+            s.set_mixer(mixer, hist, damp)
+    s.initialize()
+    return s
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_equals_solo(refcase, tmp_path, prec):
+    import rism3d as R
+    solo = []
+    for i, (deck, over) in enumerate(SOLVES):
+        s = _make(R, refcase, deck, over, prec)
+        st = s.iterate()
+        p = tmp_path / f"solo{i}.xmu"
+        if st[2] != "diverged":
+            s.output(str(p))
+        solo.append((st, p.read_text() if st[2] != "diverged" else None,
+                     s.get("g") if st[2] != "diverged" else None))
+        s.close()
+    ctxs = [_make(R, refcase, deck, over, prec) for deck, over in SOLVES]
+    b = R.Batch()
+    for s in ctxs:
+        b.add(s)
+    iters, ms = b.iterate()
+    info = b.info()
+    assert info["solves"] == len(SOLVES) and info["groups"] >= 3
+    assert iters == max(st[0] for st, _, _ in solo)
+    for i, s in enumerate(ctxs):
+        st, xmu, g = solo[i]
+        steps, rms, status = s.status()
+        assert (steps, status) == (st[0], st[2]), SOLVES[i]
+        if status == "diverged":
+            continue
+        p = tmp_path / f"batch{i}.xmu"
+        s.output(str(p))
+        assert p.read_text() == xmu, SOLVES[i]
+        assert np.array_equal(s.get("g"), g), SOLVES[i]
+    b.close()
+    for s in ctxs:
+        s.close()
+
+
+def test_batch_rejects_bad_members(refcase):
+    import rism3d as R
+    inp, xvk = refcase("s64kh")
+    a = R.RISM3D(precision="fp64")
+    a.load(inp, xvk=xvk)
+    b = R.Batch()
+    with pytest.raises(R.R3DError):
+        b.add(a)  # not initialized
+    a.initialize()
+    b.add(a)
+    with pytest.raises(R.R3DError):
+        b.add(a)  # twice
+    m = R.RISM3D(precision="mixed")
+    m.initialize(inp, xvk=xvk)
+    with pytest.raises(R.R3DError):
+        b.add(m)  # another precision
+    b.close()
+    a.close()
+    m.close()
