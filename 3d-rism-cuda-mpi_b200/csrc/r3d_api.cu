@@ -110,7 +110,7 @@ constexpr int kNumSM = 148;
 
 using namespace r3d;
 
-static std::string g_last_error;
+static thread_local std::string g_last_error;  // per calling thread
 namespace r3d {
 void set_last_error(const std::string &m) { g_last_error = m; }
 }  // namespace r3d
@@ -1572,6 +1572,7 @@ struct r3d_batch {
   std::vector<Group> groups;
   std::vector<void *> gmem;    // device blocks of the groups
   std::vector<int> order;      // gathered index -> ctxs index
+  std::vector<std::vector<int>> members;  // per group: ctxs indices
   double *dsum = nullptr, *hsum = nullptr;  // gathered control words
   cudaGraphExec_t gexec = nullptr;
   bool dirty = true;
@@ -1658,6 +1659,7 @@ static int batch_build(r3d_batch *b) {
   }
   cudaStream_t s = b->stream;
   b->order.clear();
+  b->members = members;
   for (auto &m : members) {
     const int ns = (int)m.size();
     const r3d_ctx *c0 = b->ctxs[m[0]];
@@ -1704,6 +1706,14 @@ static int batch_run(r3d_batch *b, int *iterations, double *ms_out) {
   if (b->dirty) {
     int rc = batch_build<P>(b);
     if (rc) return rc;
+  } else {  // closures and controls may have changed since the last run
+    for (size_t g = 0; g < b->groups.size(); ++g) {
+      std::vector<Desc> ds;
+      for (int i : b->members[g]) ds.push_back(b->ctxs[i]->desc);
+      BCK(cudaMemcpyAsync((void *)b->groups[g].ddescs, ds.data(), ds.size() * sizeof(Desc),
+                          cudaMemcpyHostToDevice, s));
+    }
+    BCK(cudaStreamSynchronize(s));
   }
   const int nsol = (int)b->ctxs.size();
   int maxstep = 0;
@@ -1769,3 +1779,4 @@ extern "C" int r3d_batch_info(const r3d_batch *b, int *solves, int *groups, int 
   if (kernels_per_iter) *kernels_per_iter = b->kernels_per_iter;
   return R3D_OK;
 }
+#include "r3d_server.inc"

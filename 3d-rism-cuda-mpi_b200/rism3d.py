@@ -33,12 +33,30 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
            "r3d_fft3d_noalloc", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
-           "r3d_batch_info", "r3d_batch_destroy"]
+           "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
+           "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
+           "r3d_server_destroy"]
+REQ_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed"}
 
 
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int),
                 ("hbm_budget", ctypes.c_ulonglong), ("verbose", ctypes.c_int)]
+
+
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int),
+                ("hbm_budget", ctypes.c_ulonglong), ("max_active", ctypes.c_int),
+                ("chunk", ctypes.c_int), ("closure_ladder", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("steps", ctypes.c_int),
+                ("steps_total", ctypes.c_int), ("natv", ctypes.c_int), ("rms", ctypes.c_double),
+                ("xmu", ctypes.c_double * 32), ("xmu2", ctypes.c_double * 16),
+                ("pmv", ctypes.c_double), ("pressure", ctypes.c_double),
+                ("queued_s", ctypes.c_double), ("admitted_s", ctypes.c_double),
+                ("finished_s", ctypes.c_double), ("error", ctypes.c_char * 256)]
 
 
 def _load():
@@ -80,6 +98,13 @@ def _load():
         "r3d_batch_iterate": [vp, ip, dp],
         "r3d_batch_info": [vp, ip, ip, ip],
         "r3d_batch_destroy": [vp],
+        "r3d_server_create": [ctypes.POINTER(ServerOpts), ctypes.POINTER(vp)],
+        "r3d_server_submit": [vp, cs, cs, ctypes.POINTER(ctypes.c_longlong)],
+        "r3d_server_poll": [vp, ctypes.c_longlong, ctypes.POINTER(Result)],
+        "r3d_server_wait": [vp, ctypes.c_longlong, cd, ctypes.POINTER(Result)],
+        "r3d_server_write_xmu": [vp, ctypes.c_longlong, cs],
+        "r3d_server_release": [vp, ctypes.c_longlong],
+        "r3d_server_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -303,6 +328,62 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             lib.r3d_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+
+class Server:
+    """Continuous batching of submitted decks on one device (r3d_server_*)."""
+
+    def __init__(self, device=0, precision="mixed", hbm_budget=0, max_active=0, chunk=8,
+                 closure_ladder=True):
+        o = ServerOpts(device, FP64 if precision in ("fp64", FP64) else MIXED, hbm_budget,
+                       max_active, chunk, int(closure_ladder))
+        h = ctypes.c_void_p()
+        rc = lib.r3d_server_create(ctypes.byref(o), ctypes.byref(h))
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+
+    def submit(self, inp, xvk=None):
+        t = ctypes.c_longlong()
+        self._check(lib.r3d_server_submit(self.h, inp.encode(), xvk.encode() if xvk else None,
+                                          ctypes.byref(t)))
+        return t.value
+
+    @staticmethod
+    def _dict(r):
+        n = r.natv
+        return {"state": REQ_STATE[r.state], "status": STATUS.get(r.status, "running"),
+                "steps": r.steps, "steps_total": r.steps_total, "rms": r.rms,
+                "xmu": list(r.xmu[:2 * n]), "xmu2": list(r.xmu2[:n]), "pmv": r.pmv,
+                "pressure": r.pressure, "queued_s": r.queued_s, "admitted_s": r.admitted_s,
+                "finished_s": r.finished_s, "error": r.error.decode()}
+
+    def poll(self, ticket):
+        r = Result()
+        self._check(lib.r3d_server_poll(self.h, ticket, ctypes.byref(r)))
+        return self._dict(r)
+
+    def wait(self, ticket, timeout=-1.0):
+        r = Result()
+        self._check(lib.r3d_server_wait(self.h, ticket, timeout, ctypes.byref(r)))
+        return self._dict(r)
+
+    def write_xmu(self, ticket, path):
+        self._check(lib.r3d_server_write_xmu(self.h, ticket, path.encode()))
+
+    def release(self, ticket):
+        self._check(lib.r3d_server_release(self.h, ticket))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.r3d_server_destroy(self.h)
             self.h = None
 
     __del__ = close

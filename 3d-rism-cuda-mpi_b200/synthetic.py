@@ -116,6 +116,57 @@ def config(name, outdir, solvent_dir=None, **over):
     return write_inp(os.path.join(outdir, f"{name}.inp"), sol, **kw)
 
 
+def _extent_grid(sol, sizes, spacing=0.5, buffer=12.0):
+    """Smallest grid of `sizes` whose cell holds the solute's extent plus
+    `buffer` on each side (the largest size when none does)."""
+    ext = float((sol["r"].max(axis=0) - sol["r"].min(axis=0)).max())
+    need = (ext + 2.0 * buffer) / spacing
+    return next((g for g in sizes if g >= need), sizes[-1])
+
+
+def _c1_recipe(nu, seed):
+    """C1's drug-like recipe at C1's density (20 atoms in a 6 A sphere)."""
+    radius = 6.0 * (nu / 20.0) ** (1.0 / 3.0)
+    return make_solute(nu, seed, radius=radius, dmin=1.1, sig=(2.5, 3.8), qsd=0.35)
+
+
+def c4_decks(outdir, count=64, closure="PSE3", solvent="h2o_vv.xvk", mixer=(2, 0.6, 0.2),
+             maxstep=10000):
+    """The batched screen: `count` solutes of U{8..60} atoms, each on the
+    smallest of 48^3/64^3/96^3/128^3 at 0.5 A that holds its extent plus
+    12 A; pure water, PSE-3.  Returns the deck paths."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(SEEDS["c4"])
+    paths = []
+    for i in range(count):
+        nu = int(rng.integers(8, 61))
+        sol = _c1_recipe(nu, SEEDS["c4"] * 1000 + i)
+        g = _extent_grid(sol, (48, 64, 96, 128))
+        paths.append(write_inp(os.path.join(outdir, f"c4_{i:02d}.inp"), sol, (g * 0.5,) * 3,
+                               (g,) * 3, solvent, closure=closure, mixer=mixer, maxstep=maxstep))
+    return paths
+
+
+def c5_requests(outdir, count, seed=None, solvents=("h2o_vv.xvk", "naclaq_vv.xvk"),
+                closures=("KH", "PSE2"), maxstep=10000):
+    """The served stream's solutes: log-uniform 8..500 atoms, each on the
+    smallest of 64..192^3 at 0.5 A that holds its extent plus 12 A; solvent
+    and closure each drawn 50/50.  Returns [(deck path, closure)]."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(SEEDS["c5"] if seed is None else seed)
+    out = []
+    for i in range(count):
+        nu = int(round(math.exp(rng.uniform(math.log(8), math.log(500)))))
+        sol = _c1_recipe(nu, (SEEDS["c5"] if seed is None else seed) * 1000 + i)
+        g = _extent_grid(sol, (64, 80, 96, 128, 144, 160, 192))
+        solv = solvents[int(rng.integers(0, len(solvents)))]
+        clos = closures[int(rng.integers(0, len(closures)))]
+        p = write_inp(os.path.join(outdir, f"c5_{i:03d}.inp"), sol, (g * 0.5,) * 3, (g,) * 3,
+                      solv, closure=clos, maxstep=maxstep)
+        out.append((p, clos))
+    return out
+
+
 def small(outdir, nu=12, grid=32, box=16.0, solvent="h2o_vv.xvk", seed=7, closure="KH",
           name="small", mixer=(2, 0.6, 0.2), **kw):
     """A small deck for parity tests."""

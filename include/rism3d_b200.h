@@ -231,6 +231,62 @@ int r3d_batch_info(const r3d_batch *b, int *solves, int *groups, int *kernels_pe
 /* Frees the batch's own buffers; its contexts stay valid. */
 int r3d_batch_destroy(r3d_batch *b);
 
+/* ---- serving: continuous batching of submitted solves ------------------
+ * No counterpart in the reference (one solve per process).  A server owns
+ * one device, one submission thread and an HBM budget.  Submitted decks are
+ * admitted while the budget and max_active allow: each is initialized on its
+ * own stream while the admitted solves keep iterating, then takes a slot of
+ * its geometry class (grid, solvent sites, mixer); every kernel of an
+ * iteration covers all slots of a class, so solves that arrived at different
+ * times iterate together, and each one retires on convergence (or
+ * divergence, or maxstep) without stopping the others.  With closure_ladder,
+ * a PSE-n deck is solved as KH, then PSE-2, ..., PSE-n, each stage starting
+ * from the previous one's t (the usual route to PSE-n convergence).  Each
+ * result equals the result of the same solve run alone (r3d_iterate per
+ * stage) on the same precision.  Errors: r3d_last_error(NULL). */
+#define R3D_REQ_QUEUED 0
+#define R3D_REQ_ACTIVE 1
+#define R3D_REQ_DONE 2
+#define R3D_REQ_FAILED 3
+
+typedef struct r3d_server r3d_server;
+typedef struct r3d_server_opts {
+  int device;
+  int precision;                 /* R3D_FP64 or R3D_MIXED */
+  unsigned long long hbm_budget; /* bytes for admitted solves; 0: 85% of free memory */
+  int max_active;                /* most solves admitted at once; 0: no limit */
+  int chunk;                     /* iterations between admissions/retirements; 0: 8 */
+  int closure_ladder;            /* 1: solve PSE-n decks as KH, PSE-2, ..., PSE-n */
+} r3d_server_opts;
+
+typedef struct r3d_result {
+  int state;    /* R3D_REQ_* */
+  int status;   /* R3D_CONVERGED / R3D_MAXSTEP / R3D_DIVERGED (state DONE) */
+  int steps;    /* iterations of the last closure stage */
+  int steps_total; /* iterations of all stages */
+  int natv;
+  double rms;
+  double xmu[32], xmu2[16], pmv, pressure; /* r3d_thermo's outputs (state DONE) */
+  double queued_s, admitted_s, finished_s; /* seconds since r3d_server_create */
+  char error[256];                          /* state FAILED */
+} r3d_result;
+
+int r3d_server_create(const r3d_server_opts *opts, r3d_server **out);
+/* Queues the deck (and .xvk; NULL: the one the deck names).  The deck is
+ * parsed here, so a bad deck fails the call; ticket identifies the solve. */
+int r3d_server_submit(r3d_server *s, const char *inp, const char *xvk, long long *ticket);
+/* Current state (and results once done) of a ticket. */
+int r3d_server_poll(r3d_server *s, long long ticket, r3d_result *out);
+/* Waits up to timeout_s seconds (< 0: no limit) for DONE or FAILED, then
+ * does what r3d_server_poll does. */
+int r3d_server_wait(r3d_server *s, long long ticket, double timeout_s, r3d_result *out);
+/* output_xmu's .xmu of a finished solve. */
+int r3d_server_write_xmu(r3d_server *s, long long ticket, const char *path);
+/* Forgets a finished ticket. */
+int r3d_server_release(r3d_server *s, long long ticket);
+/* Finishes every queued and admitted solve, then frees the server. */
+int r3d_server_destroy(r3d_server *s);
+
 #ifdef __cplusplus
 }
 #endif
