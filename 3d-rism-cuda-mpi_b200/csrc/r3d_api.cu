@@ -5,10 +5,13 @@
 // iterate, output.  All device memory is owned by the context; one iteration
 // is captured once as a CUDA graph and replayed, with convergence decided on
 // the device (see k_reduce) so the host only polls every few iterations.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <array>
+#include <map>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -17,6 +20,7 @@
 #include <vector>
 
 #include "../../include/rism3d_b200.h"
+#include "r3d_fft_ct.cuh"
 #include "r3d_internal.h"
 
 namespace r3d {
@@ -52,6 +56,25 @@ template <typename P>
 bool ct_launch_ix(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
 template <typename P>
 bool ct_launch_ixb(int, int, Batch, int, size_t, cudaStream_t, int);
+template <typename P>
+bool ct_launch_fxb(int, int, Batch, int, size_t, cudaStream_t, int);
+size_t ct_smem_fxb(int L, int PC, size_t csz, size_t rsz, size_t tsz);
+template <typename P>
+int ct_occupancy_bulk(int which, int L, int PC, size_t smem);
+template <typename P>
+bool ct_launch_xw(int which, int L, int PCW, Batch b, int grid, size_t smem, cudaStream_t s);
+template <typename P>
+int ct_occupancy_xw(int which, int L, int PCW, size_t smem);
+size_t ct_smem_warp(int L, int PCW, size_t csz);
+template <typename P>
+bool tma_launch_fy(int L, int dir, Batch b, int grid, size_t smem, cudaStream_t s, int per,
+                   int nst);
+template <typename P>
+bool tma_launch_zoz(int L, Batch b, int grid, size_t smem, cudaStream_t s, int per, int nst);
+template <typename P>
+int tma_occupancy(int which, int L, size_t smem);
+template <typename P>
+void tma_allow_smem_all();
 size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz);
 template <typename P>
 void launch_fwd_x(Batch, int, size_t, cudaStream_t, int, const void *);
@@ -106,6 +129,23 @@ constexpr size_t kSmemBudget = 100 * 1024;  // per CTA: two CTAs per SM
 constexpr size_t kSmemMax = 220 * 1024;
 constexpr int kNumSM = 148;
 
+// resident CTAs per SM of a bulk-staged pass (device query; smem-only
+// estimate for host-only planning)
+inline int bulk_per_sm(int device, bool fp64, int which, int L, int PC, size_t smem) {
+  int nb = 0;
+  if (device >= 0) {
+    kernels_set_smem(fp64, kSmemMax);  // the occupancy query honours the opt-in limit
+    if (which < 2)
+      nb = fp64 ? ct_occupancy_bulk<P64>(which, L, PC, smem)
+                : ct_occupancy_bulk<PMix>(which, L, PC, smem);
+    else
+      nb = fp64 ? ct_occupancy_xw<P64>(which - 2, L, PC, smem)
+                : ct_occupancy_xw<PMix>(which - 2, L, PC, smem);
+  }
+  if (nb <= 0) nb = std::max(1, (int)((228 * 1024) / (smem + 2048)));
+  return nb;
+}
+
 }  // namespace r3d
 
 using namespace r3d;
@@ -123,6 +163,18 @@ struct Geo {
   // per tile, CTAs, tiles per CTA, shared memory
   int ixb_pc = 0, ixb_ctas = 0, ixb_per = 1;
   size_t smixb = 0;
+  // the iteration's FX with bulk-staged inputs (fxb_pc = 0: not used)
+  int fxb_pc = 0, fxb_ctas = 0, fxb_per = 1;
+  size_t smfxb = 0;
+  // the iteration's FX / IX on warp tiles (pc = 0: not used): rows per warp
+  // tile, CTAs per solve, shared memory
+  int fxw_pc = 0, fxw_ctas = 0, ixw_pc = 0, ixw_ctas = 0;
+  size_t smxw = 0;
+  // the iteration's y and z passes on the tensor copy engine (yz_tma = 0:
+  // the tile-per-CTA kernels): CTAs per solve, tiles per CTA, stages, smem
+  int yz_tma = 0, fyt_pc = 0, fyt_ctas = 0, fyt_per = 1, fyt_nst = 0, zt_pc = 0, zt_ctas = 0,
+      zt_per = 1, zt_nst = 0;
+  size_t smfyt = 0, smzt = 0;
   size_t smx = 0, smy = 0, smz = 0;
 };
 
@@ -476,17 +528,86 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   g.ix_per = (d.tiles_x + g.ix_ctas - 1) / g.ix_ctas;
   g.ix_ctas = (d.tiles_x + g.ix_per - 1) / g.ix_per;
   g.ixb_pc = 0;
-  if (d.ct_x && !getenv("R3D_NO_IXB")) {  // bulk-staged IX: as many CTAs as stay resident
-    const int pcb = fp64 ? 4 : 8;
-    const size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+  if (d.ct_x) {  // bulk-staged IX: as many CTAs as stay resident
+    int pcb = fp64 ? 4 : 8;
+    size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+    if (sm > kSmemMax && d.hx >= 256) {  // long rows: half the rows per tile
+      pcb /= 2;
+      sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+    }
     if (rowsN % pcb == 0 && sm <= kSmemMax) {
       const int tiles = d.n * (rowsN / pcb);
-      const int per_sm = std::max(1, (int)((228 * 1024) / (sm + 2048)));
+      const int per_sm = bulk_per_sm(c->opts.device, fp64, 1, d.hx, pcb, sm);
       g.ixb_pc = pcb;
       g.smixb = sm;
       g.ixb_ctas = std::min(tiles, kNumSM * per_sm);
       g.ixb_per = (tiles + g.ixb_ctas - 1) / g.ixb_ctas;
       g.ixb_ctas = (tiles + g.ixb_per - 1) / g.ixb_per;
+    }
+  }
+  g.fxb_pc = 0;
+  if (d.ct_x) {  // bulk-staged FX, sized like the IX above
+    int pcb = fp64 ? 4 : 8;
+    size_t sm = ct_smem_fxb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+    if (sm > 110 * 1024 && d.hx >= 256) {  // long rows: half the rows, two CTAs per SM
+      pcb /= 2;
+      sm = ct_smem_fxb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+    }
+    if (rowsN % pcb == 0 && sm <= kSmemMax) {
+      const int tiles = d.n * (rowsN / pcb);
+      const int per_sm = bulk_per_sm(c->opts.device, fp64, 0, d.hx, pcb, sm);
+      g.fxb_pc = pcb;
+      g.smfxb = sm;
+      g.fxb_ctas = std::min(tiles, kNumSM * per_sm);
+      g.fxb_per = (tiles + g.fxb_ctas - 1) / g.fxb_ctas;
+      g.fxb_ctas = (tiles + g.fxb_per - 1) / g.fxb_per;
+    }
+  }
+  g.fxw_pc = g.ixw_pc = 0;
+  if (d.ct_x) {  // warp tiles: 4 rows per warp (2 for long rows)
+    const int pcw = d.hx >= 256 ? 2 : 4;
+    const size_t sm = ct_smem_warp(d.hx, pcw, cs);
+    if (rowsN % pcw == 0 && sm + 6 * 1024 <= kSmemMax) {
+      const int ctas = (d.n * (rowsN / pcw) + 7) / 8;
+      g.smxw = sm;
+      g.fxw_pc = g.ixw_pc = pcw;
+      g.fxw_ctas = std::min(ctas, kNumSM * bulk_per_sm(c->opts.device, fp64, 2, d.hx, pcw, sm));
+      g.ixw_ctas = std::min(ctas, kNumSM * bulk_per_sm(c->opts.device, fp64, 3, d.hx, pcw, sm));
+    }
+  }
+  g.yz_tma = 0;
+  {  // y and z passes on the tensor copy engine: lengths of the engine, 2-4 stages
+    auto tma_len = [](int L) { return ct_length_ok(L) && L <= 512; };
+    const int py = fp64 ? 4 : 8, pz = fp64 ? 2 : 4;
+    const size_t sby = (size_t)py * d.ny * cs, sbz = (size_t)pz * d.nz * d.n * cs;
+    auto stages = [&](size_t sb, size_t cap) {
+      for (int k = 4; k >= 2; --k)
+        if (k * sb <= cap) return k;
+      return 0;
+    };
+    const int ny_st = stages(sby, 64 * 1024) ? stages(sby, 64 * 1024) : stages(sby, kSmemMax);
+    const int nz_st = stages(sbz, 110 * 1024) ? stages(sbz, 110 * 1024) : stages(sbz, kSmemMax);
+    if (tma_len(d.ny) && tma_len(d.nz) && d.hx % py == 0 && d.hx % pz == 0 && ny_st && nz_st &&
+        c->opts.device >= 0) {
+      g.yz_tma = 2;  // the autotuner may step down to 1 (copy-engine y only) or 0
+      g.fyt_pc = py;
+      g.zt_pc = pz;
+      g.fyt_nst = ny_st;
+      g.zt_nst = nz_st;
+      g.smfyt = ny_st * sby;
+      g.smzt = nz_st * sbz;
+      const int ty = d.n * d.nz * (d.hx / py), tz = d.ny * (d.hx / pz);
+      kernels_set_smem(fp64, kSmemMax);
+      int oy = fp64 ? tma_occupancy<P64>(0, d.ny, g.smfyt) : tma_occupancy<PMix>(0, d.ny, g.smfyt);
+      int oz = fp64 ? tma_occupancy<P64>(1, d.nz, g.smzt) : tma_occupancy<PMix>(1, d.nz, g.smzt);
+      oy = std::max(oy, 1);
+      oz = std::max(oz, 1);
+      g.fyt_ctas = std::min(ty, kNumSM * oy);
+      g.fyt_per = (ty + g.fyt_ctas - 1) / g.fyt_ctas;
+      g.fyt_ctas = (ty + g.fyt_per - 1) / g.fyt_per;
+      g.zt_ctas = std::min(tz, kNumSM * oz);
+      g.zt_per = (tz + g.zt_ctas - 1) / g.zt_ctas;
+      g.zt_ctas = (tz + g.zt_per - 1) / g.zt_per;
     }
   }
   // mixers: one chunk of mix_chunk() elements per CTA; ANM dots: one full
@@ -506,6 +627,11 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
 template <typename P>
 static void pass_fx(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode,
                     const void *src) {
+  if (mode == 1 && g.fxw_pc && ct_launch_xw<P>(0, d.hx, g.fxw_pc, b, g.fxw_ctas, g.smxw, s))
+    return;
+  if (mode == 1 && g.fxb_pc &&
+      ct_launch_fxb<P>(d.hx, g.fxb_pc, b, g.fxb_ctas, g.smfxb, s, g.fxb_per))
+    return;
   if (!(d.ct_x && ct_launch_fx<P>(d.hx, d.ct_x, b, g.tiles_x, g.smx, s, mode, src)))
     launch_fwd_x<P>(b, g.tiles_x, g.smx, s, mode, src);
 }
@@ -522,14 +648,43 @@ static void pass_zoz(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int m
 }
 template <typename P>
 static void pass_ix(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode, void *dst) {
+  if (mode == 1 && g.ixw_pc && ct_launch_xw<P>(1, d.hx, g.ixw_pc, b, g.ixw_ctas, g.smxw, s))
+    return;
   if (mode == 1 && g.ixb_pc &&
       ct_launch_ixb<P>(d.hx, g.ixb_pc, b, g.ixb_ctas, g.smixb, s, g.ixb_per))
     return;
   if (!(d.ct_x && ct_launch_ix<P>(d.hx, d.ct_x, b, g.ix_ctas, g.smx, s, mode, dst, g.ix_per)))
     launch_inv_x<P>(b, g.ix_ctas, g.smx, s, mode, dst, g.ix_per);
 }
+// The iteration's y / z passes: on the tensor copy engine when the geometry
+// has it (the three together: they share the digit-reversed ky layout of w),
+// else the tile-per-CTA kernels.
+template <typename P>
+static void pass_fy_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int dir) {
+  if (g.yz_tma && tma_launch_fy<P>(d.ny, dir, b, g.fyt_ctas, g.smfyt, s, g.fyt_per, g.fyt_nst))
+    return;
+  pass_fy<P>(d, g, b, s, dir, 1);
+}
+template <typename P>
+static void pass_zoz_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s) {
+  if (g.yz_tma == 2 && tma_launch_zoz<P>(d.nz, b, g.zt_ctas, g.smzt, s, g.zt_per, g.zt_nst))
+    return;
+  if (g.yz_tma == 1 && ct_launch_zoz<P>(d.nz, d.ct_z, b, g.tiles_z, g.smz, s, 1 | 2)) return;
+  pass_zoz<P>(d, g, b, s, 2, 1);
+}
+
 // CTAs of the iteration's IX (each writes one row of the partials k_reduce sums)
-static int iter_ix_ctas(const Geo &g) { return g.ixb_pc ? g.ixb_ctas : g.ix_ctas; }
+static int iter_ix_ctas(const Geo &g) {
+  return g.ixw_pc ? g.ixw_ctas : g.ixb_pc ? g.ixb_ctas : g.ix_ctas;
+}
+// rows of partials the iteration's IX may need, whichever variant runs
+static int max_ix_ctas(const Geo &g) {
+  return std::max(std::max(g.ix_ctas, g.ixb_pc ? g.ixb_ctas : 0), g.ixw_pc ? g.ixw_ctas : 0);
+}
+// CTAs of the iteration's FX
+static int iter_fx_ctas(const Geo &g) {
+  return g.fxw_pc ? g.fxw_ctas : g.fxb_pc ? g.fxb_ctas : g.tiles_x;
+}
 
 // Launch prefixes of ns solves that share one geometry (a device int block):
 // the CTA prefixes of the x, y, z, IX, mix and ANM-dot passes (ns + 1 entries
@@ -542,7 +697,9 @@ static int pf_off(int ns, int k) {
 static int pf_len(int ns) { return PF_IXC * (ns + 1) + 2 * ns; }
 static std::vector<int> make_prefix(const Geo &g, int ns) {
   std::vector<int> v(pf_len(ns));
-  const int per[6] = {g.tiles_x, g.tiles_y, g.tiles_z, iter_ix_ctas(g), g.mix_ctas, g.dot_ctas};
+  const int per[6] = {iter_fx_ctas(g), g.yz_tma ? g.fyt_ctas : g.tiles_y,
+                      g.yz_tma == 2 ? g.zt_ctas : g.tiles_z, iter_ix_ctas(g), g.mix_ctas,
+                      g.dot_ctas};
   for (int k = 0; k < 6; ++k)
     for (int i = 0; i <= ns; ++i) v[pf_off(ns, k) + i] = i * per[k];
   for (int i = 0; i < ns; ++i) {
@@ -559,6 +716,11 @@ static Geo scaled(const Geo &g, int ns) {
   s.tiles_z *= ns;
   s.ix_ctas *= ns;
   s.ixb_ctas *= ns;
+  s.fxb_ctas *= ns;
+  s.fxw_ctas *= ns;
+  s.ixw_ctas *= ns;
+  s.fyt_ctas *= ns;
+  s.zt_ctas *= ns;
   s.mix_ctas *= ns;
   s.dot_ctas *= ns;
   return s;
@@ -567,6 +729,83 @@ static Geo scaled(const Geo &g, int ns) {
 // Twiddle tables of the compile-time engine for one grid: [twx | pwx | twy |
 // pwy | twz | pwz]; FP64 always (refresh pipeline), FP32 as well for the
 // mixed path.  Sets the table pointers of d (grid type of the descriptor).
+// cuTensorMapEncodeTiled from the driver, looked up once (no link-time
+// dependency on the driver library)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
+// natural index of digit-reversed position P of a length-L transform
+static int digit_rev_inv_host(int L, int P) {
+  const Fac f = factorize(L);
+  int I = 0, M = L, scale = 1;
+  for (int k = 0; k < f.n; ++k) {
+    M /= f.r[k];
+    const int dk = P / M;
+    P -= dk * M;
+    I += dk * scale;
+    scale *= f.r[k];
+  }
+  return I;
+}
+
+// Tensor maps of w for the iteration's y and z passes (4D [site][z][y][x]
+// in 8-byte elements, strides in bytes) and the ky table of the
+// digit-reversed y rows.  Without the driver entry point the geometry falls
+// back to the tile-per-CTA passes.
+static int make_tmaps(r3d_ctx *c, Desc &d) {
+  Geo &g = c->geo;
+  d.tma_pc_y = d.tma_pc_z = 0;
+  d.yrev = nullptr;
+  if (!g.yz_tma) return R3D_OK;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) {
+    g.yz_tma = 0;
+    return R3D_OK;
+  }
+  const cuuint64_t cs = c->fp64 ? 16 : 8, e8 = cs / 8;
+  const cuuint64_t dims[4] = {(cuuint64_t)d.hx * e8, (cuuint64_t)d.ny, (cuuint64_t)d.nz,
+                              (cuuint64_t)d.n};
+  const cuuint64_t strides[3] = {(cuuint64_t)d.hx * cs, (cuuint64_t)d.hx * d.ny * cs,
+                                 (cuuint64_t)d.Nhs * cs};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const cuuint32_t by[4] = {(cuuint32_t)(g.fyt_pc * e8), (cuuint32_t)std::min(d.ny, 256), 1, 1};
+  const cuuint32_t bz[4] = {(cuuint32_t)(g.zt_pc * e8), 1, (cuuint32_t)std::min(d.nz, 256), 1};
+  CUresult r1 = enc((CUtensorMap *)&d.tm_y, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, d.w, dims, strides,
+                    by, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r2 = enc((CUtensorMap *)&d.tm_z, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, d.w, dims, strides,
+                    bz, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
+    g.yz_tma = 0;
+    return R3D_OK;
+  }
+  std::vector<int> yr(d.ny);
+  for (int P = 0; P < d.ny; ++P) yr[P] = digit_rev_inv_host(d.ny, P);
+  int *dy = nullptr;
+  int rc = dalloc(c, (void **)&dy, yr.size() * sizeof(int));
+  if (rc) return rc;
+  CK(copy_h2d(c, dy, yr.data(), yr.size() * sizeof(int), c->stream));
+  d.yrev = dy;
+  d.tma_pc_y = g.fyt_pc;
+  d.tma_pc_z = g.zt_pc;
+  return R3D_OK;
+}
+
 static int make_twiddles(r3d_ctx *c, Desc &d, bool fp64_desc, void **t64, void **t32) {
   const int L[6] = {d.hx, d.hx, d.ny, d.ny, d.nz, d.nz};
   const double sc[6] = {-2.0 / d.hx, -1.0 / d.nx, -2.0 / d.ny, -1.0 / d.ny, -2.0 / d.nz,
@@ -669,10 +908,125 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   b += (size_t)nshell * n * n * R;
   size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
   b += slots * n * N * (R + T);    // mixer history (residuals, states)
-  b += (size_t)std::max(std::max(c->geo.ix_ctas, iter_ix_ctas(c->geo)), c->geo.dot_ctas) *
-       kPartials * 8;
+  b += (size_t)std::max(max_ix_ctas(c->geo), c->geo.dot_ctas) * kPartials * 8;
   b += (size_t)(c->prob.maxstep + 1) * 8 + sizeof(Ctl) + sizeof(Desc) + 4096;
   return b;
+}
+
+// ------------------------------------------------------------ autotuning
+// The iteration's x passes have two implementations each: one tile per CTA
+// with loads through registers (k_fx_ct / k_ix_ct), or persistent CTAs whose
+// inputs the bulk copy engine stages (k_fx_bulk / k_ix_bulk).  Which is
+// faster depends on the row length, the sites and the precision, so the
+// first solve of each geometry times both on its own buffers -- the mode-1 x
+// passes write only w, the residual and the partials, which every iteration
+// rewrites -- and the choice holds for the process.
+static std::mutex g_tune_mu;
+// per geometry: the FX and IX variant (0 one tile per CTA, 1 bulk-staged,
+// 2 warp tiles)
+static std::map<std::array<int, 5>, std::array<int, 3>> g_tune;  // + y/z on TMA
+
+template <typename P>
+static int autotune_x(r3d_ctx *c) {
+  Geo &g = c->geo;
+  const Desc &d = c->desc;
+  if (!g.fxb_pc && !g.ixb_pc && !g.fxw_pc && !g.ixw_pc && !g.yz_tma) return R3D_OK;
+  const std::array<int, 5> key{d.nx, d.ny, d.nz, d.n, c->fp64 ? 1 : 0};
+  std::array<int, 3> use{0, 0, g.yz_tma};
+  bool known = false;
+  // R3D_X_VARIANT=0|1|2 replaces the timing by that variant where it exists
+  // (diagnostics and the per-variant parity tests)
+  if (const char *ev = getenv("R3D_X_VARIANT")) {
+    const int k = std::atoi(ev);
+    const bool fx = k == 0 || (k == 1 && g.fxb_pc) || (k == 2 && g.fxw_pc);
+    const bool ix = k == 0 || (k == 1 && g.ixb_pc) || (k == 2 && g.ixw_pc);
+    use = {fx ? k : 0, ix ? k : 0, g.yz_tma};
+    if (const char *ey = getenv("R3D_YZ_VARIANT")) {
+      const int k = std::atoi(ey);
+      use[2] = (k == 1 && !d.ct_z) ? 0 : std::min(k, g.yz_tma);
+    }
+    known = true;
+  } else {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      use = it->second;
+      known = true;
+    }
+  }
+  // geometry with only variant k of the x passes
+  auto only = [&](int k) {
+    Geo o = g;
+    if (k != 1) o.fxb_pc = o.ixb_pc = 0;
+    if (k != 2) o.fxw_pc = o.ixw_pc = 0;
+    return o;
+  };
+  if (!known) {
+    cudaStream_t s = c->stream;
+    int *pf = nullptr;
+    CK(cudaMalloc((void **)&pf, 20 * sizeof(int)));
+    const int pre[20] = {0, d.tiles_x, 0, g.fxb_ctas, 0, g.fxw_ctas, 0, g.ix_ctas,
+                         0, g.ixb_ctas, 0, g.ixw_ctas, 0, g.tiles_y, 0, g.tiles_z,
+                         0, g.fyt_ctas, 0, g.zt_ctas};
+    CK(copy_h2d(c, pf, pre, sizeof(pre), s));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time = [&](auto &&launch) {
+      launch();
+      cudaEventRecord(e0, s);
+      for (int i = 0; i < 3; ++i) launch();
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      return ms;
+    };
+    float best[2] = {0, 0};
+    for (int k = 0; k < 3; ++k) {
+      const Geo o = only(k);
+      const bool fx = k == 0 || (k == 1 ? g.fxb_pc : g.fxw_pc);
+      const bool ix = k == 0 || (k == 1 ? g.ixb_pc : g.ixw_pc);
+      if (fx) {
+        const float ms = time([&] { pass_fx<P>(d, o, Batch{c->ddesc, pf + 2 * k, 1}, s, 1, nullptr); });
+        if (k == 0 || ms < best[0]) best[0] = ms, use[0] = k;
+      }
+      if (ix) {
+        const float ms =
+            time([&] { pass_ix<P>(d, o, Batch{c->ddesc, pf + 6 + 2 * k, 1}, s, 1, nullptr); });
+        if (k == 0 || ms < best[1]) best[1] = ms, use[1] = k;
+      }
+    }
+    if (g.yz_tma) {  // the y/z trio: tile-per-CTA, copy-engine y, copy-engine y and z
+      float best2 = 0;
+      for (int k = 0; k < 3; ++k) {
+        if (k == 1 && !d.ct_z) continue;
+        Geo o = g;
+        o.yz_tma = k;
+        const Batch by{c->ddesc, pf + (k ? 16 : 12), 1},
+            bz{c->ddesc, pf + (k == 2 ? 18 : 14), 1};
+        const float ms = time([&] {
+          pass_fy_iter<P>(d, o, by, s, -1);
+          pass_zoz_iter<P>(d, o, bz, s);
+          pass_fy_iter<P>(d, o, by, s, 1);
+        });
+        if (k == 0 || ms < best2) best2 = ms, use[2] = k;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaError_t e = cudaGetLastError();
+    cudaFree(pf);
+    if (e != cudaSuccess) return fail(c, R3D_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = use;
+  }
+  if (use[0] != 1) g.fxb_pc = 0;
+  if (use[0] != 2) g.fxw_pc = 0;
+  if (use[1] != 1) g.ixb_pc = 0;
+  if (use[1] != 2) g.ixw_pc = 0;
+  g.yz_tma = use[2];
+  return R3D_OK;
 }
 
 template <typename P>
@@ -703,7 +1057,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
   if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
   if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
-  const int npart = std::max(std::max(c->geo.ix_ctas, iter_ix_ctas(c->geo)), c->geo.dot_ctas);
+  const int npart = std::max(max_ix_ctas(c->geo), c->geo.dot_ctas);
   if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;
   double *rmslog;
   if ((rc = dalloc(c, (void **)&rmslog, (size_t)(p.maxstep + 1) * 8))) return rc;
@@ -752,6 +1106,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   d.partials = c->partials;
   d.ctl = c->ctl;
   if ((rc = make_twiddles(c, d, c->fp64, &c->tw64, &c->tw32))) return rc;
+  if ((rc = make_tmaps(c, d))) return rc;
   d.partial_base = 0;
   d.rmslog = rmslog;
 
@@ -857,6 +1212,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     h.count_left = p.count;
     CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
     CK(copy_h2d(c, c->ddesc, &d, sizeof(Desc), s));
+    if ((rc = autotune_x<P>(c))) return rc;
     const std::vector<int> pre = make_prefix(c->geo, 1);
     CK(copy_h2d(c, c->dprefix, pre.data(), pre.size() * sizeof(int), s));
     CK(cudaStreamSynchronize(s));
@@ -930,9 +1286,9 @@ static int enqueue_group(const Group &G, cudaStream_t s, int stage) {
   int k = 0;
   if (stage != 2) {
     pass_fx<P>(d, g, B(PF_X), s, 1, nullptr);
-    pass_fy<P>(d, g, B(PF_Y), s, -1, 1);
-    pass_zoz<P>(d, g, B(PF_Z), s, 2, 1);
-    pass_fy<P>(d, g, B(PF_Y), s, 1, 1);
+    pass_fy_iter<P>(d, g, B(PF_Y), s, -1);
+    pass_zoz_iter<P>(d, g, B(PF_Z), s);
+    pass_fy_iter<P>(d, g, B(PF_Y), s, 1);
     pass_ix<P>(d, g, B(PF_IX), s, 1, nullptr);
     k += 5;
     if (G.mixer == MIX_ANM) {
@@ -1104,11 +1460,11 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   timed("fwd_x", n * N * (ts + rs + cref + rs),
         [&] { pass_fx<P>(d, c->geo, bx, s, 1, nullptr); });
   timed("fft_y_fwd", n * N * 2 * rs,
-        [&] { pass_fy<P>(d, c->geo, by, s, -1, 1); });
+        [&] { pass_fy_iter<P>(d, c->geo, by, s, -1); });
   timed("zoz", n * N * 2 * rs + (double)d.Nh * 4,
-        [&] { pass_zoz<P>(d, c->geo, bz, s, 2, 1); });
+        [&] { pass_zoz_iter<P>(d, c->geo, bz, s); });
   timed("fft_y_inv", n * N * 2 * rs,
-        [&] { pass_fy<P>(d, c->geo, by, s, 1, 1); });
+        [&] { pass_fy_iter<P>(d, c->geo, by, s, 1); });
   timed("inv_x", n * N * (rs + ts + rs + rs + rs + (dots ? 2 * rs : 0)),
         [&] { pass_ix<P>(d, c->geo, bix, s, 1, nullptr); });
   if (c->mixer == MIX_AN2) {

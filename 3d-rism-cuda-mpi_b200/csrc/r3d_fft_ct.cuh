@@ -17,6 +17,7 @@
 #pragma once
 
 #include "r3d_fft.cuh"
+#include "r3d_internal.h"
 
 namespace r3d {
 
@@ -72,16 +73,17 @@ __device__ __forceinline__ C tw_load(const C *tw, int e) {
   return DIR < 0 ? w : cconj(w);
 }
 
-// One DIT stage (radix R = f.r[S], sub-length M) on all PC columns.
-template <int L, int PC, int LD, int S, int DIR, typename C>
-__device__ __forceinline__ void ct_dit_stage(C *buf, const C *tw) {
+// One DIT stage (radix R = f.r[S], sub-length M) on all PC columns, by NT
+// threads (thread tid of the group).
+template <int L, int PC, int LD, int S, int DIR, int NT, typename C>
+__device__ __forceinline__ void ct_dit_stage(C *buf, const C *tw, int tid) {
   constexpr Fac f = factorize(L);
   constexpr int R = f.r[S];
   constexpr int M = sub_len(L, S + 1);
-  constexpr int NB = L / R;           // butterflies per column
-  constexpr int TR = kThreads / PC;   // row groups
+  constexpr int NB = L / R;       // butterflies per column
+  constexpr int TR = NT / PC;     // row groups
   constexpr int TWS = L / (R * M);
-  const int p = threadIdx.x % PC, g = threadIdx.x / PC;
+  const int p = tid % PC, g = tid / PC;
 #pragma unroll
   for (int b0 = 0; b0 < NB; b0 += TR) {
     const int b = b0 + g;
@@ -103,15 +105,15 @@ __device__ __forceinline__ void ct_dit_stage(C *buf, const C *tw) {
 }
 
 // One DIF stage (radix R = f.r[S], block length Lb = R*M).
-template <int L, int PC, int LD, int S, int DIR, typename C>
-__device__ __forceinline__ void ct_dif_stage(C *buf, const C *tw) {
+template <int L, int PC, int LD, int S, int DIR, int NT, typename C>
+__device__ __forceinline__ void ct_dif_stage(C *buf, const C *tw, int tid) {
   constexpr Fac f = factorize(L);
   constexpr int R = f.r[S];
   constexpr int M = sub_len(L, S + 1);
   constexpr int NB = L / R;
-  constexpr int TR = kThreads / PC;
+  constexpr int TR = NT / PC;
   constexpr int TWS = L / (R * M);
-  const int p = threadIdx.x % PC, g = threadIdx.x / PC;
+  const int p = tid % PC, g = tid / PC;
 #pragma unroll
   for (int b0 = 0; b0 < NB; b0 += TR) {
     const int b = b0 + g;
@@ -132,21 +134,30 @@ __device__ __forceinline__ void ct_dif_stage(C *buf, const C *tw) {
   }
 }
 
-template <int L, int PC, int LD, int S, int DIR, typename C>
-__device__ __forceinline__ void ct_dit_from(C *buf, const C *tw) {
-  if constexpr (S >= 0) {
-    ct_dit_stage<L, PC, LD, S, DIR>(buf, tw);
+// barrier of the thread group: the CTA (NT = kThreads) or one warp (NT = 32)
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (NT == 32)
+    __syncwarp();
+  else
     __syncthreads();
-    ct_dit_from<L, PC, LD, S - 1, DIR>(buf, tw);
+}
+
+template <int L, int PC, int LD, int S, int DIR, int NT, typename C>
+__device__ __forceinline__ void ct_dit_from(C *buf, const C *tw, int tid) {
+  if constexpr (S >= 0) {
+    ct_dit_stage<L, PC, LD, S, DIR, NT>(buf, tw, tid);
+    group_sync<NT>();
+    ct_dit_from<L, PC, LD, S - 1, DIR, NT>(buf, tw, tid);
   }
 }
-template <int L, int PC, int LD, int S, int DIR, typename C>
-__device__ __forceinline__ void ct_dif_from(C *buf, const C *tw) {
+template <int L, int PC, int LD, int S, int DIR, int NT, typename C>
+__device__ __forceinline__ void ct_dif_from(C *buf, const C *tw, int tid) {
   constexpr Fac f = factorize(L);
   if constexpr (S < f.n) {
-    ct_dif_stage<L, PC, LD, S, DIR>(buf, tw);
-    __syncthreads();
-    ct_dif_from<L, PC, LD, S + 1, DIR>(buf, tw);
+    ct_dif_stage<L, PC, LD, S, DIR, NT>(buf, tw, tid);
+    group_sync<NT>();
+    ct_dif_from<L, PC, LD, S + 1, DIR, NT>(buf, tw, tid);
   }
 }
 
@@ -155,12 +166,23 @@ __device__ __forceinline__ void ct_dif_from(C *buf, const C *tw) {
 template <int L, int PC, int LD, int DIR, typename C>
 __device__ __forceinline__ void ct_fft_dit(C *buf, const C *tw) {
   constexpr Fac f = factorize(L);
-  ct_dit_from<L, PC, LD, f.n - 1, DIR>(buf, tw);
+  ct_dit_from<L, PC, LD, f.n - 1, DIR, kThreads>(buf, tw, threadIdx.x);
 }
 // Inverse-direction (DIF) transform; output rows digit-reversed.
 template <int L, int PC, int LD, int DIR, typename C>
 __device__ __forceinline__ void ct_fft_dif(C *buf, const C *tw) {
-  ct_dif_from<L, PC, LD, 0, DIR>(buf, tw);
+  ct_dif_from<L, PC, LD, 0, DIR, kThreads>(buf, tw, threadIdx.x);
+}
+// The same transforms by one warp on its own tile (lane = lane index); they
+// end with __syncwarp.
+template <int L, int PC, int LD, int DIR, typename C>
+__device__ __forceinline__ void ct_fft_dit_warp(C *buf, const C *tw, int lane) {
+  constexpr Fac f = factorize(L);
+  ct_dit_from<L, PC, LD, f.n - 1, DIR, 32>(buf, tw, lane);
+}
+template <int L, int PC, int LD, int DIR, typename C>
+__device__ __forceinline__ void ct_fft_dif_warp(C *buf, const C *tw, int lane) {
+  ct_dif_from<L, PC, LD, 0, DIR, 32>(buf, tw, lane);
 }
 
 }  // namespace r3d

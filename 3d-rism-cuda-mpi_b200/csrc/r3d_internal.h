@@ -147,6 +147,16 @@ struct Desc {
   double *partials;  // [ctas][kPartials]
   double *rmslog;    // [maxstep] rms of every evaluation
   Ctl *ctl;
+  // tensor maps (CUtensorMap) of the half spectrum w for the iteration's
+  // y and z passes on the copy engine: 4D [site][z][y][x] in 8-byte
+  // elements, boxes of PC x-columns by a y column (tm_y) or by a z column of
+  // every site (tm_z); tma_pc_* = 0: not built
+  struct alignas(64) Tmap {
+    unsigned char b[128];
+  };
+  Tmap tm_y, tm_z;
+  int tma_pc_y, tma_pc_z;
+  const int *yrev;  // [ny]: ky index of each digit-reversed y row of w
 };
 
 constexpr int kPartials = 1 + 5 * kMaxSites;  // sum R^2 + per-site dots

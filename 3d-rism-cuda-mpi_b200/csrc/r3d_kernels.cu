@@ -1162,6 +1162,8 @@ void launch_twiddle(double2 *o64, float2 *o32, int count, double scale, cudaStre
 template <typename P>
 void ct_allow_smem_all();
 
+template <typename P>
+void tma_allow_smem_all();
 void kernels_set_smem(bool fp64, size_t maxbytes) {
   static bool ct_done[2] = {false, false};
   if (fp64)
@@ -1169,10 +1171,13 @@ void kernels_set_smem(bool fp64, size_t maxbytes) {
   else
     set_smem_attrs<PMix>(maxbytes);
   if (!ct_done[fp64]) {  // compile-time-engine passes, once per process
-    if (fp64)
+    if (fp64) {
       ct_allow_smem_all<P64>();
-    else
+      tma_allow_smem_all<P64>();
+    } else {
       ct_allow_smem_all<PMix>();
+      tma_allow_smem_all<PMix>();
+    }
     ct_done[fp64] = true;
   }
 }

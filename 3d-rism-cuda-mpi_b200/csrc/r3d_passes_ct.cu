@@ -6,6 +6,7 @@
 // algorithm and the reference lines each step follows.
 #include "r3d_common.cuh"
 #include "r3d_fft_ct.cuh"
+#include "r3d_async.cuh"
 
 #ifndef R3D_CT_FP64
 #define R3D_CT_FP64 1
@@ -212,6 +213,8 @@ __device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const 
   }
 }
 
+// check: bit 0 = skip solves not running; bit 1 = w's y rows are in the
+// digit-reversed ky order of the copy-engine y pass (ky from d.yrev)
 template <typename P, int L, int PC>
 __global__ void __launch_bounds__(kThreads)
     k_zoz_ct(Batch b, int check) {
@@ -221,10 +224,11 @@ __global__ void __launch_bounds__(kThreads)
   C *buf = (C *)smem;
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
-  if (check && d.ctl->status != RUNNING) return;
+  if ((check & 1) && d.ctl->status != RUNNING) return;
   const int tile = blockIdx.x - b.prefix[si];
   const int hx = d.hx, n = d.n, ptiles = hx / PC;
   const int pt = tile % ptiles, y = tile / ptiles;
+  const int ky = (check & 2) ? d.yrev[y] : y;
   const long long zs = (long long)d.ny * hx;
   const C *pw = (const C *)d.pwz, *tw = (const C *)d.twz;
   C *w = (C *)d.w + (long long)y * hx + pt * PC;
@@ -240,11 +244,11 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   for (int v = 0; v < n; ++v) ct_fft_dit<L, PC, PC, -1>(buf + v * L * PC, tw);
   switch (n) {
-    case 1: ct_oz<P, L, PC, 1>(buf, d, y, pt); break;
-    case 2: ct_oz<P, L, PC, 2>(buf, d, y, pt); break;
-    case 3: ct_oz<P, L, PC, 3>(buf, d, y, pt); break;
-    case 4: ct_oz<P, L, PC, 4>(buf, d, y, pt); break;
-    default: ct_oz<P, L, PC, 0>(buf, d, y, pt); break;
+    case 1: ct_oz<P, L, PC, 1>(buf, d, ky, pt); break;
+    case 2: ct_oz<P, L, PC, 2>(buf, d, ky, pt); break;
+    case 3: ct_oz<P, L, PC, 3>(buf, d, ky, pt); break;
+    case 4: ct_oz<P, L, PC, 4>(buf, d, ky, pt); break;
+    default: ct_oz<P, L, PC, 0>(buf, d, ky, pt); break;
   }
   __syncthreads();
   for (int v = 0; v < n; ++v) ct_fft_dif<L, PC, PC, 1>(buf + v * L * PC, tw);
@@ -386,40 +390,6 @@ __global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
 // of t, u, lr and the two AN2 residual slots, so one cp.async.bulk per array
 // brings the next tile into shared memory while the current one is being
 // transformed and reduced (two stages, one mbarrier each).
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
-                                         uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-// Bounded wait for phase `parity` of `bar`; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
 template <typename P, int L, int PC>
 struct IxStage {  // byte layout of one stage of staged inputs
   static constexpr int NX = 2 * L;
@@ -428,18 +398,19 @@ struct IxStage {  // byte layout of one stage of staged inputs
   static constexpr size_t lr = u + (size_t)PC * NX * sizeof(typename P::R);
   static constexpr size_t r0 = lr + (size_t)PC * NX * sizeof(typename P::R);
   static constexpr size_t r1 = r0 + (size_t)PC * NX * sizeof(typename P::R);
-  static constexpr size_t bytes = r1 + (size_t)PC * NX * sizeof(typename P::R);
+  static constexpr size_t w = r1 + (size_t)PC * NX * sizeof(typename P::R);  // spectrum rows
+  static constexpr size_t bytes = w + (size_t)PC * L * 2 * sizeof(typename P::R);
 };
 #if R3D_CT_FP64
 size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz) {
   const size_t buf = ((csz * (size_t)L * (PC + 1) + 127) / 128) * 128;
-  const size_t stage = (size_t)PC * 2 * L * (tsz + 4 * rsz);
+  const size_t stage = (size_t)PC * 2 * L * (tsz + 4 * rsz) + (size_t)PC * L * csz;
   return buf + 2 * stage;
 }
 #endif
 
 template <typename P, int L, int PC>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 1)
     k_ix_bulk(Batch b, int per) {
   using R = typename P::R;
   using T = typename P::T;
@@ -468,20 +439,29 @@ __global__ void __launch_bounds__(kThreads)
   R *res = (R *)d.res;
   const long long niv = (long long)d.n * d.Ns;
   const uint32_t tbytes = PC * NX * sizeof(T), rbytes = PC * NX * sizeof(R);
-  const uint32_t stage_tx = tbytes + 2 * rbytes + (dots ? 2 * rbytes : 0);
-  auto issue = [&](int tile, int st) {  // thread 0: copies of one tile
+  const uint32_t wbytes = PC * L * sizeof(C);
+  const uint32_t stage_tx = tbytes + 2 * rbytes + wbytes + (dots ? 2 * rbytes : 0);
+  const Desc *dp = &d;
+  char *const stages = smem + BUF;
+  uint64_t *const bars = bar;
+  // thread 0: the copies of one tile into stage st (no captures by reference:
+  // they would keep the loop's variables in local memory)
+  auto issue = [=](int tile, int st) {
     const int v = tile / tps;
-    const long long base = (long long)v * d.Ns + (long long)(tile % tps) * PC * NX;
-    char *sb = smem + BUF + st * St::bytes;
-    uint64_t *br = &bar[st];
+    const long long base = (long long)v * dp->Ns + (long long)(tile % tps) * PC * NX;
+    char *sb = stages + st * St::bytes;
+    uint64_t *br = bars + st;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(br, stage_tx);
-    bulk_g2s(sb + St::t, (const T *)d.t + base, tbytes, br);
-    bulk_g2s(sb + St::u, (const R *)d.u + base, rbytes, br);
-    bulk_g2s(sb + St::lr, (const R *)d.lr + base, rbytes, br);
+    bulk_g2s(sb + St::t, (const T *)dp->t + base, tbytes, br);
+    bulk_g2s(sb + St::u, (const R *)dp->u + base, rbytes, br);
+    bulk_g2s(sb + St::lr, (const R *)dp->lr + base, rbytes, br);
+    bulk_g2s(sb + St::w,
+             (const C *)dp->w + (long long)v * dp->Nhs + (long long)(tile % tps) * PC * L,
+             wbytes, br);
     if (dots) {
-      bulk_g2s(sb + St::r0, (const R *)d.hist_b + base, rbytes, br);
-      bulk_g2s(sb + St::r1, (const R *)d.hist_b + niv + base, rbytes, br);
+      bulk_g2s(sb + St::r0, (const R *)dp->hist_b + base, rbytes, br);
+      bulk_g2s(sb + St::r1, (const R *)dp->hist_b + niv + base, rbytes, br);
     }
   };
   if (threadIdx.x == 0) {
@@ -524,17 +504,17 @@ __global__ void __launch_bounds__(kThreads)
       const long long row = row0 + threadIdx.x;
       par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
     }
-    const C *w = (const C *)d.w + (long long)v * d.Nhs + row0 * L;
-#pragma unroll
-    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
-      const int r = e / L, p = e % L;
-      buf[p * LD + r] = w[(long long)r * L + p];
-    }
-    __syncthreads();
-    ct_fft_dif<L, PC, LD, 1>(buf, tw);
     if (!mbar_wait(&bar[st], (phase >> st) & 1)) failed = true;
     phase ^= 1u << st;
     const char *sb = smem + BUF + st * St::bytes;
+    const C *ws = (const C *)(sb + St::w);
+#pragma unroll
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, p = e % L;
+      buf[p * LD + r] = ws[r * L + p];
+    }
+    __syncthreads();
+    ct_fft_dif<L, PC, LD, 1>(buf, tw);
     const T *ts = (const T *)(sb + St::t);
     const R *us = (const R *)(sb + St::u), *ls = (const R *)(sb + St::lr);
     const R *q0s = (const R *)(sb + St::r0), *q1s = (const R *)(sb + St::r1);
@@ -591,6 +571,313 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   double *part = d.partials + (size_t)cta * kPartials;
   for (int k = threadIdx.x; k < kPartials; k += kThreads) part[k] = sums[k];
+}
+
+// ------------------------------------------------- FX with bulk staging
+// The iteration's FX (closure + forward x transform) with t, u and c_ref
+// staged by the bulk copy engine: a tile's PC rows of one site are one
+// contiguous block of each array, brought into shared memory while the
+// previous tile is transformed (two stages, one mbarrier each).
+template <typename P, int L, int PC>
+struct FxStage {
+  static constexpr int NX = 2 * L;
+  static constexpr size_t t = 0;
+  static constexpr size_t u = t + (size_t)PC * NX * sizeof(typename P::T);
+  static constexpr size_t cref = u + (size_t)PC * NX * sizeof(typename P::R);
+  static constexpr size_t bytes = cref + (size_t)PC * NX * sizeof(typename P::R);
+};
+#if R3D_CT_FP64
+size_t ct_smem_fxb(int L, int PC, size_t csz, size_t rsz, size_t tsz) {
+  const size_t buf = ((csz * (size_t)L * (PC + 1) + 127) / 128) * 128;
+  return buf + 2 * (size_t)PC * 2 * L * (tsz + 2 * rsz);
+}
+#endif
+
+template <typename P, int L, int PC>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_fx_bulk(Batch b, int per) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  using St = FxStage<P, L, PC>;
+  constexpr int LD = PC + 1, NX = 2 * L;
+  constexpr size_t BUF = ((sizeof(C) * (size_t)L * LD + 127) / 128) * 128;
+  extern __shared__ __align__(128) char smem[];
+  C *buf = (C *)smem;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int par[PC];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (d.ctl->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int ny = d.ny;
+  const int tps = (d.ny * d.nz) / PC;
+  const int ntile = d.n * tps;
+  const int first = cta * per;
+  const int count = min(per, ntile - first);
+  if (count <= 0) return;
+  const bool has_cref = d.cref != nullptr;
+  const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
+  const uint32_t tbytes = PC * NX * sizeof(T), rbytes = PC * NX * sizeof(R);
+  const uint32_t stage_tx = tbytes + rbytes + (has_cref ? rbytes : 0);
+  const Desc *dp = &d;
+  char *const stages = smem + BUF;
+  uint64_t *const bars = bar;
+  auto issue = [=](int tile, int st) {  // thread 0: the copies of one tile
+    const int v = tile / tps;
+    const long long base = (long long)v * dp->Ns + (long long)(tile % tps) * PC * NX;
+    char *sb = stages + st * St::bytes;
+    uint64_t *br = bars + st;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(br, stage_tx);
+    bulk_g2s(sb + St::t, (const T *)dp->t + base, tbytes, br);
+    bulk_g2s(sb + St::u, (const R *)dp->u + base, rbytes, br);
+    if (has_cref) bulk_g2s(sb + St::cref, (const R *)dp->cref + base, rbytes, br);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) issue(first, 0);
+  uint32_t phase = 0;  // bit st: parity of the next wait on stage st
+  bool failed = false;
+  int stop = -1;
+  for (int it = 0; it < count; ++it) {
+    const int tile = first + it, st = it & 1;
+    const int v = tile / tps;
+    const long long row0 = (long long)(tile % tps) * PC;
+    if (threadIdx.x == 0 && it + 1 < count) issue(tile + 1, st ^ 1);
+    if (threadIdx.x < PC) {
+      const long long row = row0 + threadIdx.x;
+      par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
+    }
+    if (!mbar_wait(&bar[st], (phase >> st) & 1)) failed = true;
+    phase ^= 1u << st;
+    __syncthreads();  // par
+    const char *sb = smem + BUF + st * St::bytes;
+    const T *ts = (const T *)(sb + St::t);
+    const R *us = (const R *)(sb + St::u), *cs = (const R *)(sb + St::cref);
+#pragma unroll 4
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, m = e % L;
+      const int i0 = r * NX + m, i1 = i0 + L;
+      // trm1mt on the short-range parts (calculate_cuda.cu:18-24)
+      const double t0 = ts[i0], t1 = ts[i1];
+      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)us[i0] + t0);
+      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)us[i1] + t1);
+      double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
+      if (has_cref) {
+        c0 -= (double)cs[i0];
+        c1 -= (double)cs[i1];
+      }
+      R f0 = (R)c0, f1 = (R)c1;
+      if ((m + par[r]) & 1) f0 = -f0;
+      if ((m + L + par[r]) & 1) f1 = -f1;
+      buf[digit_rev<L>(m) * LD + r] = cmul(C{f0, -f1}, pw[m]);
+    }
+    __syncthreads();
+    ct_fft_dit<L, PC, LD, -1>(buf, tw);
+    C *w = (C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, p = e % L;
+      w[(long long)r * L + p] = buf[p * LD + r];
+    }
+    if (__syncthreads_or(failed)) {  // buf, par and this stage are free again
+      stop = it;
+      break;
+    }
+  }
+  if (stop >= 0) {  // flag the solve, wait (bounded) for the copies in flight, give up
+    if (threadIdx.x == 0) atomicExch(&d.ctl->err, 1);
+    const int st = stop & 1;
+    mbar_wait(&bar[st], ((phase >> st) & 1) ^ 1);
+    if (stop + 1 < count) mbar_wait(&bar[st ^ 1], (phase >> (st ^ 1)) & 1);
+  }
+}
+
+// ------------------------------------------------------- warp tiles
+// The iteration's x passes with one tile of PCW rows per warp: each warp
+// loads, transforms (warp-synchronous radix stages) and stores its own tile,
+// so no warp waits at a CTA barrier and the warps of an SM overlap the
+// memory phases of some tiles with the transforms of others.  CTAs are
+// persistent; the warps of a solve's CTAs stride over its tiles.
+constexpr int kWarps = kThreads / 32;
+
+#if R3D_CT_FP64
+size_t ct_smem_warp(int L, int PCW, size_t csz) {
+  return (size_t)kWarps * L * (PCW + 1) * csz;
+}
+#endif
+
+template <typename P, int L, int PCW>
+__global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
+    k_fx_warp(Batch b) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  constexpr int LD = PCW + 1, NX = 2 * L;
+  extern __shared__ __align__(16) char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C *buf = (C *)smem + warp * (L * LD);
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (d.ctl->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si], nct = b.prefix[si + 1] - b.prefix[si];
+  const int ny = d.ny, tps = (d.ny * d.nz) / PCW, ntile = d.n * tps;
+  const bool has_cref = d.cref != nullptr;
+  const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *cref = (const R *)d.cref;
+  for (int tile = cta * kWarps + warp; tile < ntile; tile += nct * kWarps) {
+    const int v = tile / tps;
+    const long long row0 = (long long)(tile % tps) * PCW;
+    const long long base0 = (long long)v * d.Ns + row0 * NX;
+    const T *tt = t + base0;
+    const R *ut = u + base0, *ct = cref + (has_cref ? base0 : 0);
+    const int pr0 = (int)((row0 % ny + row0 / ny) & 1);
+    const int y0 = (int)(row0 % ny);
+#pragma unroll 1
+    for (int e = lane; e < PCW * L; e += 32) {
+      const int r = e / L, m = e % L;
+      const int i0 = r * NX + m, i1 = i0 + L;
+      // parity of row0 + r: (y + z) & 1, y wrapping into the next z-plane
+      const int par = (pr0 + r + ((y0 + r) >= ny ? 1 : 0) * (1 - ny)) & 1;
+      // trm1mt on the short-range parts (calculate_cuda.cu:18-24)
+      const double t0 = tt[i0], t1 = tt[i1];
+      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i0] + t0);
+      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i1] + t1);
+      double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
+      if (has_cref) {
+        c0 -= (double)ct[i0];
+        c1 -= (double)ct[i1];
+      }
+      R f0 = (R)c0, f1 = (R)c1;
+      if ((m + par) & 1) f0 = -f0;
+      if ((m + L + par) & 1) f1 = -f1;
+      buf[digit_rev<L>(m) * LD + r] = cmul(C{f0, -f1}, pw[m]);
+    }
+    __syncwarp();
+    ct_fft_dit_warp<L, PCW, LD, -1>(buf, tw, lane);
+    C *w = (C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll 4
+    for (int e = lane; e < PCW * L; e += 32) {
+      const int r = e / L, p = e % L;
+      w[(long long)r * L + p] = buf[p * LD + r];
+    }
+    __syncwarp();
+  }
+}
+
+// IX with warp tiles: the residual, its sum of squares and AN2's theta dots
+// (as k_ix_ct MODE 1).  Each warp keeps its own per-site sums (its tiles in
+// order), and the CTA adds the warps' sums in warp order, so the partials do
+// not depend on scheduling.
+template <typename P, int L, int PCW>
+__global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
+    k_ix_warp(Batch b) {
+  using R = typename P::R;
+  using T = typename P::T;
+  using C = typename Cx<R>::T;
+  constexpr int LD = PCW + 1, NX = 2 * L;
+  extern __shared__ __align__(16) char smem[];
+  __shared__ double wsum[kWarps][kPartials];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C *buf = (C *)smem + warp * (L * LD);
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (d.ctl->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si], nct = b.prefix[si + 1] - b.prefix[si];
+  const int ny = d.ny, tps = (d.ny * d.nz) / PCW, ntile = d.n * tps;
+  const bool dots = d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
+  const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
+  const T *t = (const T *)d.t;
+  const R *u = (const R *)d.u, *lr = (const R *)d.lr;
+  const R *rp = (const R *)d.hist_b;
+  R *res = (R *)d.res;
+  const long long niv = (long long)d.n * d.Ns;
+  for (int k = lane; k < kPartials; k += 32) wsum[warp][k] = 0;
+  double a_ss = 0, a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0;
+  int cur_v = -1;
+  auto flush = [&]() {  // warp-uniform
+    if (cur_v < 0) return;
+    double q[6] = {a_ss, a0, a1, a2, a3, a4};
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) q[k] += __shfl_xor_sync(0xffffffffu, q[k], o);
+    if (lane == 0) {
+      wsum[warp][0] += q[0];
+      if (dots)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) wsum[warp][1 + 5 * cur_v + k] += q[1 + k];
+    }
+    a_ss = a0 = a1 = a2 = a3 = a4 = 0;
+  };
+  __syncwarp();
+  for (int tile = cta * kWarps + warp; tile < ntile; tile += nct * kWarps) {
+    const int v = tile / tps;
+    const long long row0 = (long long)(tile % tps) * PCW;
+    if (v != cur_v) {
+      flush();
+      cur_v = v;
+    }
+    const C *w = (const C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll 4
+    for (int e = lane; e < PCW * L; e += 32) {
+      const int r = e / L, p = e % L;
+      buf[p * LD + r] = w[e];
+    }
+    __syncwarp();
+    ct_fft_dif_warp<L, PCW, LD, 1>(buf, tw, lane);
+    const long long base0 = (long long)v * d.Ns + row0 * NX;
+    const T *tt = t + base0;
+    const R *ut = u + base0, *lt = lr + base0, *p0t = rp + base0, *q0t = rp + niv + base0;
+    R *rt = res + base0;
+    const int pr0 = (int)((row0 % ny + row0 / ny) & 1);
+    const int y0 = (int)(row0 % ny);
+#pragma unroll 1
+    for (int e = lane; e < PCW * L; e += 32) {
+      const int r = e / L, m = e % L;
+      const int par = (pr0 + r + ((y0 + r) >= ny ? 1 : 0) * (1 - ny)) & 1;
+      const C zc = cmul(buf[digit_rev<L>(m) * LD + r], cconj(pw[m]));
+      R h0 = zc.x, h1 = -zc.y;
+      if ((m + par) & 1) h0 = -h0;
+      if ((m + L + par) & 1) h1 = -h1;
+      const int i0 = r * NX + m, i1 = i0 + L;
+      const double t0 = tt[i0], t1 = tt[i1];
+      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i0] + t0);
+      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i1] + t1);
+      const R r0 = (R)((double)h0 + (double)lt[i0] - g0);
+      const R r1 = (R)((double)h1 + (double)lt[i1] - g1);
+      rt[i0] = r0;
+      rt[i1] = r1;
+      a_ss += (double)r0 * r0 + (double)r1 * r1;
+      if (dots) {
+        const double p0 = p0t[i0], p1 = p0t[i1];
+        const double q0 = q0t[i0], q1 = q0t[i1];
+        const double t10 = (double)r0 - p0, t20 = (double)r0 - q0;
+        const double t11 = (double)r1 - p1, t21 = (double)r1 - q1;
+        a0 += r0 * t10 + r1 * t11;
+        a1 += r0 * t20 + r1 * t21;
+        a2 += t10 * t10 + t11 * t11;
+        a3 += t10 * t20 + t11 * t21;
+        a4 += t20 * t20 + t21 * t21;
+      }
+    }
+    __syncwarp();
+  }
+  flush();
+  __syncthreads();
+  double *part = d.partials + (size_t)cta * kPartials;
+  for (int k = threadIdx.x; k < kPartials; k += kThreads) {
+    double x = 0;
+#pragma unroll
+    for (int j = 0; j < kWarps; ++j) x += wsum[j][k];
+    part[k] = x;
+  }
 }
 
 // ------------------------------------------------------------ launchers
@@ -698,7 +985,103 @@ bool ct_launch_ixb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s
   }
   R3D_CT_LENGTHS(R3D_IXB)
 #undef R3D_IXB
+  // long rows: half the rows per tile, so that two stages fit
+#define R3D_IXB_HALF(LL)                                                        \
+  if (L == LL && PC == (sizeof(typename P::R) == 4 ? 4 : 2)) {                 \
+    constexpr int PCC = sizeof(typename P::R) == 4 ? 4 : 2;                     \
+    k_ix_bulk<P, LL, PCC><<<grid, kThreads, smem, s>>>(b, per);                \
+    return true;                                                                \
+  }
+  R3D_IXB_HALF(256)
+  R3D_IXB_HALF(512)
+#undef R3D_IXB_HALF
   return false;
+}
+
+template <typename P>
+bool ct_launch_fxb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s, int per) {
+#define R3D_FXB(LL)                                                             \
+  if (L == LL && PC == (sizeof(typename P::R) == 4 ? 8 : 4)) {                 \
+    constexpr int PCC = sizeof(typename P::R) == 4 ? 8 : 4;                     \
+    k_fx_bulk<P, LL, PCC><<<grid, kThreads, smem, s>>>(b, per);                \
+    return true;                                                                \
+  }
+  R3D_CT_LENGTHS(R3D_FXB)
+#undef R3D_FXB
+#define R3D_FXB_HALF(LL)                                                        \
+  if (L == LL && PC == (sizeof(typename P::R) == 4 ? 4 : 2)) {                 \
+    constexpr int PCC = sizeof(typename P::R) == 4 ? 4 : 2;                     \
+    k_fx_bulk<P, LL, PCC><<<grid, kThreads, smem, s>>>(b, per);                \
+    return true;                                                                \
+  }
+  R3D_FXB_HALF(256)
+  R3D_FXB_HALF(512)
+#undef R3D_FXB_HALF
+  return false;
+}
+
+// Resident CTAs per SM of the bulk-staged FX (which = 0) or IX (1) for
+// length L, PC rows per tile and `smem` dynamic bytes (0: not instantiated).
+template <typename P>
+int ct_occupancy_bulk(int which, int L, int PC, size_t smem) {
+  int nb = 0;
+#define R3D_OCC(LL, PCC)                                                              \
+  if (L == LL && PC == PCC) {                                                         \
+    if (which == 0)                                                                   \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_fx_bulk<P, LL, PCC>, kThreads, \
+                                                    smem);                            \
+    else                                                                              \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ix_bulk<P, LL, PCC>, kThreads, \
+                                                    smem);                            \
+    return nb;                                                                        \
+  }
+#define R3D_OCC_FULL(LL) R3D_OCC(LL, (sizeof(typename P::R) == 4 ? 8 : 4))
+  R3D_CT_LENGTHS(R3D_OCC_FULL)
+  R3D_OCC(256, (sizeof(typename P::R) == 4 ? 4 : 2))
+  R3D_OCC(512, (sizeof(typename P::R) == 4 ? 4 : 2))
+#undef R3D_OCC_FULL
+#undef R3D_OCC
+  return 0;
+}
+
+// warp-tile x passes: PCW = 4 rows per warp, 2 for rows of 256 or more
+// complex points
+template <typename P>
+bool ct_launch_xw(int which, int L, int PCW, Batch b, int grid, size_t smem, cudaStream_t s) {
+#define R3D_XW(LL, PP)                                               \
+  if (L == LL && PCW == PP) {                                        \
+    if (which == 0)                                                  \
+      k_fx_warp<P, LL, PP><<<grid, kThreads, smem, s>>>(b);          \
+    else                                                             \
+      k_ix_warp<P, LL, PP><<<grid, kThreads, smem, s>>>(b);          \
+    return true;                                                     \
+  }
+#define R3D_XW4(LL) R3D_XW(LL, 4)
+  R3D_CT_LENGTHS(R3D_XW4)
+  R3D_XW(256, 2)
+  R3D_XW(512, 2)
+#undef R3D_XW4
+#undef R3D_XW
+  return false;
+}
+template <typename P>
+int ct_occupancy_xw(int which, int L, int PCW, size_t smem) {
+  int nb = 0;
+#define R3D_OXW(LL, PP)                                                                  \
+  if (L == LL && PCW == PP) {                                                            \
+    if (which == 0)                                                                      \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_fx_warp<P, LL, PP>, kThreads, smem); \
+    else                                                                                 \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ix_warp<P, LL, PP>, kThreads, smem); \
+    return nb;                                                                           \
+  }
+#define R3D_OXW4(LL) R3D_OXW(LL, 4)
+  R3D_CT_LENGTHS(R3D_OXW4)
+  R3D_OXW(256, 2)
+  R3D_OXW(512, 2)
+#undef R3D_OXW4
+#undef R3D_OXW
+  return 0;
 }
 
 template <typename P>
@@ -716,9 +1099,20 @@ void ct_allow_smem_all() {
   allow_smem(k_fy_ct<P, LL, 16, 1>);                                      \
   allow_smem(k_zoz_ct<P, LL, 4>);                                         \
   allow_smem(k_zoz_ct<P, LL, 8>);                                         \
-  allow_smem(k_ix_bulk<P, LL, (sizeof(typename P::R) == 4 ? 8 : 4)>);
+  allow_smem(k_ix_bulk<P, LL, (sizeof(typename P::R) == 4 ? 8 : 4)>);      \
+  allow_smem(k_fx_bulk<P, LL, (sizeof(typename P::R) == 4 ? 8 : 4)>);       \
+  allow_smem(k_fx_warp<P, LL, 4>);                                        \
+  allow_smem(k_ix_warp<P, LL, 4>);
   R3D_CT_LENGTHS(R3D_ATTR)
 #undef R3D_ATTR
+  allow_smem(k_ix_bulk<P, 256, (sizeof(typename P::R) == 4 ? 4 : 2)>);
+  allow_smem(k_fx_bulk<P, 256, (sizeof(typename P::R) == 4 ? 4 : 2)>);
+  allow_smem(k_fx_bulk<P, 512, (sizeof(typename P::R) == 4 ? 4 : 2)>);
+  allow_smem(k_fx_warp<P, 256, 2>);
+  allow_smem(k_fx_warp<P, 512, 2>);
+  allow_smem(k_ix_warp<P, 256, 2>);
+  allow_smem(k_ix_warp<P, 512, 2>);
+  allow_smem(k_ix_bulk<P, 512, (sizeof(typename P::R) == 4 ? 4 : 2)>);
 }
 template void ct_allow_smem_all<PCT>();
 
@@ -727,5 +1121,9 @@ template bool ct_launch_fy<PCT>(int, int, Batch, int, size_t, cudaStream_t, int,
 template bool ct_launch_zoz<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
 template bool ct_launch_ix<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
 template bool ct_launch_ixb<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
+template bool ct_launch_fxb<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
+template int ct_occupancy_bulk<PCT>(int, int, int, size_t);
+template bool ct_launch_xw<PCT>(int, int, int, Batch, int, size_t, cudaStream_t);
+template int ct_occupancy_xw<PCT>(int, int, int, size_t);
 
 }  // namespace r3d

@@ -271,6 +271,13 @@ def run_gpu(args, rank, world, local):
     achieved = kbytes / (kms * 1e-3) / 1e9
     iter_bytes = sum(b for _, _, b in prof)
 
+    batch = serve = None
+    if rank == 0 and world == 1 and not custom:
+        if not args.no_batch:
+            batch = run_batch_screen(local)
+        if not args.no_serve:
+            serve = run_served(local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and not custom:
         rate, cores, sample = cpu_oracle_rate(CPU_SAMPLE_ITERS, 1)
@@ -310,6 +317,8 @@ def run_gpu(args, rank, world, local):
             "kernels": [{"name": n, "ms": m, "bytes": b, "gbs": b / (m * 1e-3) / 1e9}
                         for n, m, b in prof],
             "fp64": fp64,
+            "batched_screen": batch,
+            "served": serve,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
@@ -317,6 +326,191 @@ def run_gpu(args, rank, world, local):
     shutil.rmtree(tmp, ignore_errors=True)
     if dist:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------- batched and served solves
+def _sfe_kcal(path):
+    for ln in open(path):
+        if ln.startswith("SFE_SC="):
+            return float(ln.split()[1]) / 4184.0
+    return None
+
+
+def _solvents(d):
+    for name in ("h2o_vv", "naclaq_vv"):
+        with gzip.open(os.path.join(ROOT, "tests", "golden", name + ".xvk.gz"), "rb") as fi, \
+                open(os.path.join(d, name + ".xvk"), "wb") as fo:
+            shutil.copyfileobj(fi, fo)
+
+
+def run_batch_screen(local):
+    """64 seeded drug-like solutes (8-60 atoms) on 48^3-128^3 grids, water,
+    PSE-3 reached as KH -> PSE-2 -> PSE-3: mixed precision through one batch
+    (r3d_batch_*) against the plain FP64 path solving them one by one.  Both
+    timed end to end from the deck files to the .xmu files."""
+    import rism3d as R
+    import synthetic as S
+    d = tempfile.mkdtemp(prefix="r3dc4_")
+    _solvents(d)
+    decks = S.c4_decks(d)
+    ladder = [(R.KH, 1), (R.PSE, 2), (R.PSE, 3)]
+    # mixed, batched
+    t0 = time.perf_counter()
+    ss = []
+    for p in decks:
+        s = R.RISM3D(device=local, precision="mixed")
+        s.load(p)
+        s.set_closure(*ladder[0])
+        s.initialize()
+        ss.append(s)
+    b = R.Batch(local)
+    for s in ss:
+        b.add(s)
+    iters, ms = 0, 0.0
+    for st in ladder:
+        for s in ss:
+            s.set_closure(*st)
+        it, m = b.iterate()
+        iters += it
+        ms += m
+    mixed_status = [s.status()[2] for s in ss]
+    sfe_mixed = []
+    for i, s in enumerate(ss):
+        p = os.path.join(d, f"m{i}.xmu")
+        s.output(p)
+        sfe_mixed.append(_sfe_kcal(p))
+    t_mixed = time.perf_counter() - t0
+    info = b.info()
+    b.close()
+    for s in ss:
+        s.close()
+    # mixed, served: the same decks submitted at once; each solve moves to
+    # its next closure stage and retires on its own (continuous batching)
+    t0 = time.perf_counter()
+    srv = R.Server(device=local, precision="mixed")
+    tickets = [srv.submit(p) for p in decks]
+    res = [srv.wait(t, 600.0) for t in tickets]
+    t_served = time.perf_counter() - t0
+    sfe_served = []
+    for i, (t, r) in enumerate(zip(tickets, res)):
+        if r["state"] == "done" and r["status"] == "converged":
+            q = os.path.join(d, f"s{i}.xmu")
+            srv.write_xmu(t, q)
+            sfe_served.append(_sfe_kcal(q))
+        else:
+            sfe_served.append(None)
+    srv.close()
+    # plain FP64, one solve at a time
+    t0 = time.perf_counter()
+    sfe64, st64 = [], []
+    for i, p in enumerate(decks):
+        s = R.RISM3D(device=local, precision="fp64")
+        s.load(p)
+        s.set_closure(*ladder[0])
+        s.initialize()
+        for st in ladder:
+            s.set_closure(*st)
+            status = s.iterate()[2]
+        st64.append(status)
+        q = os.path.join(d, f"f{i}.xmu")
+        s.output(q)
+        sfe64.append(_sfe_kcal(q))
+        s.close()
+    t64 = time.perf_counter() - t0
+    err = sorted(abs(a - b) for a, b, x, y in zip(sfe_mixed, sfe64, mixed_status, st64)
+                 if x == y == "converged")
+    err_served = sorted(abs(a - b) for a, b in zip(sfe_served, sfe64) if a is not None
+                        and b is not None)
+    grids = {}
+    for p in decks:
+        g = open(p).read().split("\n")[6].split()[0]
+        grids[g + "^3"] = grids.get(g + "^3", 0) + 1
+    shutil.rmtree(d, ignore_errors=True)
+    return {
+        "workload": "64 seeded solutes of 8-60 atoms, water (n=2), PSE-3 via KH->PSE-2->PSE-3, "
+                    "AN2 (2 0.6 0.2), RMS 1e-6",
+        "grids": grids, "solutes": len(decks),
+        "mixed_batched": {"solves_per_s": len(decks) / t_mixed, "wall_s": t_mixed,
+                          "iterations": iters, "device_ms": ms,
+                          "converged": mixed_status.count("converged"), **info},
+        "mixed_served": {"solves_per_s": len(decks) / t_served, "wall_s": t_served,
+                         "converged": sum(r["status"] == "converged" for r in res)},
+        "fp64_single": {"solves_per_s": len(decks) / t64, "wall_s": t64,
+                        "converged": st64.count("converged")},
+        "speedup_vs_fp64_single": {"batched": t64 / t_mixed, "served": t64 / t_served},
+        "sfe_err_kcal": {"max": err[-1] if err else None,
+                         "p50": err[len(err) // 2] if err else None, "n": len(err)},
+        "sfe_err_kcal_served": {"max": err_served[-1] if err_served else None,
+                                "n": len(err_served)},
+    }
+
+
+def run_served(local, rates=(10.0, 30.0, 100.0), count=48):
+    """The served stream: Poisson arrivals of seeded solutes (8-500 atoms,
+    64^3-192^3 grids, water or 0.2 M NaCl, KH or PSE-2) into one server
+    (r3d_server_*: continuous batching); latency = finish - submit."""
+    import numpy as np
+    import rism3d as R
+    import synthetic as S
+    d = tempfile.mkdtemp(prefix="r3dc5_")
+    _solvents(d)
+    reqs = S.c5_requests(d, count)
+
+    def stream(srv, rate, seed):
+        gaps = np.random.default_rng(seed).exponential(1.0 / rate, len(reqs))
+        t0 = time.perf_counter()
+        due, tickets = 0.0, []
+        for (p, _), gap in zip(reqs, gaps):
+            due += gap
+            while time.perf_counter() - t0 < due:
+                time.sleep(0.0002)
+            tickets.append(srv.submit(p))
+        res = [srv.wait(t, 600.0) for t in tickets]
+        lat = sorted(r["finished_s"] - r["queued_s"] for r in res)
+        span = max(r["finished_s"] for r in res) - min(r["queued_s"] for r in res)
+        out = {"rate_per_s": rate, "requests": len(res),
+               "done": sum(r["state"] == "done" for r in res),
+               "converged": sum(r["status"] == "converged" for r in res),
+               "p50_s": lat[len(lat) // 2], "p99_s": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+               "solves_per_s": len(res) / span}
+        return out, tickets, res
+
+    lines = {}
+    sfe = {}
+    for prec, rs in (("mixed", rates), ("fp64", rates[:1])):
+        srv = R.Server(device=local, precision=prec)
+        w = srv.submit(reqs[0][0])  # loads the kernels
+        srv.wait(w, 600.0)
+        srv.release(w)
+        lines[prec] = []
+        for k, rate in enumerate(rs):
+            out, tickets, res = stream(srv, rate, 100 + k)
+            lines[prec].append(out)
+            if k == 0:
+                vals = []
+                for i, (t, r) in enumerate(zip(tickets, res)):
+                    if r["state"] == "done" and r["status"] == "converged":
+                        q = os.path.join(d, f"{prec}{i}.xmu")
+                        srv.write_xmu(t, q)
+                        vals.append(_sfe_kcal(q))
+                    else:
+                        vals.append(None)
+                sfe[prec] = vals
+            for t in tickets:
+                srv.release(t)
+        srv.close()
+    err = sorted(abs(a - b) for a, b in zip(sfe["mixed"], sfe["fp64"])
+                 if a is not None and b is not None)
+    grids = {}
+    for p, _ in reqs:
+        g = open(p).read().split("\n")[6].split()[0] + "^3"
+        grids[g] = grids.get(g, 0) + 1
+    shutil.rmtree(d, ignore_errors=True)
+    return {"workload": f"{count} seeded requests per rate: 8-500 atoms (log-uniform), "
+                        "water or 0.2 M NaCl, KH or PSE-2 (via KH), AN2, RMS 1e-6",
+            "grids": grids, "mixed": lines["mixed"], "fp64": lines["fp64"],
+            "sfe_err_kcal": {"max": err[-1] if err else None,
+                             "p50": err[len(err) // 2] if err else None, "n": len(err)}}
 
 
 # ------------------------------------------------------- reference arm
@@ -355,6 +549,8 @@ def main():
     ap.add_argument("--atoms", type=int, default=2000, help="profiling only: solute atoms")
     ap.add_argument("--e2e-reps", type=int, default=3, help="warm end-to-end solves timed")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
