@@ -881,7 +881,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
 }
 
 // ------------------------------------------------------------ launchers
-#define R3D_CT_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
+#define R3D_CT_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(72) X(80) X(96) X(128) X(144) X(160) X(192) X(256) X(512)
 
 #if R3D_CT_FP64
 size_t ct_smem_x(int L, int PC, size_t csz) { return csz * (size_t)L * (PC + 1); }

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kThreads)
 // ------------------------------------------------------------ launchers
 // x-columns per tile: FY 8 (FP32) / 4 (FP64), ZOZ 4 / 2 -- rows of 32 to
 // 64 bytes; lengths up to 512 (two tensor copies per column beyond 256)
-#define R3D_TMA_LENGTHS(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(512)
+#define R3D_TMA_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(72) X(80) X(96) X(128) X(144) X(160) X(192) X(256) X(512)
 
 template <typename P>
 constexpr int tma_pc_y() {

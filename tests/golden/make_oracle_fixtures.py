@@ -33,12 +33,34 @@ CASES = {
     "s_rect_pse3_anm10": ("s_rect", PSE, 3, ANM, 10, 0.3),
     "s64kh_pse2": ("s64kh", PSE, 2, AN2, 2, -1.0),
     "s64nacl_anm10": ("s64nacl", KH, 1, ANM, 10, 0.3),
+    "g80kh": ("g80kh", KH, 1, AN2, 2, -1.0),
+    "g80x72x96": ("g80x72x96", KH, 1, AN2, 2, -1.0),
 }
 SOLVENTS = ["h2o_vv", "naclaq_vv", "kclaq_vv", "ctip3p"]
 
+# grids outside the reference's power-of-two decks (lengths 40, 72, 80, 96 of
+# the served configurations): decks written here from the seeded recipe
+# case -> (nu, grid, box, solvent, seed)
+GRID_CASES = {
+    "g80kh": (12, (80, 80, 80), (40.0, 40.0, 40.0), "h2o_vv.xvk", 81),
+    "g80x72x96": (12, (80, 72, 96), (40.0, 36.0, 48.0), "naclaq_vv.xvk", 82),
+}
+
+
+def write_grid_deck(case):
+    sys.path.insert(0, os.path.join(HERE, "..", "..", "3d-rism-cuda-mpi_b200"))
+    import synthetic as S
+    nu, grid, box, solv, seed = GRID_CASES[case]
+    dst = os.path.join(HERE, "oracle")
+    os.makedirs(dst, exist_ok=True)
+    return S.small(dst, nu=nu, grid=grid, box=box, solvent=solv, seed=seed, name=case)
+
 
 def materialise(deck, d):
-    inp = shutil.copyfile(os.path.join(HERE, "ref", deck + ".inp"), os.path.join(d, deck + ".inp"))
+    src = os.path.join(HERE, "ref", deck + ".inp")
+    if not os.path.exists(src):
+        src = os.path.join(HERE, "oracle", deck + ".inp")
+    inp = shutil.copyfile(src, os.path.join(d, deck + ".inp"))
     txt = open(inp).read()
     for k in SOLVENTS:
         if k + ".xvk" in txt:
@@ -57,6 +79,8 @@ def main(only=None):
     for case, (deck, clos, pse_n, mixer, hist, damp) in CASES.items():
         if only and case not in only:
             continue
+        if deck in GRID_CASES:
+            write_grid_deck(deck)
         inp, xvk = materialise(deck, tmp)
         o = O.Oracle(inp, xvk=xvk)
         o.set_closure(clos, pse_n)
