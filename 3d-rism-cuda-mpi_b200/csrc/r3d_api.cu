@@ -196,6 +196,12 @@ struct r3d_ctx {
        *fk = nullptr, *chi = nullptr, *lr = nullptr, *hist_a = nullptr,
        *hist_b = nullptr, *cref = nullptr, *chi64 = nullptr;
   double next_refresh = 0;  // mixed path: refresh when rms drops below this
+  // mixed path: the refresh's FP64 geometry and work buffer, kept from the
+  // first refresh on (the FP64 path refreshes once, at setup, and frees it)
+  bool rplanned = false;
+  Desc rdesc{};
+  Geo rgeo;
+  char *rtmp = nullptr;
   void *tw64 = nullptr, *tw32 = nullptr;  // compile-time engine twiddles
   uint32_t *kidx = nullptr;
   double *partials = nullptr, *scratch = nullptr;
@@ -258,6 +264,7 @@ static void free_all(r3d_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   c->allocs.clear();
   c->bytes = 0;
+  c->rtmp = nullptr;
   c->initialized = false;
 }
 
@@ -458,6 +465,7 @@ extern "C" int r3d_set_control(r3d_ctx *c, double convergence, int maxstep) {
 
 // ------------------------------------------------------------ geometry
 static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites);
+static bool ixb_config(int device, const Desc &d, bool fp64, int pcb, Geo &g);
 static int plan_geometry(r3d_ctx *c, Desc &d) {
   return plan_geo(c, d, c->geo, c->fp64, c->prob.natv);
 }
@@ -529,21 +537,9 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   g.ix_ctas = (d.tiles_x + g.ix_per - 1) / g.ix_per;
   g.ixb_pc = 0;
   if (d.ct_x) {  // bulk-staged IX: as many CTAs as stay resident
-    int pcb = fp64 ? 4 : 8;
-    size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
-    if (sm > kSmemMax && d.hx >= 256) {  // long rows: half the rows per tile
-      pcb /= 2;
-      sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
-    }
-    if (rowsN % pcb == 0 && sm <= kSmemMax) {
-      const int tiles = d.n * (rowsN / pcb);
-      const int per_sm = bulk_per_sm(c->opts.device, fp64, 1, d.hx, pcb, sm);
-      g.ixb_pc = pcb;
-      g.smixb = sm;
-      g.ixb_ctas = std::min(tiles, kNumSM * per_sm);
-      g.ixb_per = (tiles + g.ixb_ctas - 1) / g.ixb_ctas;
-      g.ixb_ctas = (tiles + g.ixb_per - 1) / g.ixb_per;
-    }
+    const int pcb = fp64 ? 4 : 8;
+    if (!ixb_config(c->opts.device, d, fp64, pcb, g) && d.hx >= 256)
+      ixb_config(c->opts.device, d, fp64, pcb / 2, g);  // long rows: half the rows per tile
   }
   g.fxb_pc = 0;
   if (d.ct_x) {  // bulk-staged FX, sized like the IX above
@@ -619,6 +615,22 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   const int bps = c->opts.device >= 0 ? dot_blocks_per_sm(fp64) : 4;
   g.dot_ctas = (int)std::min<long long>((d.N + kThreads - 1) / kThreads, (long long)nsm * bps);
   return R3D_OK;
+}
+
+// Geometry of the bulk-staged IX with pcb rows per tile (false: does not fit).
+static bool ixb_config(int device, const Desc &d, bool fp64, int pcb, Geo &g) {
+  const size_t cs = fp64 ? 16 : 8;
+  const int rowsN = d.ny * d.nz;
+  const size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
+  if (rowsN % pcb || sm > kSmemMax) return false;
+  const int tiles = d.n * (rowsN / pcb);
+  const int per_sm = bulk_per_sm(device, fp64, 1, d.hx, pcb, sm);
+  g.ixb_pc = pcb;
+  g.smixb = sm;
+  g.ixb_ctas = std::min(tiles, kNumSM * per_sm);
+  g.ixb_per = (tiles + g.ixb_ctas - 1) / g.ixb_ctas;
+  g.ixb_ctas = (tiles + g.ixb_per - 1) / g.ixb_per;
+  return true;
 }
 
 // ---------------------------------------------------------- pass dispatch
@@ -843,6 +855,12 @@ static void set_twiddles64(const void *t64, Desc &d) {
   d.pwz = p + 2 * d.hx + 2 * d.ny + d.nz;
 }
 
+// device bytes of the refresh's work buffer: FP64 c_ref / h_ref, n half
+// spectra, descriptor, control block, launch prefixes
+static size_t refresh_bytes(const Desc &d) {
+  return (size_t)d.n * d.Ns * 8 + (size_t)d.n * d.Nhs * 16 + sizeof(Desc) + sizeof(Ctl) + 64;
+}
+
 // Refresh (also the setup's long-range term): freeze c_ref = c_s(t) (zero at
 // setup) and set lr = 1 + h_ref, h_ref = F^-1[chi (F(c_ref) - q phi_L(k))],
 // with the FP64 pass kernels.  Leaves t, R and the mixer state untouched: the
@@ -853,13 +871,24 @@ static int refresh(r3d_ctx *c, bool zero) {
   const int n = d.n;
   const long long N = d.Ns, Nh = d.Nhs;  // padded site strides
   cudaStream_t s = c->stream;
-  Desc dr{};
-  Geo g;
-  int rc = plan_geo(c, dr, g, true, n);
-  if (rc) return rc;
-  char *tmp = nullptr;
-  const size_t bytes = (size_t)n * N * 8 + (size_t)n * Nh * 16 + sizeof(Desc) + sizeof(Ctl) + 64;
-  CK(cudaMalloc((void **)&tmp, bytes));
+  if (!c->rplanned) {
+    int rc = plan_geo(c, c->rdesc, c->rgeo, true, n);
+    if (rc) return rc;
+    c->rplanned = true;
+  }
+  Desc dr = c->rdesc;
+  const Geo &g = c->rgeo;
+  const size_t bytes = refresh_bytes(d);
+  char *tmp = c->rtmp;
+  if (!tmp) {
+    if (c->fp64) {
+      CK(cudaMalloc((void **)&tmp, bytes));
+    } else {
+      int rc = dalloc(c, (void **)&c->rtmp, bytes);
+      if (rc) return rc;
+      tmp = c->rtmp;
+    }
+  }
   double *c64 = (double *)tmp;                      // c_ref, then h_ref
   double2 *w64 = (double2 *)(c64 + (size_t)n * N);  // n half spectra
   Desc *dd = (Desc *)(w64 + (size_t)n * Nh);
@@ -893,7 +922,7 @@ static int refresh(r3d_ctx *c, bool zero) {
   launch_lr_update<P>(c64, c->lr, (long long)n * N, s);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
-  cudaFree(tmp);
+  if (tmp != c->rtmp) cudaFree(tmp);
   return R3D_OK;
 }
 
@@ -904,6 +933,7 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   b += n * N * R;                  // w (n half spectra)
   b += N * R + N * 8;              // fr, fk (FP64 half spectrum)
   if (!c->fp64) b += n * N * R + (size_t)nshell * n * n * 8;  // cref, chi64
+  b += refresh_bytes(d);           // refresh work buffer (kept on the mixed path)
   b += (size_t)d.Nh * 4;           // kidx
   b += (size_t)nshell * n * n * R;
   size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
@@ -939,8 +969,8 @@ static int autotune_x(r3d_ctx *c) {
   if (const char *ev = getenv("R3D_X_VARIANT")) {
     const int k = std::atoi(ev);
     const bool fx = k == 0 || (k == 1 && g.fxb_pc) || (k == 2 && g.fxw_pc);
-    const bool ix = k == 0 || (k == 1 && g.ixb_pc) || (k == 2 && g.ixw_pc);
-    use = {fx ? k : 0, ix ? k : 0, g.yz_tma};
+    const bool ix = k == 0 || ((k == 1 || k == 3) && g.ixb_pc) || (k == 2 && g.ixw_pc);
+    use = {fx ? std::min(k, 2) : 0, ix ? k : 0, g.yz_tma};
     if (const char *ey = getenv("R3D_YZ_VARIANT")) {
       const int k = std::atoi(ey);
       use[2] = (k == 1 && !d.ct_z) ? 0 : std::min(k, g.yz_tma);
@@ -964,10 +994,13 @@ static int autotune_x(r3d_ctx *c) {
   if (!known) {
     cudaStream_t s = c->stream;
     int *pf = nullptr;
-    CK(cudaMalloc((void **)&pf, 20 * sizeof(int)));
-    const int pre[20] = {0, d.tiles_x, 0, g.fxb_ctas, 0, g.fxw_ctas, 0, g.ix_ctas,
+    // the bulk IX with half the rows per tile (more CTAs per SM)
+    Geo half = g;
+    const bool has_half = g.ixb_pc >= 4 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, half);
+    CK(cudaMalloc((void **)&pf, 22 * sizeof(int)));
+    const int pre[22] = {0, d.tiles_x, 0, g.fxb_ctas, 0, g.fxw_ctas, 0, g.ix_ctas,
                          0, g.ixb_ctas, 0, g.ixw_ctas, 0, g.tiles_y, 0, g.tiles_z,
-                         0, g.fyt_ctas, 0, g.zt_ctas};
+                         0, g.fyt_ctas, 0, g.zt_ctas, 0, half.ixb_ctas};
     CK(copy_h2d(c, pf, pre, sizeof(pre), s));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -996,6 +1029,15 @@ static int autotune_x(r3d_ctx *c) {
             time([&] { pass_ix<P>(d, o, Batch{c->ddesc, pf + 6 + 2 * k, 1}, s, 1, nullptr); });
         if (k == 0 || ms < best[1]) best[1] = ms, use[1] = k;
       }
+      if (k == 1 && has_half) {  // variant 3: bulk IX, half the rows per tile
+        Geo o3 = only(1);
+        o3.ixb_pc = half.ixb_pc;
+        o3.smixb = half.smixb;
+        o3.ixb_ctas = half.ixb_ctas;
+        o3.ixb_per = half.ixb_per;
+        const float ms = time([&] { pass_ix<P>(d, o3, Batch{c->ddesc, pf + 20, 1}, s, 1, nullptr); });
+        if (ms < best[1]) best[1] = ms, use[1] = 3;
+      }
     }
     if (g.yz_tma) {  // the y/z trio: tile-per-CTA, copy-engine y, copy-engine y and z
       float best2 = 0;
@@ -1023,7 +1065,11 @@ static int autotune_x(r3d_ctx *c) {
   }
   if (use[0] != 1) g.fxb_pc = 0;
   if (use[0] != 2) g.fxw_pc = 0;
-  if (use[1] != 1) g.ixb_pc = 0;
+  if (use[1] == 3) {
+    if (!(g.ixb_pc >= 4 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, g))) g.ixb_pc = 0;
+  } else if (use[1] != 1) {
+    g.ixb_pc = 0;
+  }
   if (use[1] != 2) g.ixw_pc = 0;
   g.yz_tma = use[2];
   return R3D_OK;

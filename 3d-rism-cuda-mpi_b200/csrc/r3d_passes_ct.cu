@@ -409,8 +409,9 @@ size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz) {
 }
 #endif
 
+// half-size tiles (PC 4 / 2) are the occupancy variant: three CTAs per SM
 template <typename P, int L, int PC>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8 : 4) ? 3 : 1)
     k_ix_bulk(Batch b, int per) {
   using R = typename P::R;
   using T = typename P::T;
@@ -985,15 +986,14 @@ bool ct_launch_ixb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s
   }
   R3D_CT_LENGTHS(R3D_IXB)
 #undef R3D_IXB
-  // long rows: half the rows per tile, so that two stages fit
+  // half the rows per tile: long rows (two stages fit) and the occupancy variant
 #define R3D_IXB_HALF(LL)                                                        \
   if (L == LL && PC == (sizeof(typename P::R) == 4 ? 4 : 2)) {                 \
     constexpr int PCC = sizeof(typename P::R) == 4 ? 4 : 2;                     \
     k_ix_bulk<P, LL, PCC><<<grid, kThreads, smem, s>>>(b, per);                \
     return true;                                                                \
   }
-  R3D_IXB_HALF(256)
-  R3D_IXB_HALF(512)
+  R3D_CT_LENGTHS(R3D_IXB_HALF)
 #undef R3D_IXB_HALF
   return false;
 }
@@ -1040,6 +1040,15 @@ int ct_occupancy_bulk(int which, int L, int PC, size_t smem) {
   R3D_OCC(256, (sizeof(typename P::R) == 4 ? 4 : 2))
   R3D_OCC(512, (sizeof(typename P::R) == 4 ? 4 : 2))
 #undef R3D_OCC_FULL
+  // the IX's half-size tiles at the other lengths
+#define R3D_OCC_IXH(LL)                                                                    \
+  if (which == 1 && L == LL && PC == (sizeof(typename P::R) == 4 ? 4 : 2)) {              \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                         \
+        &nb, k_ix_bulk<P, LL, (sizeof(typename P::R) == 4 ? 4 : 2)>, kThreads, smem);      \
+    return nb;                                                                             \
+  }
+  R3D_CT_LENGTHS(R3D_OCC_IXH)
+#undef R3D_OCC_IXH
 #undef R3D_OCC
   return 0;
 }
@@ -1100,19 +1109,18 @@ void ct_allow_smem_all() {
   allow_smem(k_zoz_ct<P, LL, 4>);                                         \
   allow_smem(k_zoz_ct<P, LL, 8>);                                         \
   allow_smem(k_ix_bulk<P, LL, (sizeof(typename P::R) == 4 ? 8 : 4)>);      \
+  allow_smem(k_ix_bulk<P, LL, (sizeof(typename P::R) == 4 ? 4 : 2)>);      \
   allow_smem(k_fx_bulk<P, LL, (sizeof(typename P::R) == 4 ? 8 : 4)>);       \
   allow_smem(k_fx_warp<P, LL, 4>);                                        \
   allow_smem(k_ix_warp<P, LL, 4>);
   R3D_CT_LENGTHS(R3D_ATTR)
 #undef R3D_ATTR
-  allow_smem(k_ix_bulk<P, 256, (sizeof(typename P::R) == 4 ? 4 : 2)>);
   allow_smem(k_fx_bulk<P, 256, (sizeof(typename P::R) == 4 ? 4 : 2)>);
   allow_smem(k_fx_bulk<P, 512, (sizeof(typename P::R) == 4 ? 4 : 2)>);
   allow_smem(k_fx_warp<P, 256, 2>);
   allow_smem(k_fx_warp<P, 512, 2>);
   allow_smem(k_ix_warp<P, 256, 2>);
   allow_smem(k_ix_warp<P, 512, 2>);
-  allow_smem(k_ix_bulk<P, 512, (sizeof(typename P::R) == 4 ? 4 : 2)>);
 }
 template void ct_allow_smem_all<PCT>();
 
