@@ -163,6 +163,7 @@ struct Geo {
   // per tile, CTAs, tiles per CTA, shared memory
   int ixb_pc = 0, ixb_ctas = 0, ixb_per = 1;
   size_t smixb = 0;
+  int ixh_ctas = 0;  // CTAs of the same with half the rows per tile (autotuner's variant)
   // the iteration's FX with bulk-staged inputs (fxb_pc = 0: not used)
   int fxb_pc = 0, fxb_ctas = 0, fxb_per = 1;
   size_t smfxb = 0;
@@ -205,6 +206,7 @@ struct r3d_ctx {
   void *tw64 = nullptr, *tw32 = nullptr;  // compile-time engine twiddles
   uint32_t *kidx = nullptr;
   double *partials = nullptr, *scratch = nullptr;
+  int npart = 0;  // rows of partials
   size_t scratch_bytes = 0;
   Ctl *ctl = nullptr;
   Desc *ddesc = nullptr;
@@ -540,6 +542,9 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
     const int pcb = fp64 ? 4 : 8;
     if (!ixb_config(c->opts.device, d, fp64, pcb, g) && d.hx >= 256)
       ixb_config(c->opts.device, d, fp64, pcb / 2, g);  // long rows: half the rows per tile
+    Geo h = g;  // the half-size tiles the autotuner may choose write as many partials rows
+    g.ixh_ctas = (g.ixb_pc >= 4 && ixb_config(c->opts.device, d, fp64, g.ixb_pc / 2, h))
+                     ? h.ixb_ctas : 0;
   }
   g.fxb_pc = 0;
   if (d.ct_x) {  // bulk-staged FX, sized like the IX above
@@ -691,7 +696,9 @@ static int iter_ix_ctas(const Geo &g) {
 }
 // rows of partials the iteration's IX may need, whichever variant runs
 static int max_ix_ctas(const Geo &g) {
-  return std::max(std::max(g.ix_ctas, g.ixb_pc ? g.ixb_ctas : 0), g.ixw_pc ? g.ixw_ctas : 0);
+  return std::max(std::max(std::max(g.ix_ctas, g.ixb_pc ? g.ixb_ctas : 0),
+                           g.ixw_pc ? g.ixw_ctas : 0),
+                  g.ixh_ctas);
 }
 // CTAs of the iteration's FX
 static int iter_fx_ctas(const Geo &g) {
@@ -996,7 +1003,9 @@ static int autotune_x(r3d_ctx *c) {
     int *pf = nullptr;
     // the bulk IX with half the rows per tile (more CTAs per SM)
     Geo half = g;
-    const bool has_half = g.ixb_pc >= 4 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, half);
+    const bool has_half = g.ixb_pc >= 4 &&
+                          ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, half) &&
+                          half.ixb_ctas <= c->npart;
     CK(cudaMalloc((void **)&pf, 22 * sizeof(int)));
     const int pre[22] = {0, d.tiles_x, 0, g.fxb_ctas, 0, g.fxw_ctas, 0, g.ix_ctas,
                          0, g.ixb_ctas, 0, g.ixw_ctas, 0, g.tiles_y, 0, g.tiles_z,
@@ -1105,6 +1114,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
   const int npart = std::max(max_ix_ctas(c->geo), c->geo.dot_ctas);
   if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;
+  c->npart = npart;
   double *rmslog;
   if ((rc = dalloc(c, (void **)&rmslog, (size_t)(p.maxstep + 1) * 8))) return rc;
   if ((rc = dalloc(c, (void **)&c->ctl, sizeof(Ctl)))) return rc;
@@ -1259,6 +1269,9 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     CK(copy_h2d(c, c->ctl, &h, sizeof(Ctl), s));
     CK(copy_h2d(c, c->ddesc, &d, sizeof(Desc), s));
     if ((rc = autotune_x<P>(c))) return rc;
+    // every IX variant writes one row of partials per CTA
+    if (std::max(iter_ix_ctas(c->geo), c->geo.dot_ctas) > c->npart)
+      return fail(c, R3D_ECUDA, "internal: partials rows for the chosen IX variant");
     const std::vector<int> pre = make_prefix(c->geo, 1);
     CK(copy_h2d(c, c->dprefix, pre.data(), pre.size() * sizeof(int), s));
     CK(cudaStreamSynchronize(s));

@@ -35,6 +35,7 @@
 // iteration never applies it.  All passes take a descriptor table so that one
 // launch can serve many solves of different grids (batching).
 #include <cuda_runtime.h>
+#include <type_traits>
 #include <math.h>
 #include <stdint.h>
 
@@ -597,7 +598,13 @@ __global__ void __launch_bounds__(kThreads)
 template <typename P>
 __global__ void __launch_bounds__(kThreads)
     k_anm_dots(Batch b) {
+  // The dots of the new residual with itself and with the stored residuals,
+  // eight slots per pass: each pass reads the residual once and its slots
+  // once, with 16-byte vector loads.
   using R = typename P::R;
+  using V = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
+  constexpr int VEC = 16 / sizeof(R);
+  constexpr int G = 8;
   __shared__ double red[kThreads / 32];
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
@@ -610,21 +617,58 @@ __global__ void __launch_bounds__(kThreads)
   const R *f = (const R *)d.hist_a;
   const R *res = (const R *)d.res;
   double *part = d.partials + (size_t)cta * kPartials;
-  for (int i = 0; i <= c->hcount; ++i) {
-    // i == 0: self dot; i >= 1: history slot (head - i) mod H1
-    int slot = (c->hhead - i + 2 * H1) % H1;
-    const R *fi = i == 0 ? res : f + (long long)slot * niv;
-    double acc = 0;
-    for (int v = 0; v < d.n; ++v) {
-      double sv = 0;
-      const R *a = res + (long long)v * d.Ns, *bq = fi + (long long)v * d.Ns;
-      for (long long x = (long long)cta * blockDim.x + threadIdx.x; x < d.N;
-           x += (long long)nct * blockDim.x)
-        sv += (double)a[x] * (double)bq[x];
-      acc += sv * d.irho[v];
+  const int m = c->hcount;
+  // vector loads when every site's block starts on a 16-byte boundary
+  const long long nv = d.Ns % VEC == 0 ? d.N / VEC : 0;
+  const long long stride = (long long)nct * blockDim.x;
+  for (int i0 = 0; i0 <= m; i0 += G) {
+    const int ng = min(G, m + 1 - i0);
+    const R *src[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      // i == 0: self dot; i >= 1: history slot (head - i) mod H1
+      const int i = i0 + g;
+      const int slot = (c->hhead - i + 2 * H1) % H1;
+      src[g] = (i == 0 || g >= ng) ? res : f + (long long)slot * niv;
     }
-    double s = block_sum(acc, red);
-    if (threadIdx.x == 0) part[1 + i] = s;
+    double acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = 0;
+    for (int v = 0; v < d.n; ++v) {
+      const long long off = (long long)v * d.Ns;
+      double sv[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) sv[g] = 0;
+      const V *a = reinterpret_cast<const V *>(res + off);
+      for (long long q = (long long)cta * blockDim.x + threadIdx.x; q < nv; q += stride) {
+        const V x = a[q];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          if (g < ng) {
+            const V y = reinterpret_cast<const V *>(src[g] + off)[q];
+            if constexpr (VEC == 4) {
+              sv[g] += (double)x.x * (double)y.x + (double)x.y * (double)y.y +
+                       (double)x.z * (double)y.z + (double)x.w * (double)y.w;
+            } else {
+              sv[g] += (double)x.x * (double)y.x + (double)x.y * (double)y.y;
+            }
+          }
+        }
+      }
+      for (long long e = nv * VEC + (long long)cta * blockDim.x + threadIdx.x; e < d.N; e += stride)
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+          if (g < ng) sv[g] += (double)res[off + e] * (double)src[g][off + e];
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc[g] += sv[g] * d.irho[v];
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      if (g < ng) {
+        const double s = block_sum(acc[g], red);
+        if (threadIdx.x == 0) part[1 + i0 + g] = s;
+      }
+    }
   }
 }
 

@@ -38,6 +38,9 @@ sys.path.insert(0, PKG)
 METRIC = "ms/iter & solves/s at RMS<1e-6, mixed vs FP64, 1 B200; served p50/p99 latency"
 WORKLOAD = ("256^3 grid, 128 A cell, 2000-atom seeded globule, 0.2 M NaCl water "
             "(4 sites), KH, AN2 (2 0.6 0.2), RMS 1e-6")
+WORKLOAD_C3 = ("LARGE SINGLE SOLVE (not the headline): 512^3 grid, 256 A cell, 12,877-atom "
+               "seeded globule, 0.2 M NaCl water (4 sites), KH, history-10 Anderson (damping "
+               "0.3), RMS 1e-6")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -185,8 +188,18 @@ def run_gpu(args, rank, world, local):
 
     prec = args.precision
     tmp = tempfile.mkdtemp(prefix=f"r3dbench{rank}_")
-    custom = args.grid != 256 or args.atoms != 2000
-    inp, xvk = make_deck(tmp, atoms=args.atoms if custom else None, grid=args.grid)
+    c3 = args.config == "c3"
+    custom = (args.grid != 256 or args.atoms != 2000) and not c3
+    if c3:  # the large single solve: 512^3, 12,877 atoms, history-10 Anderson
+        import synthetic
+        _solvents(tmp)
+        inp, xvk = synthetic.config("c3", tmp), os.path.join(tmp, "naclaq_vv.xvk")
+    else:
+        inp, xvk = make_deck(tmp, atoms=args.atoms if custom else None, grid=args.grid)
+
+    def configure(s):  # the workload's mixer
+        if c3:
+            s.set_mixer(R.MIX_ANM, 10, 0.3)
 
     # ---- end to end: complete solves through the C-ABI ------------------
     # Each solve creates a context, reads the deck and the .xvk from the
@@ -201,6 +214,7 @@ def run_gpu(args, rank, world, local):
         ph["create_s"] = time.perf_counter() - t0
         t1 = time.perf_counter()
         s.load(inp, xvk=xvk)
+        configure(s)
         ph["load_s"] = time.perf_counter() - t1
         t1 = time.perf_counter()
         s.initialize()
@@ -236,6 +250,7 @@ def run_gpu(args, rank, world, local):
     # ---- device-resident iteration throughput --------------------------
     s = R.RISM3D(device=local, precision=prec)
     s.load(inp, xvk=xvk)
+    configure(s)
     s.set_control(convergence=1e-300, maxstep=10 ** 8)
     s.initialize()
     s.step(args.warmup)
@@ -256,6 +271,7 @@ def run_gpu(args, rank, world, local):
     if prec == "mixed" and not args.no_fp64:
         s64 = R.RISM3D(device=local, precision="fp64")
         s64.load(inp, xvk=xvk)
+        configure(s64)
         s64.set_control(convergence=1e-300, maxstep=10 ** 8)
         s64.initialize()
         s64.step(args.warmup)
@@ -272,14 +288,14 @@ def run_gpu(args, rank, world, local):
     iter_bytes = sum(b for _, _, b in prof)
 
     batch = serve = None
-    if rank == 0 and world == 1 and not custom:
+    if rank == 0 and world == 1 and not custom and not c3:
         if not args.no_batch:
             batch = run_batch_screen(local)
         if not args.no_serve:
             serve = run_served(local)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and not custom:
+    if rank == 0 and world == 1 and not args.no_cpu and not custom and not c3:
         rate, cores, sample = cpu_oracle_rate(CPU_SAMPLE_ITERS, 1)
         cpu = {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port", "sample": sample}
 
@@ -289,12 +305,13 @@ def run_gpu(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_iter,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 grids+transforms, f64 state/reductions" if prec == "mixed" else "f64",
-            "data": "synthetic (seeded 2000-atom globule; shipped 0.2 M NaCl .xvk)",
-            "config": {"workload": WORKLOAD if not custom else
+            "data": "synthetic (seeded %s-atom globule; shipped 0.2 M NaCl .xvk)"
+                    % ("12,877" if c3 else "2000"),
+            "config": {"workload": WORKLOAD_C3 if c3 else WORKLOAD if not custom else
                        f"PROFILING CASE (not the headline): {args.grid}^3 grid, "
                        f"{args.atoms} atoms, NaCl water, KH, AN2",
-                       "precision": prec, "grid": args.grid, "sites": 4,
-                       "atoms": args.atoms, "replicas": world,
+                       "precision": prec, "grid": 512 if c3 else args.grid, "sites": 4,
+                       "atoms": 12877 if c3 else args.atoms, "replicas": world,
                        "l2": "inputs larger than L2 (>8 GB touched per iteration)"},
             "ms_per_iter": ms_iter,
             "iters_to_converge": steps, "solve_status": status, "final_rms": rms,
@@ -554,6 +571,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--config", choices=["c2", "c3"], default="c2",
+                    help="c3: the 512^3 single solve instead of the headline workload")
     ap.add_argument("--grid", type=int, default=256, help="profiling only: grid size")
     ap.add_argument("--atoms", type=int, default=2000, help="profiling only: solute atoms")
     ap.add_argument("--e2e-reps", type=int, default=3, help="warm end-to-end solves timed")

@@ -1270,6 +1270,11 @@ int orc_iterate(orc_solver *s, int maxstep_override, int *steps, double *rms,
   int maxstep = maxstep_override > 0 ? maxstep_override : s->maxstep;
   int conver = 0, diverge = 0, istep;
   double r = 0.0;
+  /* fresh mixer state, as AN2::initialize inside iterate (iterate.cu:39) */
+  s->binary = 0;
+  s->count_left = s->count;
+  s->hcount = 0;
+  s->hhead = 0;
   for (istep = 1; istep <= maxstep; ++istep) {
     r = orc_calculate(s);
     diverge = !isfinite(r);

@@ -99,16 +99,21 @@ def test_oracle_fft_is_the_shifted_transform(shape):
 
 def test_oracle_reproduces_extension_fixture(refcase, tmp_path):
     """The oracle's sums are order-fixed (thread-count independent), so it
-    reproduces its own PSE-3 / history-10 fixture exactly."""
+    reproduces its own PSE-3 / history-10 fixture (reached through KH and
+    PSE-2) exactly."""
     gold = os.path.join(os.path.dirname(__file__), "golden", "oracle")
-    meta = json.load(open(os.path.join(gold, "s_rect_pse3_anm10.json")))
+    meta = json.load(open(os.path.join(gold, "s_rect_pse3_ladder.json")))
     inp, xvk = refcase(meta["deck"])
     o = O.Oracle(inp, xvk=xvk)
-    o.set_closure(meta["closure"], meta["pse_n"])
+    o.set_closure(*meta["ladder"][0])
     o.set_mixer(meta["mixer"], meta["history"], meta["damping"])
     o.initialize()
-    steps, rms, status = o.iterate()
-    assert (steps, status) == (meta["steps"], meta["status"])
+    total = 0
+    for st in meta["ladder"]:
+        o.set_closure(*st)
+        steps, rms, status = o.iterate()
+        total += steps
+    assert (steps, total, status) == (meta["steps"], meta["steps_total"], meta["status"])
     out = tmp_path / "o.xmu"
     o.write_xmu(str(out))
-    assert out.read_text() == open(os.path.join(gold, "s_rect_pse3_anm10.xmu")).read()
+    assert out.read_text() == open(os.path.join(gold, "s_rect_pse3_ladder.xmu")).read()
