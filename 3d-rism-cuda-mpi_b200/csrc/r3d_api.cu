@@ -142,7 +142,9 @@ inline int bulk_per_sm(int device, bool fp64, int which, int L, int PC, size_t s
       nb = fp64 ? ct_occupancy_xw<P64>(which - 2, L, PC, smem)
                 : ct_occupancy_xw<PMix>(which - 2, L, PC, smem);
   }
-  if (nb <= 0) nb = std::max(1, (int)((228 * 1024) / (smem + 2048)));
+  // 0 on a device: no kernel for (L, PC), or it does not fit -- the variant
+  // is not offered; host-only planning estimates from shared memory
+  if (device < 0) nb = std::max(1, (int)((228 * 1024) / (smem + 2048)));
   return nb;
 }
 
@@ -557,11 +559,13 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
     if (rowsN % pcb == 0 && sm <= kSmemMax) {
       const int tiles = d.n * (rowsN / pcb);
       const int per_sm = bulk_per_sm(c->opts.device, fp64, 0, d.hx, pcb, sm);
-      g.fxb_pc = pcb;
-      g.smfxb = sm;
-      g.fxb_ctas = std::min(tiles, kNumSM * per_sm);
-      g.fxb_per = (tiles + g.fxb_ctas - 1) / g.fxb_ctas;
-      g.fxb_ctas = (tiles + g.fxb_per - 1) / g.fxb_per;
+      if (per_sm > 0) {
+        g.fxb_pc = pcb;
+        g.smfxb = sm;
+        g.fxb_ctas = std::min(tiles, kNumSM * per_sm);
+        g.fxb_per = (tiles + g.fxb_ctas - 1) / g.fxb_ctas;
+        g.fxb_ctas = (tiles + g.fxb_per - 1) / g.fxb_per;
+      }
     }
   }
   g.fxw_pc = g.ixw_pc = 0;
@@ -574,6 +578,8 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
       g.fxw_pc = g.ixw_pc = pcw;
       g.fxw_ctas = std::min(ctas, kNumSM * bulk_per_sm(c->opts.device, fp64, 2, d.hx, pcw, sm));
       g.ixw_ctas = std::min(ctas, kNumSM * bulk_per_sm(c->opts.device, fp64, 3, d.hx, pcw, sm));
+      if (!g.fxw_ctas) g.fxw_pc = 0;
+      if (!g.ixw_ctas) g.ixw_pc = 0;
     }
   }
   g.yz_tma = 0;
@@ -601,6 +607,7 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
       kernels_set_smem(fp64, kSmemMax);
       int oy = fp64 ? tma_occupancy<P64>(0, d.ny, g.smfyt) : tma_occupancy<PMix>(0, d.ny, g.smfyt);
       int oz = fp64 ? tma_occupancy<P64>(1, d.nz, g.smzt) : tma_occupancy<PMix>(1, d.nz, g.smzt);
+      if (oy <= 0 || oz <= 0) g.yz_tma = 0;  // no kernels for these lengths
       oy = std::max(oy, 1);
       oz = std::max(oz, 1);
       g.fyt_ctas = std::min(ty, kNumSM * oy);
@@ -624,12 +631,15 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
 
 // Geometry of the bulk-staged IX with pcb rows per tile (false: does not fit).
 static bool ixb_config(int device, const Desc &d, bool fp64, int pcb, Geo &g) {
+  // rows per tile with compiled kernels: 8 or 4 (FP32 grids), 4 or 2 (FP64)
+  if (pcb != (fp64 ? 4 : 8) && pcb != (fp64 ? 2 : 4)) return false;
   const size_t cs = fp64 ? 16 : 8;
   const int rowsN = d.ny * d.nz;
   const size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
   if (rowsN % pcb || sm > kSmemMax) return false;
   const int tiles = d.n * (rowsN / pcb);
   const int per_sm = bulk_per_sm(device, fp64, 1, d.hx, pcb, sm);
+  if (per_sm <= 0) return false;
   g.ixb_pc = pcb;
   g.smixb = sm;
   g.ixb_ctas = std::min(tiles, kNumSM * per_sm);
