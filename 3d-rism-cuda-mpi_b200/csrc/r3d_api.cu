@@ -545,7 +545,7 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
     if (!ixb_config(c->opts.device, d, fp64, pcb, g) && d.hx >= 256)
       ixb_config(c->opts.device, d, fp64, pcb / 2, g);  // long rows: half the rows per tile
     Geo h = g;  // the half-size tiles the autotuner may choose write as many partials rows
-    g.ixh_ctas = (g.ixb_pc >= 4 && ixb_config(c->opts.device, d, fp64, g.ixb_pc / 2, h))
+    g.ixh_ctas = (g.ixb_pc >= 2 && ixb_config(c->opts.device, d, fp64, g.ixb_pc / 2, h))
                      ? h.ixb_ctas : 0;
   }
   g.fxb_pc = 0;
@@ -631,8 +631,10 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
 
 // Geometry of the bulk-staged IX with pcb rows per tile (false: does not fit).
 static bool ixb_config(int device, const Desc &d, bool fp64, int pcb, Geo &g) {
-  // rows per tile with compiled kernels: 8 or 4 (FP32 grids), 4 or 2 (FP64)
-  if (pcb != (fp64 ? 4 : 8) && pcb != (fp64 ? 2 : 4)) return false;
+  // rows per tile with compiled kernels: 8 or 4 (FP32 grids; 2 as well for
+  // rows of 256 or more), 4 or 2 (FP64)
+  if (pcb != (fp64 ? 4 : 8) && pcb != (fp64 ? 2 : 4) && !(!fp64 && pcb == 2 && d.hx >= 256))
+    return false;
   const size_t cs = fp64 ? 16 : 8;
   const int rowsN = d.ny * d.nz;
   const size_t sm = ct_smem_ixb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
@@ -1013,7 +1015,7 @@ static int autotune_x(r3d_ctx *c) {
     int *pf = nullptr;
     // the bulk IX with half the rows per tile (more CTAs per SM)
     Geo half = g;
-    const bool has_half = g.ixb_pc >= 4 &&
+    const bool has_half = g.ixb_pc >= 2 &&
                           ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, half) &&
                           half.ixb_ctas <= c->npart;
     CK(cudaMalloc((void **)&pf, 22 * sizeof(int)));
@@ -1085,7 +1087,7 @@ static int autotune_x(r3d_ctx *c) {
   if (use[0] != 1) g.fxb_pc = 0;
   if (use[0] != 2) g.fxw_pc = 0;
   if (use[1] == 3) {
-    if (!(g.ixb_pc >= 4 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, g))) g.ixb_pc = 0;
+    if (!(g.ixb_pc >= 2 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, g))) g.ixb_pc = 0;
   } else if (use[1] != 1) {
     g.ixb_pc = 0;
   }

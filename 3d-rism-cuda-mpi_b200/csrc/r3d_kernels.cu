@@ -752,7 +752,18 @@ __global__ void __launch_bounds__(kThreads)
       acc[k] = w0 * zk[k];
     }
   }
-  for (int j = 0; j < m; ++j) {
+  int j = 0;
+  for (; j + 1 < m; j += 2) {  // two history slots per step: twice the loads in flight
+    const T *__restrict__ za = zr + (long long)c->mix_slots[j] * niv;
+    const T *__restrict__ zb = zr + (long long)c->mix_slots[j + 1] * niv;
+    const double ca = c->coef[1 + j], cb = c->coef[2 + j];
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) acc[k] += ca * (double)za[i] + cb * (double)zb[i];
+    }
+  }
+  if (j < m) {
     const T *__restrict__ zj = zr + (long long)c->mix_slots[j] * niv;
     const double cj = c->coef[1 + j];
 #pragma unroll

@@ -995,6 +995,17 @@ bool ct_launch_ixb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s
   }
   R3D_CT_LENGTHS(R3D_IXB_HALF)
 #undef R3D_IXB_HALF
+  // two rows per tile for the longest FP32 rows (the occupancy variant there)
+  if constexpr (sizeof(typename P::R) == 4) {
+    if (L == 256 && PC == 2) {
+      k_ix_bulk<P, 256, 2><<<grid, kThreads, smem, s>>>(b, per);
+      return true;
+    }
+    if (L == 512 && PC == 2) {
+      k_ix_bulk<P, 512, 2><<<grid, kThreads, smem, s>>>(b, per);
+      return true;
+    }
+  }
   return false;
 }
 
@@ -1049,6 +1060,15 @@ int ct_occupancy_bulk(int which, int L, int PC, size_t smem) {
   }
   R3D_CT_LENGTHS(R3D_OCC_IXH)
 #undef R3D_OCC_IXH
+  if constexpr (sizeof(typename P::R) == 4) {
+    if (which == 1 && PC == 2 && (L == 256 || L == 512)) {
+      if (L == 256)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ix_bulk<P, 256, 2>, kThreads, smem);
+      else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_ix_bulk<P, 512, 2>, kThreads, smem);
+      return nb;
+    }
+  }
 #undef R3D_OCC
   return 0;
 }
@@ -1117,6 +1137,10 @@ void ct_allow_smem_all() {
 #undef R3D_ATTR
   allow_smem(k_fx_bulk<P, 256, (sizeof(typename P::R) == 4 ? 4 : 2)>);
   allow_smem(k_fx_bulk<P, 512, (sizeof(typename P::R) == 4 ? 4 : 2)>);
+  if constexpr (sizeof(typename P::R) == 4) {
+    allow_smem(k_ix_bulk<P, 256, 2>);
+    allow_smem(k_ix_bulk<P, 512, 2>);
+  }
   allow_smem(k_fx_warp<P, 256, 2>);
   allow_smem(k_fx_warp<P, 512, 2>);
   allow_smem(k_ix_warp<P, 256, 2>);
