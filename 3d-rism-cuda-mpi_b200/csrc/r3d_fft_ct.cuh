@@ -84,6 +84,7 @@ __device__ __forceinline__ void ct_dit_stage(C *buf, const C *tw, int tid) {
   constexpr int TR = NT / PC;     // row groups
   constexpr int TWS = L / (R * M);
   const int p = tid % PC, g = tid / PC;
+  if (g >= TR) return;  // NT not a multiple of PC: the remainder idles
 #pragma unroll
   for (int b0 = 0; b0 < NB; b0 += TR) {
     const int b = b0 + g;
@@ -114,6 +115,7 @@ __device__ __forceinline__ void ct_dif_stage(C *buf, const C *tw, int tid) {
   constexpr int TR = NT / PC;
   constexpr int TWS = L / (R * M);
   const int p = tid % PC, g = tid / PC;
+  if (g >= TR) return;  // NT not a multiple of PC: the remainder idles
 #pragma unroll
   for (int b0 = 0; b0 < NB; b0 += TR) {
     const int b = b0 + g;

@@ -134,7 +134,9 @@ __global__ void __launch_bounds__(kThreads)
 // ------------------------------------------------------------------ ZOZ
 // tile = PC x-columns at one y, all n sites; smem [site][L = nz][PC].
 // Forward z, (mqvfk when d.fk is set), Ornstein-Zernike, inverse z.
-template <typename P, int L, int PC, int NS>
+// ZMAJOR: the tile is [z][site][p] (all sites' columns side by side, one
+// transform over NS * PC columns); else [site][z][p]
+template <typename P, int L, int PC, int NS, bool ZMAJOR = false>
 __device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const Desc &d,
                                       int y, int pt) {
   using R = typename P::R;
@@ -185,7 +187,7 @@ __device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const 
     C c[M];
 #pragma unroll
     for (int q = 0; q < M; ++q)
-      if (q < n) c[q] = buf[(q * L + z) * PC + p];
+      if (q < n) c[q] = buf[ZMAJOR ? (z * NS + q) * PC + p : (q * L + z) * PC + p];
     if (fk) {  // mqvfk (refresh pipeline only)
       const double2 f = fk[gi];
 #pragma unroll
@@ -207,16 +209,43 @@ __device__ __forceinline__ void ct_oz(typename Cx<typename P::R>::T *buf, const 
             hi += c[q].y * xq;
           }
         }
-        buf[(a * L + z) * PC + p] = C{hr, hi};
+        buf[ZMAJOR ? (z * NS + a) * PC + p : (a * L + z) * PC + p] = C{hr, hi};
       }
     }
+  }
+}
+
+// z transform, OZ and inverse z transform of one tile with the NS sites'
+// columns side by side: smem [z][site][p], rows digit-reversed for the DIT
+template <typename P, int L, int PC, int NS>
+__device__ __forceinline__ void zoz_sites(typename Cx<typename P::R>::T *buf, const Desc &d,
+                                          typename Cx<typename P::R>::T *w, long long zs,
+                                          const typename Cx<typename P::R>::T *pw,
+                                          const typename Cx<typename P::R>::T *tw, int ky,
+                                          int pt) {
+  using C = typename Cx<typename P::R>::T;
+  constexpr int W = NS * PC;  // columns of the transform
+#pragma unroll 4
+  for (int e = threadIdx.x; e < W * L; e += kThreads) {
+    const int p = e % PC, v = (e / PC) % NS, z = e / W;
+    buf[(digit_rev<L>(z) * NS + v) * PC + p] = cmul(w[v * d.Nhs + z * zs + p], pw[z]);
+  }
+  __syncthreads();
+  ct_fft_dit<L, W, W, -1>(buf, tw);
+  ct_oz<P, L, PC, NS, true>(buf, d, ky, pt);
+  __syncthreads();
+  ct_fft_dif<L, W, W, 1>(buf, tw);
+#pragma unroll 4
+  for (int e = threadIdx.x; e < W * L; e += kThreads) {
+    const int p = e % PC, v = (e / PC) % NS, z = e / W;
+    w[v * d.Nhs + z * zs + p] = cmul(buf[(digit_rev<L>(z) * NS + v) * PC + p], cconj(pw[z]));
   }
 }
 
 // check: bit 0 = skip solves not running; bit 1 = w's y rows are in the
 // digit-reversed ky order of the copy-engine y pass (ky from d.yrev)
 template <typename P, int L, int PC>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
     k_zoz_ct(Batch b, int check) {
   using R = typename P::R;
   using C = typename Cx<R>::T;
@@ -232,6 +261,15 @@ __global__ void __launch_bounds__(kThreads)
   const long long zs = (long long)d.ny * hx;
   const C *pw = (const C *)d.pwz, *tw = (const C *)d.twz;
   C *w = (C *)d.w + (long long)y * hx + pt * PC;
+  // up to four sites: one transform over all sites' columns ([z][site][p]),
+  // a quarter of the barriers of one transform per site
+  switch (n) {
+    case 1: zoz_sites<P, L, PC, 1>(buf, d, w, zs, pw, tw, ky, pt); return;
+    case 2: zoz_sites<P, L, PC, 2>(buf, d, w, zs, pw, tw, ky, pt); return;
+    case 3: zoz_sites<P, L, PC, 3>(buf, d, w, zs, pw, tw, ky, pt); return;
+    case 4: zoz_sites<P, L, PC, 4>(buf, d, w, zs, pw, tw, ky, pt); return;
+    default: break;
+  }
   for (int v = 0; v < n; ++v) {
     const C *wv = w + (long long)v * d.Nhs;
     C *bv = buf + v * L * PC;
