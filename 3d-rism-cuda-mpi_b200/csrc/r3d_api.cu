@@ -1603,6 +1603,8 @@ extern "C" int r3d_transfer_bytes(const r3d_ctx *c, unsigned long long *h2d,
   return R3D_OK;
 }
 
+extern "C" int r3d_write_tuv(r3d_ctx *c, const char *path);
+
 extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
   if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
   if (!c->initialized) return fail(c, R3D_ESTATE, "iterate before initialize");
@@ -1626,13 +1628,18 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
   CK(cudaEventRecord(e0, s));
   Ctl h{};
   int printed = 0;
-  const int chunk = 8;
   std::vector<double> log;
   c->next_refresh = 1e-3;
+  const int ksave = c->prob.ksave;  // iterate.cu:63-70: save t every ksave steps / at the end
   for (;;) {
+    // chunks end on the multiples of ksave, where t is saved
+    const int chunk = ksave > 0 ? std::min(8, ksave - h.step % ksave) : 8;
     for (int i = 0; i < chunk; ++i) CK(cudaGraphLaunch(c->gexec, s));
     int rc = read_ctl(c, h);
     if (rc) return rc;
+    if (ksave > 0 && h.status == RUNNING && h.step % ksave == 0 &&
+        (rc = r3d_write_tuv(c, nullptr)))
+      return rc;
     if (!c->fp64 && h.status == RUNNING && h.rms < c->next_refresh) {
       // mixed path: move the converged part of c into the FP64 reference
       if ((rc = refresh<PMix>(c, false))) return rc;
@@ -1657,6 +1664,10 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
   c->ms_per_iter = h.step > 0 ? ms / h.step : 0;
   int st = h.status == CONVERGED ? R3D_CONVERGED
                                  : (h.status == DIVERGED ? R3D_DIVERGED : R3D_MAXSTEP);
+  if (ksave != 0 && st == R3D_CONVERGED) {
+    int rc = r3d_write_tuv(c, nullptr);
+    if (rc) return rc;
+  }
   if (c->opts.verbose) {
     if (st == R3D_DIVERGED)
       std::printf("Calculation diverged.\n");
@@ -1849,6 +1860,78 @@ extern "C" int r3d_set_t(r3d_ctx *c, const double *host) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
   return R3D_OK;
+}
+
+// ------------------------------------------------------------ grid files
+static int grid_host(r3d_ctx *c, int which, std::vector<double> &v) {
+  v.resize((size_t)c->desc.n * c->desc.N);
+  return r3d_get_grid(c, which, v.data());
+}
+static std::string out_path(const r3d_ctx *c, const char *path, const char *ext) {
+  return path ? std::string(path) : c->prob.fname + ext;
+}
+
+extern "C" int r3d_write_guv(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> g;
+  int rc = grid_host(c, R3D_GRID_G, g);
+  if (rc) return rc;
+  std::string m = write_guv(c->prob, g.data(), out_path(c, path, ".guv"));
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
+extern "C" int r3d_write_huv(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> h;
+  int rc = grid_host(c, R3D_GRID_H, h);
+  if (rc) return rc;
+  std::string m = write_grid_text(c->prob, h.data(), out_path(c, path, ".huv0"));
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
+extern "C" int r3d_write_cuv(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> h, t;
+  int rc = grid_host(c, R3D_GRID_H, h);
+  if (!rc) rc = grid_host(c, R3D_GRID_T, t);
+  if (rc) return rc;
+  for (size_t i = 0; i < h.size(); ++i) h[i] -= t[i];  // c = h - t
+  std::string m = write_grid_text(c->prob, h.data(), out_path(c, path, ".cuv0"));
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
+extern "C" int r3d_write_tuv(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> t;
+  int rc = grid_host(c, R3D_GRID_T, t);
+  if (rc) return rc;
+  std::string m = write_tuv(c->prob, t.data(), out_path(c, path, ".tuv"));
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
+extern "C" int r3d_read_tuv(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "read_tuv before initialize");
+  std::vector<double> t((size_t)c->desc.n * c->desc.N);
+  std::string m = read_tuv(c->prob, t.data(), out_path(c, path, ".tuv"));
+  if (!m.empty()) return fail(c, R3D_EIO, m);
+  return r3d_set_t(c, t.data());
+}
+
+extern "C" int r3d_output(r3d_ctx *c, const char *outlist) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::string ol = outlist ? outlist : c->prob.outlist;
+  std::transform(ol.begin(), ol.end(), ol.begin(), ::tolower);
+  for (char ch : ol)
+    if (ch == 'd' || ch == 'a' || ch == 'b')
+      return fail(c, R3D_EINVAL, std::string("output '") + ch +
+                                     "' (forces, lambda derivatives, energies) is not built");
+  int rc = R3D_OK;
+  if (ol.find('m') != std::string::npos) rc = r3d_write_xmu(c, nullptr);
+  if (!rc && ol.find('c') != std::string::npos) rc = r3d_write_cuv(c, nullptr);
+  if (!rc && ol.find('g') != std::string::npos) rc = r3d_write_guv(c, nullptr);
+  if (!rc && ol.find('h') != std::string::npos) rc = r3d_write_huv(c, nullptr);
+  return rc;
 }
 
 extern "C" int r3d_info(const r3d_ctx *c, int *grid3, int *natv, long long *ngrid, int *nu) {

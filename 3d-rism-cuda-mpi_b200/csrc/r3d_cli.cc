@@ -9,10 +9,22 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <cctype>
 #include <cstring>
 #include <string>
 
 #include "../../include/rism3d_b200.h"
+
+// first token of the deck: RISM3D's outlist (read_input.cu:32)
+static std::string outlist_of(const std::string &inp) {
+  std::string ol = "m";
+  if (FILE *f = std::fopen(inp.c_str(), "r")) {
+    char buf[256];
+    if (std::fscanf(f, "%255s", buf) == 1) ol = buf;
+    std::fclose(f);
+  }
+  return ol;
+}
 
 static int die(r3d_ctx *c, const char *what) {
   std::fprintf(stderr, "%s: %s\n", what, r3d_last_error(c));
@@ -67,13 +79,32 @@ int main(int argc, char **argv) {
   }
   if (history > 0 && r3d_set_mixer(c, R3D_MIX_ANM, history, damping)) return die(c, "mixer");
   if (r3d_initialize(c)) return die(c, "initialize");
+  // iterate.cu:26-35: a saved <stem>.tuv is the starting t
+  const std::string stem = input.substr(0, input.rfind('.'));
+  if (FILE *tf = std::fopen((stem + ".tuv").c_str(), "r")) {
+    std::fclose(tf);
+    std::printf("restarting from %s.tuv\n", stem.c_str());
+    if (r3d_read_tuv(c, (stem + ".tuv").c_str())) return die(c, "read_tuv");
+  }
   int steps = 0, status = 0;
   double rms = 0;
   if (r3d_iterate(c, &steps, &rms, &status)) return die(c, "iterate");
   double ms = 0;
   r3d_iter_timing(c, &ms, nullptr);
   std::printf("Iteration   :\t%lf sec. (%d steps, %.3f ms/step)\n", ms * steps * 1e-3, steps, ms);
-  if (r3d_write_xmu(c, nullptr)) return die(c, "output");
+  if (status != R3D_DIVERGED) {
+    // output.cu: the deck's outlist, without the outputs not built here
+    std::string ol = outlist_of(input);
+    std::string keep;
+    for (char ch : ol) {
+      const char lc = (char)std::tolower((unsigned char)ch);
+      if (lc == 'd' || lc == 'a' || lc == 'b')
+        std::fprintf(stderr, "output '%c' (forces, lambda derivatives, energies) is not built\n", ch);
+      else
+        keep += lc;
+    }
+    if (r3d_output(c, keep.c_str())) return die(c, "output");
+  }
   r3d_destroy(c);
   return status == R3D_DIVERGED ? 3 : 0;
 }

@@ -396,6 +396,71 @@ std::string build_shells(const Problem &p, ShellTable &st) {
 }
 
 // --------------------------------------------------------------- .xmu
+// .guv (output_guv.cu:19-49): int natv, int grid[3], double box[3],
+// double shift[3], then g of every site as z-planes of x-fastest rows.
+std::string write_guv(const Problem &p, const double *g, const std::string &path) {
+  FILE *f = std::fopen(path.c_str(), "wb");
+  if (!f) return "cannot write " + path;
+  const int hdr[4] = {p.natv, p.grid[0], p.grid[1], p.grid[2]};
+  const size_t n = (size_t)p.natv * p.grid[0] * p.grid[1] * p.grid[2];
+  bool ok = std::fwrite(hdr, sizeof(int), 4, f) == 4 &&
+            std::fwrite(p.box, sizeof(double), 3, f) == 3 &&
+            std::fwrite(p.shift, sizeof(double), 3, f) == 3 &&
+            std::fwrite(g, sizeof(double), n, f) == n;
+  ok = std::fclose(f) == 0 && ok;
+  return ok ? "" : "short write to " + path;
+}
+
+// .huv / .cuv text (output_huv.cu, output_cuv.cu at one rank): box, grid,
+// the solute (q sig eps x y z per atom), natv, then one line per grid point
+// with the value of every site; iostream's default formatting.
+std::string write_grid_text(const Problem &p, const double *v, const std::string &path) {
+  std::ofstream out(path);
+  if (!out) return "cannot write " + path;
+  out << p.box[0] << " " << p.box[1] << " " << p.box[2] << " " << std::endl
+      << p.grid[0] << " " << p.grid[1] << " " << p.grid[2] << " " << std::endl
+      << p.q.size() << std::endl;
+  for (size_t iu = 0; iu < p.q.size(); ++iu)
+    out << p.q[iu] << " " << p.sig[iu] << " " << p.eps[iu] << " " << p.r[3 * iu] << " "
+        << p.r[3 * iu + 1] << " " << p.r[3 * iu + 2] << std::endl;
+  out << p.natv << std::endl;
+  const size_t N = (size_t)p.grid[0] * p.grid[1] * p.grid[2];
+  for (size_t ig = 0; ig < N; ++ig) {
+    for (int iv = 0; iv < p.natv; ++iv) out << v[(size_t)iv * N + ig] << " ";
+    out << "\n";
+  }
+  out.flush();
+  return out ? "" : "short write to " + path;
+}
+
+// .tuv (write_tuv.cu): "nx ny nz natv", then t of every site, one value per
+// line, iostream's default formatting.
+std::string write_tuv(const Problem &p, const double *t, const std::string &path) {
+  std::ofstream out(path);
+  if (!out) return "cannot write " + path;
+  out << p.grid[0] << " " << p.grid[1] << " " << p.grid[2] << " " << p.natv << std::endl;
+  const size_t n = (size_t)p.natv * p.grid[0] * p.grid[1] * p.grid[2];
+  for (size_t i = 0; i < n; ++i) out << t[i] << "\n";
+  out.flush();
+  return out ? "" : "short write to " + path;
+}
+
+// read_tuv.cu: the grid and site count must match the problem (the
+// reference only prints the mismatch; here it is an error).
+std::string read_tuv(const Problem &p, double *t, const std::string &path) {
+  std::ifstream in(path);
+  if (!in) return "cannot read " + path;
+  int g0 = 0, g1 = 0, g2 = 0, nv = 0;
+  if (!(in >> g0 >> g1 >> g2 >> nv)) return path + ": bad header";
+  if (g0 != p.grid[0] || g1 != p.grid[1] || g2 != p.grid[2] || nv != p.natv)
+    return path + ": saved grid " + std::to_string(g0) + "x" + std::to_string(g1) + "x" +
+           std::to_string(g2) + " with " + std::to_string(nv) + " sites does not match";
+  const size_t n = (size_t)p.natv * p.grid[0] * p.grid[1] * p.grid[2];
+  for (size_t i = 0; i < n; ++i)
+    if (!(in >> t[i])) return path + ": truncated";
+  return "";
+}
+
 std::string write_xmu(const Problem &p, const double *xmu, const double *xmu2,
                       double pmv, double pressure, const std::string &path) {
   FILE *f = std::fopen(path.c_str(), "w");

@@ -51,6 +51,12 @@ struct Problem {
 std::string parse_inp(Problem &p, const std::string &inp,
                       const std::string &structure, bool centering, bool q0);
 std::string parse_xvk(Problem &p, const std::string &path);
+// Grid files (output_guv.cu:19-49, output_huv.cu, output_cuv.cu,
+// write_tuv.cu, read_tuv.cu): grids [site][z][y][x], N = nx ny nz per site.
+std::string write_guv(const Problem &p, const double *g, const std::string &path);
+std::string write_grid_text(const Problem &p, const double *v, const std::string &path);
+std::string write_tuv(const Problem &p, const double *t, const std::string &path);
+std::string read_tuv(const Problem &p, double *t, const std::string &path);
 std::string write_xmu(const Problem &p, const double *xmu, const double *xmu2,
                       double pmv, double pressure, const std::string &path);
 

@@ -35,7 +35,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_fft3d_noalloc", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
            "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
-           "r3d_server_destroy"]
+           "r3d_server_destroy", "r3d_write_guv", "r3d_write_huv", "r3d_write_cuv",
+           "r3d_write_tuv", "r3d_read_tuv", "r3d_output"]
 REQ_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed"}
 
 
@@ -105,6 +106,12 @@ def _load():
         "r3d_server_write_xmu": [vp, ctypes.c_longlong, cs],
         "r3d_server_release": [vp, ctypes.c_longlong],
         "r3d_server_destroy": [vp],
+        "r3d_write_guv": [vp, cs],
+        "r3d_write_huv": [vp, cs],
+        "r3d_write_cuv": [vp, cs],
+        "r3d_write_tuv": [vp, cs],
+        "r3d_read_tuv": [vp, cs],
+        "r3d_output": [vp, cs],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -176,6 +183,19 @@ class RISM3D:
         self._check(lib.r3d_iterate(self.h, ctypes.byref(st), ctypes.byref(rms),
                                     ctypes.byref(status)))
         return st.value, rms.value, STATUS[status.value]
+
+    def write_grid_file(self, kind, path=None):
+        """kind 'g' (.guv, binary), 'h' (.huv), 'c' (.cuv), 't' (.tuv)."""
+        f = {"g": lib.r3d_write_guv, "h": lib.r3d_write_huv, "c": lib.r3d_write_cuv,
+             "t": lib.r3d_write_tuv}[kind]
+        self._check(f(self.h, path.encode() if path else None))
+
+    def read_tuv(self, path=None):
+        self._check(lib.r3d_read_tuv(self.h, path.encode() if path else None))
+
+    def output_files(self, outlist=None):
+        """RISM3D::output: the files of the outlist letters (m, c, g, h)."""
+        self._check(lib.r3d_output(self.h, outlist.encode() if outlist else None))
 
     def output(self, path=None):
         self._check(lib.r3d_write_xmu(self.h, path.encode() if path else None))

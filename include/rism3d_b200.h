@@ -177,6 +177,30 @@ int r3d_status(r3d_ctx *ctx, int *steps, double *rms, int *status);
 int r3d_transfer_bytes(const r3d_ctx *ctx, unsigned long long *h2d,
                        unsigned long long *d2h);
 
+/* ---- grid files (RISM3D::output's 'g', 'h', 'c' and the .tuv restart) ----
+ * path NULL: the deck's stem (set_fname.cu) with the reference's extension.
+ * r3d_write_guv: output_guv.cu:19-49, binary: int natv, int grid[3],
+ *   double box[3], double shift[3], then g per site as z-planes of x-fastest
+ *   rows (default <stem>.guv).
+ * r3d_write_huv / r3d_write_cuv: output_huv.cu / output_cuv.cu at one rank,
+ *   text: box, grid, solute atoms (q sig eps x y z), natv, then one line per
+ *   grid point with h (or c = h - t) of every site (default <stem>.huv0 /
+ *   <stem>.cuv0, the rank-0 file names).
+ * r3d_write_tuv: write_tuv.cu, text "nx ny nz natv" then t per site, one value
+ *   per line (default <stem>.tuv).  r3d_iterate also writes it every ksave
+ *   steps (ksave > 0) and at convergence (ksave != 0), as iterate.cu:63-70.
+ * r3d_read_tuv: read_tuv.cu, then loads t into the solve (the reference reads
+ *   the file but never copies it to the device); after r3d_initialize.
+ * r3d_output: RISM3D::output (output.cu): the files of the letters of
+ *   outlist (NULL: the deck's) -- m (.xmu), c, g, h; d, a, b (forces,
+ *   lambda derivatives, energies) are not built and give R3D_EINVAL. */
+int r3d_write_guv(r3d_ctx *ctx, const char *path);
+int r3d_write_huv(r3d_ctx *ctx, const char *path);
+int r3d_write_cuv(r3d_ctx *ctx, const char *path);
+int r3d_write_tuv(r3d_ctx *ctx, const char *path);
+int r3d_read_tuv(r3d_ctx *ctx, const char *path);
+int r3d_output(r3d_ctx *ctx, const char *outlist);
+
 /* FFT3D::execute (fft3d.cu:72-78), stand-alone test seam: the reference's
  * half-shifted 3D transform F(k) = dv sum_r f(r) e^{-i k.r} of a real grid.
  * dir -1: in = real [N], out = complex interleaved half spectrum [z][y][p]
