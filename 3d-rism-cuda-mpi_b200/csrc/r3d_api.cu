@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -86,6 +87,8 @@ template <typename P>
 void launch_inv_x(Batch, int, size_t, cudaStream_t, int, void *, int);
 void launch_reduce(const Desc *, const int *, int, int, cudaStream_t);
 void launch_ctl_gather(const Desc *, int, double *, cudaStream_t);
+void launch_atom_integrals(const IntAtoms &, const double *, long long, const int *,
+                           const double *, double *, int, double *, cudaStream_t);
 template <typename P>
 void launch_mix_an2(Batch, int, cudaStream_t);
 template <typename P>
@@ -1918,19 +1921,133 @@ extern "C" int r3d_read_tuv(r3d_ctx *c, const char *path) {
   return r3d_set_t(c, t.data());
 }
 
+// ------------------------------------------------ per-atom integrals
+// cal_grad.cu, cal_euv.cu, cal_ad1.cu / cal_ad2.cu over g of the solve, in
+// the units of their files: grad [nu][3] kcal/(mol A), euv [nu][natv] J/mol,
+// ad [nu] kcal/mol (ad: the LJ lambda derivative after set_ad(lambda, 1),
+// else the Coulomb one).  Any output may be NULL.
+extern "C" int r3d_atom_integrals(r3d_ctx *c, double *grad, double *euv, double *ad) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  if (!c->initialized) return fail(c, R3D_ESTATE, "atom integrals before initialize");
+  CK(cudaSetDevice(c->opts.device));
+  const Problem &p = c->prob;
+  const Desc &d = c->desc;
+  const int nu = (int)p.q.size(), n = p.natv;
+  const long long N = d.N, niv = (long long)n * N;
+  cudaStream_t s = c->stream;
+  Ctl h;
+  int rc = read_ctl(c, h);
+  if (rc) return rc;
+  if ((rc = ensure_scratch(c, niv * 8))) return rc;  // g, FP64
+  const void *tg = t_of_residual(c, h);
+  if (c->fp64)
+    launch_gh<P64>(d, tg, c->scratch, nullptr, s);
+  else
+    launch_gh<PMix>(d, tg, c->scratch, nullptr, s);
+  const double lambda1 = p.adswitch == 1 ? p.lambda : 1.0;
+  std::vector<double> tab((size_t)nu * (4 + 2 * n));
+  for (int a = 0; a < nu; ++a) {
+    tab[a] = p.r[3 * a];
+    tab[nu + a] = p.r[3 * a + 1];
+    tab[2 * nu + a] = p.r[3 * a + 2];
+    tab[3 * nu + a] = p.q[a];
+    for (int v = 0; v < n; ++v) {  // cal_LJ.cu:30-40
+      tab[(size_t)(4 + v) * nu + a] = (p.sig[a] + p.sigv[v]) * 0.5 * lambda1;
+      tab[(size_t)(4 + n + v) * nu + a] = std::sqrt(p.eps[a] * p.epsv[v]);
+    }
+  }
+  const int nchunk = (int)std::max<long long>(1, std::min<long long>(256, N / 4096));
+  const long long nk = (long long)nu * (4 + n);
+  double *buf = nullptr;
+  const size_t bytes = (tab.size() + (size_t)nchunk * nk + nk) * sizeof(double);
+  CK(cudaMalloc((void **)&buf, std::max<size_t>(bytes, 16)));
+  double *dtab = buf, *part = buf + tab.size(), *out = part + (size_t)nchunk * nk;
+  int rcc = R3D_OK;
+  std::vector<double> host(nk);
+  if (nu > 0) {
+    cudaError_t e = cudaMemcpyAsync(dtab, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, s);
+    IntAtoms at{};
+    at.x = dtab;
+    at.y = dtab + nu;
+    at.z = dtab + 2 * nu;
+    at.q = dtab + 3 * nu;
+    at.sig = dtab + 4 * (size_t)nu;
+    at.eps = dtab + (size_t)(4 + n) * nu;
+    for (int v = 0; v < n; ++v) {
+      at.qv[v] = p.qv[v];
+      at.rhov[v] = p.rhov[v];
+    }
+    at.nu = nu;
+    at.n = n;
+    at.ad1 = p.adswitch == 1;
+    at.lambda = p.lambda;
+    at.cc = phys::hartree * phys::bohr * phys::avogadro;
+    const double dr[3] = {p.box[0] / d.nx, p.box[1] / d.ny, p.box[2] / d.nz};
+    if (e == cudaSuccess) {
+      launch_atom_integrals(at, c->scratch, N, p.grid, dr, part, nchunk, out, s);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), out, nk * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) rcc = fail(c, R3D_ECUDA, cudaGetErrorString(e));
+    c->d2h += nk * 8;
+    c->h2d += tab.size() * 8;
+  }
+  cudaFree(buf);
+  if (rcc) return rcc;
+  const double dv = p.box[0] * p.box[1] * p.box[2] / (double)N, kcal2J = 4184.0;
+  for (int a = 0; a < nu; ++a) {
+    const double *o = host.data() + (size_t)a * (4 + n);
+    if (grad)
+      for (int k = 0; k < 3; ++k) grad[3 * a + k] = o[k] * dv / kcal2J;
+    if (ad) ad[a] = o[3] * dv / kcal2J;
+    if (euv)
+      for (int v = 0; v < n; ++v) euv[(size_t)a * n + v] = o[4 + v] * dv;
+  }
+  return R3D_OK;
+}
+
+extern "C" int r3d_write_gra(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> g(3 * c->prob.q.size());
+  int rc = r3d_atom_integrals(c, g.data(), nullptr, nullptr);
+  if (rc) return rc;
+  std::string m = write_atom_file(c->prob, 'd', g.data(), out_path(c, path, ".gra"));
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
+extern "C" int r3d_write_euv(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> e(c->prob.q.size() * c->prob.natv);
+  int rc = r3d_atom_integrals(c, nullptr, e.data(), nullptr);
+  if (rc) return rc;
+  std::string m = write_atom_file(c->prob, 'b', e.data(), out_path(c, path, ".euv"));
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
+extern "C" int r3d_write_ad(r3d_ctx *c, const char *path) {
+  if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
+  std::vector<double> v(c->prob.q.size());
+  int rc = r3d_atom_integrals(c, nullptr, nullptr, v.data());
+  if (rc) return rc;
+  std::ostringstream nm;  // output_ad.cu: <stem>-<adswitch>-<lambda>
+  nm << c->prob.fname << "-" << c->prob.adswitch << "-" << c->prob.lambda;
+  std::string m = write_atom_file(c->prob, 'a', v.data(), path ? std::string(path) : nm.str());
+  return m.empty() ? R3D_OK : fail(c, R3D_EIO, m);
+}
+
 extern "C" int r3d_output(r3d_ctx *c, const char *outlist) {
   if (!c) return fail(c, R3D_EINVAL, "ctx is NULL");
   std::string ol = outlist ? outlist : c->prob.outlist;
   std::transform(ol.begin(), ol.end(), ol.begin(), ::tolower);
-  for (char ch : ol)
-    if (ch == 'd' || ch == 'a' || ch == 'b')
-      return fail(c, R3D_EINVAL, std::string("output '") + ch +
-                                     "' (forces, lambda derivatives, energies) is not built");
-  int rc = R3D_OK;
+  int rc = R3D_OK;  // output.cu's order: m, d, c, g, h, a, b
   if (ol.find('m') != std::string::npos) rc = r3d_write_xmu(c, nullptr);
+  if (!rc && ol.find('d') != std::string::npos) rc = r3d_write_gra(c, nullptr);
   if (!rc && ol.find('c') != std::string::npos) rc = r3d_write_cuv(c, nullptr);
   if (!rc && ol.find('g') != std::string::npos) rc = r3d_write_guv(c, nullptr);
   if (!rc && ol.find('h') != std::string::npos) rc = r3d_write_huv(c, nullptr);
+  if (!rc && ol.find('a') != std::string::npos) rc = r3d_write_ad(c, nullptr);
+  if (!rc && ol.find('b') != std::string::npos) rc = r3d_write_euv(c, nullptr);
   return rc;
 }
 

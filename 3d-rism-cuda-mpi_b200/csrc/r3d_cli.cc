@@ -15,17 +15,6 @@
 
 #include "../../include/rism3d_b200.h"
 
-// first token of the deck: RISM3D's outlist (read_input.cu:32)
-static std::string outlist_of(const std::string &inp) {
-  std::string ol = "m";
-  if (FILE *f = std::fopen(inp.c_str(), "r")) {
-    char buf[256];
-    if (std::fscanf(f, "%255s", buf) == 1) ol = buf;
-    std::fclose(f);
-  }
-  return ol;
-}
-
 static int die(r3d_ctx *c, const char *what) {
   std::fprintf(stderr, "%s: %s\n", what, r3d_last_error(c));
   return 1;
@@ -93,17 +82,8 @@ int main(int argc, char **argv) {
   r3d_iter_timing(c, &ms, nullptr);
   std::printf("Iteration   :\t%lf sec. (%d steps, %.3f ms/step)\n", ms * steps * 1e-3, steps, ms);
   if (status != R3D_DIVERGED) {
-    // output.cu: the deck's outlist, without the outputs not built here
-    std::string ol = outlist_of(input);
-    std::string keep;
-    for (char ch : ol) {
-      const char lc = (char)std::tolower((unsigned char)ch);
-      if (lc == 'd' || lc == 'a' || lc == 'b')
-        std::fprintf(stderr, "output '%c' (forces, lambda derivatives, energies) is not built\n", ch);
-      else
-        keep += lc;
-    }
-    if (r3d_output(c, keep.c_str())) return die(c, "output");
+    // output.cu: the files of the deck's outlist
+    if (r3d_output(c, nullptr)) return die(c, "output");
   }
   r3d_destroy(c);
   return status == R3D_DIVERGED ? 3 : 0;

@@ -461,6 +461,30 @@ std::string read_tuv(const Problem &p, double *t, const std::string &path) {
   return "";
 }
 
+// Per-atom files, iostream formatting: kind 'd' .gra (output_grad.cu: three
+// values per atom), 'b' .euv (output_euv.cu: fixed, the sum over sites then
+// each site), 'a' lambda derivative (output_ad.cu: one value per atom).
+std::string write_atom_file(const Problem &p, char kind, const double *v,
+                            const std::string &path) {
+  std::ofstream out(path);
+  if (!out) return "cannot write " + path;
+  const size_t nu = p.q.size(), n = (size_t)p.natv;
+  for (size_t a = 0; a < nu; ++a) {
+    if (kind == 'd') {
+      out << v[3 * a] << " " << v[3 * a + 1] << " " << v[3 * a + 2] << std::endl;
+    } else if (kind == 'b') {
+      double sum = 0;
+      for (size_t iv = 0; iv < n; ++iv) sum += v[a * n + iv];
+      out << std::fixed << sum;
+      for (size_t iv = 0; iv < n; ++iv) out << " " << std::fixed << v[a * n + iv];
+      out << std::endl;
+    } else {
+      out << v[a] << std::endl;
+    }
+  }
+  return out ? "" : "short write to " + path;
+}
+
 std::string write_xmu(const Problem &p, const double *xmu, const double *xmu2,
                       double pmv, double pressure, const std::string &path) {
   FILE *f = std::fopen(path.c_str(), "w");

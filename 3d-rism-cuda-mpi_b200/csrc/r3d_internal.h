@@ -57,6 +57,7 @@ std::string write_guv(const Problem &p, const double *g, const std::string &path
 std::string write_grid_text(const Problem &p, const double *v, const std::string &path);
 std::string write_tuv(const Problem &p, const double *t, const std::string &path);
 std::string read_tuv(const Problem &p, double *t, const std::string &path);
+std::string write_atom_file(const Problem &p, char kind, const double *v, const std::string &path);
 std::string write_xmu(const Problem &p, const double *xmu, const double *xmu2,
                       double pmv, double pressure, const std::string &path);
 
@@ -166,5 +167,14 @@ struct Desc {
 };
 
 constexpr int kPartials = 1 + 5 * kMaxSites;  // sum R^2 + per-site dots
+
+// Atoms of the post-solve per-atom integrals (k_atom_integrals)
+struct IntAtoms {
+  const double *x, *y, *z, *q;  // [nu], device
+  const double *sig, *eps;      // [n][nu], device: sigma_uv (with the LJ lambda), sqrt(eps_u eps_v)
+  double qv[kMaxSites], rhov[kMaxSites];
+  int nu, n, ad1;  // ad1: the LJ lambda derivative (else the Coulomb one)
+  double lambda, cc;
+};
 
 }  // namespace r3d

@@ -35,6 +35,7 @@
 // iteration never applies it.  All passes take a descriptor table so that one
 // launch can serve many solves of different grids (batching).
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <type_traits>
 #include <math.h>
 #include <stdint.h>
@@ -903,6 +904,121 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
+}
+
+// ======================================================================
+// Post-solve per-atom integrals over g (cal_grad.cu:41-90, cal_euv.cu:29-65,
+// cal_ad1.cu, cal_ad2.cu), all atoms, sites and voxels in one launch: a CTA
+// takes one chunk of voxels and 256 atoms (one per thread); the chunk goes
+// through shared memory in tiles (g of every site and the voxel positions),
+// every thread sums its atom's terms over the tile, and the chunk's sums go
+// to partials [chunk][atom][k] that k_atom_reduce adds up.  Per atom
+// (k): 0-2 the force integrand sum_v rho_v g (24 eps s6 (2 s6 - 1) / r^2 +
+// q_u q_v cc / r^3) (x, y, z of voxel - atom), 3 the lambda derivative
+// (LJ: 24 eps s6 (2 s6 - 1) / lambda, r >= sigma lambda / 2; otherwise the
+// Coulomb term q_u q_v cc / r), 4.. the energy per site rho_v g (4 eps s6
+// (s6 - 1) + q_u q_v cc / r); terms only for r >= sigma_uv / 2.
+// ======================================================================
+constexpr int kIntTile = 256;  // voxels per shared-memory tile
+
+template <int NS>
+__global__ void __launch_bounds__(kThreads)
+    k_atom_integrals(IntAtoms at, const double *g, long long N, int nx, int ny, int nz,
+                     double dx, double dy, double dz, long long chunk, double *part) {
+  constexpr int M = NS > 0 ? NS : kMaxSites;
+  __shared__ double sg[M][kIntTile];
+  __shared__ double sx[kIntTile], sy[kIntTile], sz[kIntTile];
+  const int n = NS > 0 ? NS : at.n;
+  const int a = blockIdx.y * blockDim.x + threadIdx.x;
+  const bool live = a < at.nu;
+  const double ax = live ? at.x[a] : 0, ay = live ? at.y[a] : 0, az = live ? at.z[a] : 0;
+  const double qa = live ? at.q[a] : 0;
+  double sig[M], eps[M];
+#pragma unroll
+  for (int v = 0; v < M; ++v) {
+    sig[v] = (live && v < n) ? at.sig[v * at.nu + a] : 0;
+    eps[v] = (live && v < n) ? at.eps[v * at.nu + a] : 0;
+  }
+  double fx = 0, fy = 0, fz = 0, ad = 0, e[M];
+#pragma unroll
+  for (int v = 0; v < M; ++v) e[v] = 0;
+  const long long c0 = blockIdx.x * chunk, c1 = min(N, c0 + chunk);
+  for (long long t0 = c0; t0 < c1; t0 += kIntTile) {
+    const int nt = (int)min((long long)kIntTile, c1 - t0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+      const long long ip = t0 + i;
+      const int x = (int)(ip % nx), y = (int)((ip / nx) % ny), z = (int)(ip / ((long long)nx * ny));
+      sx[i] = (x - nx / 2) * dx;
+      sy[i] = (y - ny / 2) * dy;
+      sz[i] = (z - nz / 2) * dz;
+      for (int v = 0; v < n; ++v) sg[v][i] = g[(long long)v * N + ip];
+    }
+    __syncthreads();
+    if (!live) continue;
+    for (int i = 0; i < nt; ++i) {
+      const double ddx = sx[i] - ax, ddy = sy[i] - ay, ddz = sz[i] - az;
+      const double r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+      const double r1 = sqrt(r2);
+#pragma unroll
+      for (int v = 0; v < M; ++v) {
+        if (NS == 0 && v >= n) break;
+        const double gv = sg[v][i];
+        const double qq = qa * at.qv[v] * at.cc;
+        const double s2 = sig[v] * sig[v] / r2, s6 = s2 * s2 * s2;
+        const double w = at.rhov[v] * gv;
+        if (r1 >= sig[v] * 0.5) {
+          const double fm = (eps[v] * 24.0 * s6 / r2 * (2.0 * s6 - 1.0) + qq / (r2 * r1)) * w;
+          fx += fm * ddx;
+          fy += fm * ddy;
+          fz += fm * ddz;
+          e[v] += (eps[v] * 4.0 * s6 * (s6 - 1.0) + qq / r1) * w;
+          if (!at.ad1) ad += qq / r1 * w;
+        }
+        if (at.ad1 && r1 >= sig[v] * at.lambda * 0.5)
+          ad += eps[v] * 24.0 * s6 * (2.0 * s6 - 1.0) / at.lambda * w;
+      }
+    }
+  }
+  if (!live) return;
+  const int K = 4 + n;
+  double *o = part + ((long long)blockIdx.x * at.nu + a) * K;
+  o[0] = fx;
+  o[1] = fy;
+  o[2] = fz;
+  o[3] = ad;
+  for (int v = 0; v < n; ++v) o[4 + v] = e[v];
+}
+
+// out[a][k] = sum over the chunks of part[chunk][a][k]
+__global__ void k_atom_reduce(const double *part, int nchunk, long long nk, double *out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nk;
+       i += (long long)gridDim.x * blockDim.x) {
+    double s = 0;
+    for (int c = 0; c < nchunk; ++c) s += part[(long long)c * nk + i];
+    out[i] = s;
+  }
+}
+
+void launch_atom_integrals(const IntAtoms &at, const double *g, long long N, const int *grid,
+                           const double *dr, double *part, int nchunk, double *out,
+                           cudaStream_t s) {
+  const long long chunk = (N + nchunk - 1) / nchunk;
+  dim3 gr(nchunk, (at.nu + kThreads - 1) / kThreads);
+#define R3D_INT(NS)                                                                      \
+  k_atom_integrals<NS><<<gr, kThreads, 0, s>>>(at, g, N, grid[0], grid[1], grid[2], dr[0], \
+                                               dr[1], dr[2], chunk, part)
+  switch (at.n) {
+    case 1: R3D_INT(1); break;
+    case 2: R3D_INT(2); break;
+    case 3: R3D_INT(3); break;
+    case 4: R3D_INT(4); break;
+    default: R3D_INT(0); break;
+  }
+#undef R3D_INT
+  const long long nk = (long long)at.nu * (4 + at.n);
+  k_atom_reduce<<<(int)std::min<long long>((nk + kThreads - 1) / kThreads, 1184), kThreads, 0,
+                  s>>>(part, nchunk, nk, out);
 }
 
 // Per-axis phase tables e^{-i k_j x_u} (FP64): ex[u][p] (k index j = 2p),

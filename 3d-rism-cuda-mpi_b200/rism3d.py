@@ -36,7 +36,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
            "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
            "r3d_server_destroy", "r3d_write_guv", "r3d_write_huv", "r3d_write_cuv",
-           "r3d_write_tuv", "r3d_read_tuv", "r3d_output"]
+           "r3d_write_tuv", "r3d_read_tuv", "r3d_output", "r3d_atom_integrals",
+           "r3d_write_gra", "r3d_write_euv", "r3d_write_ad"]
 REQ_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed"}
 
 
@@ -112,6 +113,10 @@ def _load():
         "r3d_write_tuv": [vp, cs],
         "r3d_read_tuv": [vp, cs],
         "r3d_output": [vp, cs],
+        "r3d_atom_integrals": [vp, dp, dp, dp],
+        "r3d_write_gra": [vp, cs],
+        "r3d_write_euv": [vp, cs],
+        "r3d_write_ad": [vp, cs],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -188,6 +193,19 @@ class RISM3D:
         """kind 'g' (.guv, binary), 'h' (.huv), 'c' (.cuv), 't' (.tuv)."""
         f = {"g": lib.r3d_write_guv, "h": lib.r3d_write_huv, "c": lib.r3d_write_cuv,
              "t": lib.r3d_write_tuv}[kind]
+        self._check(f(self.h, path.encode() if path else None))
+
+    def atom_integrals(self):
+        """(grad [nu, 3] kcal/(mol A), euv [nu, natv] J/mol, ad [nu] kcal/mol)"""
+        inf = self.info()
+        nu, n = inf["nu"], inf["natv"]
+        g, e, a = np.zeros((nu, 3)), np.zeros((nu, n)), np.zeros(nu)
+        self._check(lib.r3d_atom_integrals(self.h, _dp(g), _dp(e), _dp(a)))
+        return g, e, a
+
+    def write_atom_file(self, kind, path=None):
+        """kind 'd' (.gra), 'b' (.euv), 'a' (lambda derivative)."""
+        f = {"d": lib.r3d_write_gra, "b": lib.r3d_write_euv, "a": lib.r3d_write_ad}[kind]
         self._check(f(self.h, path.encode() if path else None))
 
     def read_tuv(self, path=None):

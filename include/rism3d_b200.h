@@ -192,14 +192,28 @@ int r3d_transfer_bytes(const r3d_ctx *ctx, unsigned long long *h2d,
  * r3d_read_tuv: read_tuv.cu, then loads t into the solve (the reference reads
  *   the file but never copies it to the device); after r3d_initialize.
  * r3d_output: RISM3D::output (output.cu): the files of the letters of
- *   outlist (NULL: the deck's) -- m (.xmu), c, g, h; d, a, b (forces,
- *   lambda derivatives, energies) are not built and give R3D_EINVAL. */
+ *   outlist (NULL: the deck's) -- m (.xmu), d (.gra), c, g, h, a (lambda
+ *   derivative), b (.euv). */
 int r3d_write_guv(r3d_ctx *ctx, const char *path);
 int r3d_write_huv(r3d_ctx *ctx, const char *path);
 int r3d_write_cuv(r3d_ctx *ctx, const char *path);
 int r3d_write_tuv(r3d_ctx *ctx, const char *path);
 int r3d_read_tuv(r3d_ctx *ctx, const char *path);
 int r3d_output(r3d_ctx *ctx, const char *outlist);
+
+/* ---- post-solve per-atom integrals over g ---------------------------------
+ * cal_grad.cu:41-90 (grad, [nu][3], kcal/(mol A)), cal_euv.cu:29-65 (euv,
+ * [nu][natv], J/mol), cal_ad1.cu / cal_ad2.cu (ad, [nu], kcal/mol: the LJ
+ * lambda derivative after r3d_set_ad(ctx, lambda, 1), else the Coulomb one),
+ * in the units the reference writes them; any output may be NULL.  One
+ * launch covers every atom, site and voxel (the reference launches a full
+ * grid per atom and site).  The writers produce output_grad.cu's .gra,
+ * output_euv.cu's .euv and output_ad.cu's <stem>-<adswitch>-<lambda>
+ * (path NULL: those names). */
+int r3d_atom_integrals(r3d_ctx *ctx, double *grad, double *euv, double *ad);
+int r3d_write_gra(r3d_ctx *ctx, const char *path);
+int r3d_write_euv(r3d_ctx *ctx, const char *path);
+int r3d_write_ad(r3d_ctx *ctx, const char *path);
 
 /* FFT3D::execute (fft3d.cu:72-78), stand-alone test seam: the reference's
  * half-shifted 3D transform F(k) = dv sum_r f(r) e^{-i k.r} of a real grid.

@@ -61,7 +61,23 @@ def deck(case, d):
         _xvk("h2o_vv.xvk" if case == "c1" else "naclaq_vv.xvk", d)
         p = synthetic.config(case, d, outlist="mg" if case == "c1" else "m")
         return os.path.basename(p)
+    # post-solve per-atom integrals: forces (.gra), energies (.euv) and the
+    # lambda derivatives of the LJ (-l) or Coulomb (-e) scaling
+    if case == "s64nacl_post":
+        _xvk("naclaq_vv.xvk", d)
+        synthetic.small(d, nu=24, grid=64, box=32.0, solvent="naclaq_vv.xvk", name=case,
+                        outlist="mdb", seed=11)
+        return case + ".inp"
+    if case in ("c1_post", "c1_ad1", "c1_ad2"):
+        _xvk("h2o_vv.xvk", d)
+        p = synthetic.config("c1", d, outlist="mdb" if case == "c1_post" else "ma")
+        os.rename(p, os.path.join(d, case + ".inp"))
+        return case + ".inp"
     raise ValueError(case)
+
+
+# command-line flags of a case (main.cu:6-69)
+ARGS = {"c1_ad1": ["-l", "0.8"], "c1_ad2": ["-e", "0.7"]}
 
 
 def main():
@@ -75,8 +91,8 @@ def main():
         inp = deck(case, d)
         t0 = time.time()
         with open(os.path.join(d, "stdout.log"), "w") as log:
-            rc = subprocess.run([BIN, inp], cwd=d, env=env, stdout=log, stderr=subprocess.STDOUT,
-                                timeout=1800).returncode
+            rc = subprocess.run([BIN] + ARGS.get(case, []) + [inp], cwd=d, env=env, stdout=log,
+                                stderr=subprocess.STDOUT, timeout=1800).returncode
         print(f"{case}: rc={rc} wall={time.time() - t0:.1f}s", flush=True)
         for f in os.listdir(d):
             if f.endswith(".xvk"):

@@ -42,6 +42,10 @@ def main(outdir):
         xmu = os.path.join(d, case + ".xmu")
         if os.path.exists(xmu):
             shutil.copyfile(xmu, os.path.join(dst, case + ".xmu"))
+        # per-atom integrals: <stem>.gra, <stem>.euv, <stem>-<switch>-<lambda>
+        for f in os.listdir(d):
+            if f.endswith((".gra", ".euv")) or f.startswith(case + "-"):
+                shutil.copyfile(os.path.join(d, f), os.path.join(dst, f))
         log = open(os.path.join(d, "stdout.log")).read()
         steps = re.findall(r"Step = (\d+) Reside = (\S+)", log)
         status = "diverged" if "diverged" in log else ("maxstep" if "reached limit" in log

@@ -85,8 +85,6 @@ def test_tuv_restart_and_outputs(refcase, tmp_path):
     s.output_files("mgh")  # the deck's stem with the reference's extensions
     for ext in (".xmu", ".guv", ".huv0"):
         assert os.path.exists(str(d / ("c1" + ext)))
-    with pytest.raises(R.R3DError):
-        s.output_files("d")  # forces: not built
     s.write_grid_file("t")
     sfe = _sfe(str(d / "c1.xmu"))
     s.close()
