@@ -37,7 +37,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
            "r3d_server_destroy", "r3d_write_guv", "r3d_write_huv", "r3d_write_cuv",
            "r3d_write_tuv", "r3d_read_tuv", "r3d_output", "r3d_atom_integrals",
-           "r3d_write_gra", "r3d_write_euv", "r3d_write_ad"]
+           "r3d_write_gra", "r3d_write_euv", "r3d_write_ad", "r3d_xrism_default_opts",
+           "r3d_xrism_read_deck", "r3d_xrism_solve", "r3d_xrism_write_xvk"]
 REQ_STATE = {0: "queued", 1: "active", 2: "done", 3: "failed"}
 
 
@@ -59,6 +60,27 @@ class Result(ctypes.Structure):
                 ("pmv", ctypes.c_double), ("pressure", ctypes.c_double),
                 ("queued_s", ctypes.c_double), ("admitted_s", ctypes.c_double),
                 ("finished_s", ctypes.c_double), ("error", ctypes.c_char * 256)]
+
+
+class XrismAtom(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 8), ("species", ctypes.c_int), ("sym", ctypes.c_int),
+                ("sigma", ctypes.c_double), ("epsilon", ctypes.c_double),
+                ("charge", ctypes.c_double), ("x", ctypes.c_double), ("y", ctypes.c_double),
+                ("z", ctypes.c_double), ("density", ctypes.c_double)]
+
+
+class XrismOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("ntab", ctypes.c_int), ("dr", ctypes.c_double),
+                ("temperature", ctypes.c_double), ("closure", ctypes.c_int),
+                ("pse_n", ctypes.c_int), ("tol", ctypes.c_double), ("maxstep", ctypes.c_int),
+                ("history", ctypes.c_int), ("mix", ctypes.c_double), ("nladder", ctypes.c_int),
+                ("verbose", ctypes.c_int)]
+
+
+class XrismResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("steps", ctypes.c_int), ("natv", ctypes.c_int),
+                ("rms", ctypes.c_double), ("xt", ctypes.c_double),
+                ("ms_device", ctypes.c_double)]
 
 
 def _load():
@@ -117,11 +139,18 @@ def _load():
         "r3d_write_gra": [vp, cs],
         "r3d_write_euv": [vp, cs],
         "r3d_write_ad": [vp, cs],
+        "r3d_xrism_read_deck": [cs, ctypes.POINTER(XrismAtom), ci, ip, ctypes.POINTER(XrismOpts)],
+        "r3d_xrism_solve": [ctypes.POINTER(XrismOpts), ctypes.POINTER(XrismAtom), ci, dp,
+                            ctypes.POINTER(XrismResult)],
+        "r3d_xrism_write_xvk": [cs, ctypes.POINTER(XrismOpts), ctypes.POINTER(XrismAtom), ci,
+                                dp, cd],
     }
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = ci
+    L.r3d_xrism_default_opts.argtypes = [ctypes.POINTER(XrismOpts)]
+    L.r3d_xrism_default_opts.restype = None
     L.r3d_last_error.argtypes = [vp]
     L.r3d_last_error.restype = cs
     return L
@@ -425,3 +454,87 @@ class Server:
             self.h = None
 
     __del__ = close
+
+
+class XRISM:
+    """1D XRISM solve of a bulk solvent on the GPU, making the .xvk table the
+    3D solve reads (solvent_read.cc:10-94); r3d_xrism_* in the C-ABI.
+
+        x = XRISM.from_deck("h2o_vv.xvk", temperature=298.15)
+        table = x.solve()               # [ntab][natv][natv]
+        x.write_xvk("water_298.xvk")
+
+    atoms: dicts with name, species (spc), sym, sigma [A], epsilon [J/mol],
+    charge [e], xyz [A] and density [M] -- the .xvk atom table."""
+
+    def __init__(self, atoms, device=0, **opts):
+        o = XrismOpts()
+        lib.r3d_xrism_default_opts(ctypes.byref(o))
+        o.device = device
+        for k, v in opts.items():
+            if not hasattr(o, k):
+                raise TypeError(f"unknown option {k}")
+            setattr(o, k, v)
+        self.opts = o
+        self.atoms = [dict(a) for a in atoms]
+        self.table = None
+        self.result = None
+
+    @classmethod
+    def from_deck(cls, path, device=0, **opts):
+        """Atoms, ntab, dr and temperature from an .xvk header (its table, if
+        any, is ignored); keyword options override them."""
+        arr = (XrismAtom * 1024)()
+        n = ctypes.c_int()
+        o = XrismOpts()
+        lib.r3d_xrism_default_opts(ctypes.byref(o))
+        rc = lib.r3d_xrism_read_deck(os.fsencode(path), arr, 1024, ctypes.byref(n), ctypes.byref(o))
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+        atoms = [dict(name=a.name.decode(), species=a.species, sym=a.sym, sigma=a.sigma,
+                      epsilon=a.epsilon, charge=a.charge, xyz=(a.x, a.y, a.z),
+                      density=a.density) for a in arr[:n.value]]
+        base = dict(ntab=o.ntab, dr=o.dr, temperature=o.temperature)
+        base.update(opts)
+        return cls(atoms, device=device, **base)
+
+    def _atoms(self):
+        arr = (XrismAtom * len(self.atoms))()
+        for a, d in zip(arr, self.atoms):
+            a.name = str(d.get("name", "X")).encode()[:7]
+            a.species = int(d.get("species", d.get("spc", 1)))
+            a.sym = int(d["sym"])
+            a.sigma = float(d.get("sigma", d.get("sig", 0.0)))
+            a.epsilon = float(d.get("epsilon", d.get("eps", 0.0)))
+            a.charge = float(d.get("charge", d.get("q", 0.0)))
+            a.x, a.y, a.z = (float(v) for v in d["xyz"])
+            a.density = float(d.get("density", d.get("den", 0.0)))
+        return arr
+
+    @property
+    def natv(self):
+        return max(abs(int(d["sym"])) for d in self.atoms)
+
+    def solve(self):
+        """Runs the solve; returns the table [ntab][natv][natv] (None unless
+        it converged).  self.result: status, steps, rms, xt, ms_device."""
+        arr = self._atoms()
+        nv = self.natv
+        tab = np.zeros((self.opts.ntab, nv, nv))
+        r = XrismResult()
+        rc = lib.r3d_xrism_solve(ctypes.byref(self.opts), arr, len(self.atoms), _dp(tab),
+                                 ctypes.byref(r))
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())
+        self.result = dict(status=STATUS[r.status], steps=r.steps, rms=r.rms, xt=r.xt,
+                           ms_device=r.ms_device, natv=r.natv)
+        self.table = tab if r.status == CONVERGED else None
+        return self.table
+
+    def write_xvk(self, path):
+        if self.table is None:
+            raise R3DError(5, "no converged table to write")
+        rc = lib.r3d_xrism_write_xvk(os.fsencode(path), ctypes.byref(self.opts), self._atoms(),
+                                     len(self.atoms), _dp(self.table), self.result["xt"])
+        if rc:
+            raise R3DError(rc, lib.r3d_last_error(None).decode())

@@ -325,6 +325,78 @@ int r3d_server_release(r3d_server *s, long long ticket);
 /* Finishes every queued and admitted solve, then frees the server. */
 int r3d_server_destroy(r3d_server *s);
 
+/* ---- 1D XRISM solvent solve: making .xvk tables -------------------------
+ * The reference reads its solvent susceptibility from an .xvk table
+ * (solvent_read.cc:10-94) and ships no program that makes one.  These calls
+ * make it: an extended-RISM (XRISM) solve of the bulk solvent on a radial
+ * grid, written in the format solvent_read.cc:31-85 reads.
+ *
+ * The solvent is the .xvk atom table: one line per atom of each molecule
+ * (species) with its site class `sym` (atoms whose |sym| agree are one site
+ * of the 3D solve, solvent_read.cc:70-76), LJ sigma [A] and epsilon
+ * [J/mol] (Lorentz-Berthelot mixing), charge [e], position [A] in its
+ * molecule and density [M].  Grid: r_i = i dr and k_j = j pi/(ntab dr),
+ * i, j = 1..ntab-1; ntab a power of two in [64, 16384].  Closure on
+ * t = h - c_s with the Coulomb split erf(r/1 A)/r (its k-space part added
+ * analytically); charges switched on over `nladder` stages (every stage but
+ * the last stops at RMS 1e-5); modified-DIIS mixing of `history` entries
+ * with step `mix`, halved (and the stage's best state restored) whenever
+ * the RMS grows tenfold over the stage's best.  The table row j holds
+ * xvv[A][B](k_j) = sum_{b in B} (w_ab(k_j) + rho_b h_ab(k_j)) (row ntab: the
+ * intramolecular part alone), the quantity calculate_cuda.cu:39-52 uses.
+ * Errors are reported by r3d_last_error(NULL). */
+typedef struct r3d_xrism_atom {
+  char name[8];      /* label written to the table                 */
+  int species;       /* molecule index (SPC column), 1-based        */
+  int sym;           /* site class (SYM column); sign ignored       */
+  double sigma;      /* A                                           */
+  double epsilon;    /* J/mol                                       */
+  double charge;     /* e                                           */
+  double x, y, z;    /* A, within the molecule                      */
+  double density;    /* M (mol/L) of the molecule                   */
+} r3d_xrism_atom;
+
+typedef struct r3d_xrism_opts {
+  int device;         /* CUDA device ordinal                         */
+  int ntab;           /* grid points (power of two, 64..16384)        */
+  double dr;          /* A                                           */
+  double temperature; /* K                                           */
+  int closure;        /* R3D_KH, R3D_HNC or R3D_PSE                   */
+  int pse_n;          /* PSE order (R3D_PSE)                          */
+  double tol;         /* RMS of the t update that ends the solve      */
+  int maxstep;        /* evaluations per coupling stage               */
+  int history;        /* DIIS entries, 1..32                          */
+  double mix;         /* DIIS step                                    */
+  int nladder;        /* charge-coupling stages, >= 1                 */
+  int verbose;        /* 1: print the RMS of each evaluation          */
+} r3d_xrism_opts;
+
+typedef struct r3d_xrism_result {
+  int status;        /* R3D_CONVERGED / R3D_MAXSTEP / R3D_DIVERGED   */
+  int steps;         /* evaluations over all stages                  */
+  int natv;          /* site classes (table is [ntab][natv][natv])   */
+  double rms;        /* RMS of the last evaluation                   */
+  double xt;         /* isothermal compressibility [1/Pa]            */
+  double ms_device;  /* device time of the iterations                */
+} r3d_xrism_result;
+
+/* Defaults: KH, tol 1e-10, maxstep 10000, history 20, mix 0.3, nladder 5,
+ * ntab 8192, dr 0.05, 298.15 K, device 0. */
+void r3d_xrism_default_opts(r3d_xrism_opts *opts);
+/* Reads the header and atom table of an .xvk (the table itself, if any, is
+ * ignored) into atoms[0..max_atoms) and opts' ntab, dr and temperature. */
+int r3d_xrism_read_deck(const char *path, r3d_xrism_atom *atoms, int max_atoms,
+                        int *natom, r3d_xrism_opts *opts);
+/* One solve on the GPU.  xvv (may be NULL): [ntab][natv][natv] host array,
+ * natv = the largest |sym|.  The table is written only when the solve
+ * converged (status R3D_CONVERGED); the call returns R3D_OK either way. */
+int r3d_xrism_solve(const r3d_xrism_opts *opts, const r3d_xrism_atom *atoms, int natom,
+                    double *xvv, r3d_xrism_result *result);
+/* Writes the .xvk (solvent_read.cc:31-58 layout, one table row per line). */
+int r3d_xrism_write_xvk(const char *path, const r3d_xrism_opts *opts,
+                        const r3d_xrism_atom *atoms, int natom, const double *xvv,
+                        double xt);
+
 #ifdef __cplusplus
 }
 #endif

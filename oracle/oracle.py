@@ -59,6 +59,9 @@ def lib():
         L.orc_get.argtypes = [c_p, c_i, dp]
         L.orc_set_t.argtypes = [c_p, dp]
         L.orc_fft3d.argtypes = [c_i, c_i, c_i, dp, dp, c_i]
+        L.orc_dst1.argtypes = [dp, dp, c_i]
+        L.orc_xrism_solve.argtypes = [c_i, ip, ip, dp, dp, dp, dp, dp, c_d, c_i, c_d,
+                                      c_i, c_i, c_d, c_i, c_i, c_d, c_i, dp, dp]
         _lib = L
     return _lib
 
@@ -188,3 +191,63 @@ def fft3d(data, box, direction):
     flat = a.view(np.float64).reshape(-1)
     lib().orc_fft3d(nx, ny, nz, _dp(b), _dp(flat), direction)
     return a
+
+
+# ---------------------------------------------------------------------------
+# 1D XRISM solvent solve (oracle/xrism_oracle.c)
+
+def read_xvk(path):
+    """Parse an .xvk table the way the reference reader does
+    (src-cuda-mpi/solvent_read.cc:31-58): header, atom table and
+    ntab rows of natv*natv values [iv2][iv1]; tokens may wrap lines."""
+    import gzip
+    op = gzip.open if str(path).endswith(".gz") else open
+    with op(path, "rt") as fh:
+        lines = fh.read().splitlines()
+    h = lines[1].split()
+    num, natv, ntab, dr = int(h[1]), int(h[2]), int(h[3]), float(h[4])
+    h2 = lines[2].split()
+    atoms = []
+    for ln in lines[4:4 + num]:
+        t = ln.split()
+        atoms.append(dict(name=t[1], spc=int(t[2]), sym=int(t[3]), sig=float(t[4]),
+                          eps=float(t[5]), q=float(t[6]),
+                          xyz=(float(t[7]), float(t[8]), float(t[9])), den=float(t[10])))
+    toks = " ".join(lines[5 + num:]).split()
+    xvv = np.array([float(v) for v in toks[:ntab * natv * natv]]).reshape(ntab, natv, natv)
+    return dict(num=num, natv=natv, ntab=ntab, dr=dr, nspecies=int(h2[1]),
+                temper=float(h2[2]), xt=float(h2[3]), atoms=atoms, xvv=xvv)
+
+
+def dst1(f):
+    """S_j = sum_{i=1}^{N-1} f_i sin(pi i j / N) on f[1..N-1] (f[0] ignored)."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    S = np.zeros_like(f)
+    lib().orc_dst1(_dp(f), _dp(S), len(f))
+    return S
+
+
+def xrism_solve(atoms, temper, ntab, dr, closure=CLOS_KH, pse_n=1, tol=1e-10,
+                maxstep=10000, history=20, mix=0.3, nladder=5):
+    """1D XRISM solve; atoms as read_xvk()["atoms"].  Returns (xvv, info) with
+    xvv [ntab][natv][natv] and info = dict(xt, rms, steps, status)."""
+    n = len(atoms)
+    spc = np.array([a["spc"] for a in atoms], dtype=np.int32)
+    sym = np.array([a["sym"] for a in atoms], dtype=np.int32)
+    sig = np.array([a["sig"] for a in atoms], dtype=np.float64)
+    eps = np.array([a["eps"] for a in atoms], dtype=np.float64)
+    q = np.array([a["q"] for a in atoms], dtype=np.float64)
+    xyz = np.array([a["xyz"] for a in atoms], dtype=np.float64).reshape(n, 3)
+    den = np.array([a["den"] for a in atoms], dtype=np.float64)
+    natv = int(np.abs(sym).max())
+    xvv = np.zeros((ntab, natv, natv))
+    info = np.zeros(5)
+    ip = ctypes.POINTER(ctypes.c_int)
+    rc = lib().orc_xrism_solve(n, spc.ctypes.data_as(ip), sym.ctypes.data_as(ip), _dp(sig),
+                               _dp(eps), _dp(q), _dp(xyz), _dp(den), float(temper), int(ntab),
+                               float(dr), int(closure), int(pse_n), float(tol), int(maxstep),
+                               int(history), float(mix), int(nladder), _dp(xvv), _dp(info))
+    if rc != 0:
+        raise OracleError("orc_xrism_solve: bad input (%d)" % rc)
+    return xvv, dict(xt=info[0], rms=info[1], steps=int(info[2]),
+                     status=STATUS[int(info[3])])
