@@ -149,27 +149,34 @@ __device__ __forceinline__ void pack_pair(double2 *z, int N, int i, double s, do
 }
 
 // q radix-2 decimation-in-frequency stages starting at span L, fused in
-// registers: group g holds Z[base + e*S], e < 2^q, S = L / 2^q.
+// registers: group g holds Z[base + e*S], e < 2^q, S = L / 2^q.  The
+// twiddle of element e at stage t is e^{-2 pi i u / Lt} with u = j +
+// (e mod 2^{q-t}) S: one table load per stage (e^{-2 pi i j / Lt}) times a
+// 2^q-th root of unity held in registers.
 template <int Q>
-__device__ void fft_pass(double2 *Z, const double2 *tw, int M, int L) {
+__device__ void fft_pass(double2 *Z, const double2 *tw, int lgM, int lgL) {
   constexpr int G = 1 << Q;
-  const int S = L >> Q;
-  const int ngroups = M >> Q;
+  const int lgS = lgL - Q;
+  const int S = 1 << lgS;
+  const int ngroups = 1 << (lgM - Q);
+  double2 root[G / 2];  // e^{-2 pi i k / 2^Q}
+#pragma unroll
+  for (int k = 0; k < G / 2; ++k) root[k] = tw[k << (lgM - Q)];
   for (int g = threadIdx.x; g < ngroups; g += blockDim.x) {
-    const int b = g / S, j = g - b * S;
-    const int base = b * L + j;
+    const int b = g >> lgS, j = g & (S - 1);
+    const int base = (b << lgL) + j;
     double2 x[G];
 #pragma unroll
     for (int e = 0; e < G; ++e) x[e] = Z[zpad(base + e * S)];
 #pragma unroll
     for (int t = 0; t < Q; ++t) {
-      const int Lt = L >> t;
       const int d = G >> (t + 1);
+      const double2 wj = tw[j << (lgM - lgL + t)];  // e^{-2 pi i j / Lt}
 #pragma unroll
       for (int e = 0; e < G; ++e) {
         if (e & d) continue;
-        const int u = (j + e * S) & (Lt - 1);
-        const double2 w = tw[u * (M / Lt)];  // e^{-2 pi i u / Lt}
+        const int k = (e & (2 * d - 1)) << t;  // (e mod 2^{Q-t}) 2^t
+        const double2 w = k == 0 ? wj : cmul(wj, root[k]);
         const double2 a = x[e], c = x[e + d];
         x[e] = make_double2(a.x + c.x, a.y + c.y);
         x[e + d] = cmul(make_double2(a.x - c.x, a.y - c.y), w);
@@ -206,20 +213,19 @@ __device__ void sine_transform(const XP &p, const double2 *z, double2 *Z, double
   }
   __syncthreads();
   // log2(M) stages in passes of up to four
-  int L = M, s = 31 - __clz(M);
-  while (s > 0) {
-    const int q = s >= 4 ? 4 : s;
-    if (q == 4) fft_pass<4>(Z, tw, M, L);
-    else if (q == 3) fft_pass<3>(Z, tw, M, L);
-    else if (q == 2) fft_pass<2>(Z, tw, M, L);
-    else fft_pass<1>(Z, tw, M, L);
+  const int lgM = 31 - __clz(M);
+  for (int lgL = lgM; lgL > 0;) {
+    const int q = lgL >= 4 ? 4 : lgL;
+    if (q == 4) fft_pass<4>(Z, tw, lgM, lgL);
+    else if (q == 3) fft_pass<3>(Z, tw, lgM, lgL);
+    else if (q == 2) fft_pass<2>(Z, tw, lgM, lgL);
+    else fft_pass<1>(Z, tw, lgM, lgL);
     __syncthreads();
-    L >>= q;
-    s -= q;
+    lgL -= q;
   }
   // Y_m = (Z_m + conj Z_{M-m})/2 + e^{-2 pi i m/N} (Z_m - conj Z_{M-m})/(2i);
   // Z is in bit-reversed order
-  const int lg = 31 - __clz(M);
+  const int lg = lgM;
   const int C = (M + nt - 1) / nt;  // m per thread (<= 16 for M <= 8192)
   const int m0 = tid * C;
   double ry[16], iy[16];
@@ -588,20 +594,23 @@ __global__ void __launch_bounds__(kXWide) xr_pack_inv(XP p) {
   pack_pair(p.zi + (size_t)pr * p.M, p.N, j, p.E[j].y, t[j], t[p.N - j]);
 }
 
-// bordered DIIS system [G 1; 1^T 0] c = e_n (order m = n + 1 <= 32) by the
-// whole CTA in shared memory: partial pivoting on the column, row updates
-// spread over the threads.  G: the Gram matrix of the n entries (oldest
+// bordered DIIS system [G 1; 1^T 0] c = e_n (order m = n + 1 <= 32) in
+// shared memory by the CTA: partial pivoting on the column, one multiplier
+// per row, the row updates spread over the threads, back substitution by
+// one warp (row r on lane r).  G: the Gram matrix of the n entries (oldest
 // first), stride 33.
 __device__ void diis_solve_block(const double *G, int n, double *coef) {
   __shared__ double A[kXMaxH + 1][kXMaxH + 2];  // [row][col], col m = rhs
+  __shared__ double mult[kXMaxH + 1];
   __shared__ int piv_row;
   __shared__ bool ok;
   const int m = n + 1, tid = threadIdx.x, nt = blockDim.x;
   double sc = 0.0;
   for (int i = 0; i < n; ++i) sc = fmax(sc, G[i * 33 + i]);
   sc = sc > 0.0 ? 1.0 / sc : 1.0;
-  for (int e = tid; e < m * (m + 1); e += nt) {
-    const int r = e / (m + 1), x = e - r * (m + 1);
+  for (int e = tid; e < 32 * 33; e += nt) {
+    const int r = e / 33, x = e - r * 33;
+    if (r >= m || x > m) continue;
     double v;
     if (x == m) v = r == n ? 1.0 : 0.0;
     else if (r < n && x < n) v = G[r * 33 + x] * sc;
@@ -611,74 +620,85 @@ __device__ void diis_solve_block(const double *G, int n, double *coef) {
   if (tid == 0) ok = true;
   __syncthreads();
   for (int col = 0; col < m; ++col) {
-    if (tid < 32) {  // pivot search over rows col..m-1
-      double best = -1.0;
-      int bl = col;
-      for (int r = col + tid; r < m; r += 32)
-        if (fabs(A[r][col]) > best) { best = fabs(A[r][col]); bl = r; }
+    if (tid < 32) {  // pivot: largest |A[r][col]|, r >= col; swap; multipliers
+      const int r = tid;
+      double best = (r >= col && r < m) ? fabs(A[r][col]) : -1.0;
+      int bl = r;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const double ob = __shfl_xor_sync(0xffffffffu, best, o);
         const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
         if (ob > best || (ob == best && ol < bl)) { best = ob; bl = ol; }
       }
-      if (tid == 0) {
-        piv_row = bl;
-        if (!(best > 1e-300)) ok = false;
+      if (!(best > 1e-300)) {
+        if (tid == 0) ok = false;
+      } else {
+        if (bl != col)
+          for (int x = tid; x <= m; x += 32) {
+            const double t = A[col][x];
+            A[col][x] = A[bl][x];
+            A[bl][x] = t;
+          }
+        __syncwarp();
+        if (r > col && r < m) mult[r] = A[r][col] / A[col][col];
       }
     }
     __syncthreads();
     if (!ok) break;
-    const int pr = piv_row;
-    if (pr != col)
-      for (int x = tid; x <= m; x += nt) {
-        const double t = A[col][x];
-        A[col][x] = A[pr][x];
-        A[pr][x] = t;
-      }
-    __syncthreads();
-    const int rows = m - col - 1, cols = m + 1 - col;
-    for (int e = tid; e < rows * cols; e += nt) {
-      const int r = col + 1 + e / cols, x = col + e % cols;
-      if (x == col) continue;  // the multiplier column is read below
-      A[r][x] -= A[r][col] / A[col][col] * A[col][x];
+    for (int e = tid; e < 32 * 33; e += nt) {
+      const int r = e / 33, x = e - r * 33;
+      if (r > col && r < m && x > col && x <= m) A[r][x] -= mult[r] * A[col][x];
     }
     __syncthreads();
   }
-  if (tid == 0) {
-    double sol[kXMaxH + 1];
+  if (tid < 32) {
+    const int r = tid;
+    double rhs = r < m ? A[r][m] : 0.0, sol = 0.0;
     bool fin = ok;
     if (ok)
-      for (int r = m - 1; r >= 0; --r) {
-        double v = A[r][m];
-        for (int x = r + 1; x < m; ++x) v -= A[r][x] * sol[x];
-        sol[r] = v / A[r][r];
-        if (r < n && !isfinite(sol[r])) fin = false;
+      for (int col = m - 1; col >= 0; --col) {
+        const double v = __shfl_sync(0xffffffffu, rhs / (r < m ? A[r][r] : 1.0), col);
+        if (r == col) sol = v;
+        if (r < col) rhs -= A[r][col] * v;
       }
-    for (int i = 0; i < n; ++i) coef[i] = fin ? sol[i] : (i == n - 1 ? 1.0 : 0.0);
+    fin = __all_sync(0xffffffffu, fin && (r >= n || isfinite(sol)));
+    if (r < n) coef[r] = fin ? sol : (r == n - 1 ? 1.0 : 0.0);
   }
 }
 
 // f = t_new - t of the evaluation into the ring, <f, f_n> against the ring
 // entries in one pass; the last CTA reduces (fixed order), updates the Gram
 // matrix, decides (converged, next stage, rollback, mix) and solves the
-// DIIS system.
+// DIIS system.  Every CTA stages the control fields and the Gram block at
+// its start, so the last one finds them in shared memory.
 __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
   XCtl *c = p.ctl;
   if (!xr_running(c)) return;
   const int H = p.H;
-  __shared__ int s_head, s_nn;
+  __shared__ int s_head, s_nn, s_stage, s_stage_steps, s_rollbacks;
+  __shared__ double s_best, s_eta;
   __shared__ int slot[kXMaxH];
   __shared__ double red[kXWide / 32][kXMaxH];
+  __shared__ double G[32 * 33];  // Gram of the nn entries, oldest first
+  __shared__ double dots[kXMaxH];
   __shared__ bool last;
   if (threadIdx.x == 0) {
     s_head = c->head;
     s_nn = c->nh < H ? c->nh + 1 : H;  // entries after the push
+    s_stage = c->stage;
+    s_stage_steps = c->stage_steps;
+    s_rollbacks = c->rollbacks;
+    s_best = c->best;
+    s_eta = c->eta;
   }
   __syncthreads();
   const int head = s_head, nn = s_nn;
   if (threadIdx.x < nn) slot[threadIdx.x] = (head - (nn - 1) + (int)threadIdx.x + H) % H;
   __syncthreads();
+  for (int e = threadIdx.x; e < nn * nn; e += blockDim.x) {
+    const int a = e / nn, b = e - a * nn;
+    G[a * 33 + b] = c->gram[slot[a] * H + slot[b]];
+  }
   const size_t rows = (size_t)p.P * p.Ns;
   const double *t0 = p.ring_t + (size_t)head * rows;
   double *f0 = p.ring_f + (size_t)head * rows;
@@ -715,8 +735,6 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
   if (!last) return;
   __threadfence();
   // ---- the last CTA
-  __shared__ double G[32 * 33];  // Gram of the nn entries, oldest first
-  __shared__ double dots[kXMaxH];
   {  // 8 threads per entry sum the partials of all CTAs (fixed order)
     const int n = threadIdx.x >> 3, part = threadIdx.x & 7;
     double s = 0.0;
@@ -726,10 +744,6 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
 #pragma unroll
     for (int o = 4; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, 8);
     if (part == 0 && n < nn) dots[n] = s;
-  }
-  for (int e = threadIdx.x; e < nn * nn; e += blockDim.x) {
-    const int a = e / nn, b = e - a * nn;
-    G[a * 33 + b] = c->gram[slot[a] * H + slot[b]];
   }
   __syncthreads();
   if (threadIdx.x < nn) {  // the newest entry's row and column
@@ -744,9 +758,9 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
   if (threadIdx.x == 0) {
     c->counter = 0;
     const double err = sqrt(G[(nn - 1) * 33 + nn - 1] / ((double)p.P * (p.N - 1)));
-    const int stage = c->stage;
-    const int stage_steps = c->stage_steps + 1;
-    const double best = c->best;
+    const int stage = s_stage;
+    const int stage_steps = s_stage_steps + 1;
+    const double best = s_best;
     c->rms = err;
     c->steps += 1;
     c->stage_steps = stage_steps;
@@ -773,7 +787,7 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
       c->status = MAXSTEP;
       dcs = 0;
     } else if (!(err <= 10.0 * best)) {
-      const int rb = c->rollbacks + 1;
+      const int rb = s_rollbacks + 1;
       c->rollbacks = rb;
       if (!isfinite(best) || rb > kXRollbacks) {
         c->status = DIVERGED;
@@ -781,7 +795,7 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
       } else {
         c->mode = XM_ROLLBACK;
         c->nh = 0;
-        c->eta = 0.5 * c->eta;
+        c->eta = 0.5 * s_eta;
         c->head = (head + 1) % H;
         dcs = 2;
       }
@@ -1021,7 +1035,7 @@ int r3d_xrism_solve(const r3d_xrism_opts *opts, const r3d_xrism_atom *atoms, int
   char *dmem = nullptr;
   XCtl *hctl = nullptr;
   const int nblk_dots =
-      std::max(1, std::min(296, (int)(((size_t)P * Ns + 8 * kXWide - 1) / (8 * kXWide))));
+      std::max(1, std::min(296, (int)(((size_t)P * Ns + 4 * kXWide - 1) / (4 * kXWide))));
   const size_t rowsz = (size_t)P * Ns * sizeof(double);
   const size_t zsz = (size_t)P * M * sizeof(double2);
   size_t off = 0;
