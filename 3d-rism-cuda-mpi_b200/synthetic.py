@@ -175,3 +175,60 @@ def small(outdir, nu=12, grid=32, box=16.0, solvent="h2o_vv.xvk", seed=7, closur
     sol = make_solute(nu, seed, radius=min(3.0, min(b) / 5), dmin=1.1, sig=(2.5, 3.8), qsd=0.35)
     return write_inp(os.path.join(outdir, f"{name}.inp"), sol, b, g, solvent,
                      closure=closure, mixer=mixer, **kw)
+
+
+# ---------------------------------------------------------------------------
+# Solvents of the benchmark configurations, made by the 1D XRISM solve
+# (rism3d.XRISM, on the GPU).  The reference ships water at 300 K and 0.2 M
+# NaCl with other ion LJ parameters; the configurations name:
+#   water     3-site water, O sigma 3.1507 A / eps 0.1521 kcal/mol / q -0.834,
+#             H sigma 0.4 A / eps 0.046 kcal/mol / q +0.417, O-H 0.9572 A,
+#             H-O-H 104.52 deg, 298.15 K, 0.0334 molecules/A^3
+#   nacl02    0.2 M NaCl in that water, Na+ sigma 2.43 A / eps 0.0874
+#             kcal/mol, Cl- sigma 4.40 A / eps 0.1 kcal/mol
+#   nacl01    0.1 M, same ions
+# The water density of the salt solutions drops by 0.98545 M per M of salt,
+# the ratio of the reference's own 0.2 M table (55.13587 M against 55.33296 M
+# for pure water).
+AVOGADRO = 6.02214076e23
+WATER_M = 0.0334 / (AVOGADRO * 1e-27)   # 0.0334 A^-3 in mol/L
+SALT_WATER_DROP = (55.33296 - 55.13587) / 0.2
+
+
+def water_atoms(density_m=WATER_M):
+    half = math.radians(104.52) / 2.0
+    hy, hz = 0.9572 * math.sin(half), 0.9572 * math.cos(half)
+    o = dict(name="O", species=1, sym=1, sigma=3.1507, epsilon=0.1521 * KCAL2J, charge=-0.834,
+             xyz=(0.0, 0.0, 0.0), density=density_m)
+    h = dict(name="H", species=1, sym=2, sigma=0.4, epsilon=0.046 * KCAL2J, charge=0.417,
+             xyz=(0.0, hy, hz), density=density_m)
+    return [o, h, dict(h, sym=-2, xyz=(0.0, -hy, hz))]
+
+
+def nacl_atoms(conc_m):
+    water = water_atoms(WATER_M - SALT_WATER_DROP * conc_m)
+    return water + [
+        dict(name="Na", species=2, sym=3, sigma=2.43, epsilon=0.0874 * KCAL2J, charge=1.0,
+             xyz=(0.0, 0.0, 0.0), density=conc_m),
+        dict(name="Cl", species=3, sym=4, sigma=4.40, epsilon=0.1 * KCAL2J, charge=-1.0,
+             xyz=(0.0, 0.0, 0.0), density=conc_m)]
+
+
+BASELINE_SOLVENTS = {"water_298": lambda: water_atoms(),
+                     "nacl02_298": lambda: nacl_atoms(0.2),
+                     "nacl01_298": lambda: nacl_atoms(0.1)}
+
+
+def make_solvent(name, outdir, device=0, ntab=8192, dr=0.05, temperature=298.15):
+    """Solve one of BASELINE_SOLVENTS with the 1D XRISM solver and write
+    <outdir>/<name>.xvk; returns (path, result dict)."""
+    import rism3d
+    x = rism3d.XRISM(BASELINE_SOLVENTS[name](), device=device, ntab=ntab, dr=dr,
+                     temperature=temperature)
+    x.solve()
+    if x.result["status"] != "converged":
+        raise RuntimeError(f"1D solve of {name}: {x.result}")
+    os.makedirs(outdir, exist_ok=True)
+    path = os.path.join(outdir, name + ".xvk")
+    x.write_xvk(path)
+    return path, x.result

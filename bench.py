@@ -44,20 +44,111 @@ WORKLOAD_C3 = ("LARGE SINGLE SOLVE (not the headline): 512^3 grid, 256 A cell, 1
 FALLBACK_HBM_GBS = 6650.0
 
 
+# ------------------------------------------------------------- solvents
+# The configurations name 298.15 K water and 0.1 / 0.2 M NaCl with their own
+# ion LJ parameters; the reference ships water at 300 K and 0.2 M NaCl with
+# other ion parameters.  By default the run makes the named tables with the
+# 1D XRISM solve (synthetic.BASELINE_SOLVENTS; on the GPU, or with the CPU
+# oracle on the reference arm); --solvent shipped uses the reference's files.
+SOLVENT_FILES = {
+    "shipped": {"water": "h2o_vv.xvk", "nacl02": "naclaq_vv.xvk", "nacl01": "naclaq_vv.xvk"},
+    "baseline": {"water": "water_298.xvk", "nacl02": "nacl02_298.xvk",
+                 "nacl01": "nacl01_298.xvk"},
+}
+SOLVENT_DATA = {
+    "shipped": "the reference's shipped .xvk tables (water 300 K, 0.2 M NaCl)",
+    "baseline": "298.15 K water and 0.1 / 0.2 M NaCl of the configuration, tables made by "
+                "this repository's 1D XRISM solve",
+}
+SOLV = dict(SOLVENT_FILES["baseline"])
+_SOLVENT_DIR = None
+
+
+def prepare_solvents(kind, device=None):
+    """Makes this run's solvent tables once.  device: the GPU for the 1D
+    solves (None: the CPU oracle, for the reference arm).  Returns the 1D
+    solves' measurements (baseline tables made on the GPU) or None."""
+    global _SOLVENT_DIR
+    SOLV.clear()
+    SOLV.update(SOLVENT_FILES[kind])
+    d = tempfile.mkdtemp(prefix="r3dsolv_")
+    _SOLVENT_DIR = d
+    if kind == "shipped":
+        for name in ("h2o_vv", "naclaq_vv"):
+            with gzip.open(os.path.join(ROOT, "tests", "golden", name + ".xvk.gz"), "rb") as fi, \
+                    open(os.path.join(d, name + ".xvk"), "wb") as fo:
+                shutil.copyfileobj(fi, fo)
+        return None
+    import synthetic as S
+    if device is None:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        for name, make in S.BASELINE_SOLVENTS.items():
+            atoms = [dict(name=a["name"], spc=a["species"], sym=a["sym"], sig=a["sigma"],
+                          eps=a["epsilon"], q=a["charge"], xyz=a["xyz"], den=a["density"])
+                     for a in make()]
+            xvv, info = O.xrism_solve(atoms, 298.15, 8192, 0.05)
+            O.write_xvk(os.path.join(d, name + ".xvk"), atoms, 298.15, 8192, 0.05, xvv,
+                        info["xt"])
+        return None
+    report = {}
+    for name in S.BASELINE_SOLVENTS:
+        runs = []
+        for _ in range(2):  # the first also pays the CUDA context
+            t0 = time.perf_counter()
+            _, res = S.make_solvent(name, d, device=device)
+            runs.append((time.perf_counter() - t0, res))
+        (cold, _), (warm, res) = runs
+        report[name] = {"evaluations": res["steps"], "ms_device": res["ms_device"],
+                        "us_per_evaluation": 1e3 * res["ms_device"] / res["steps"],
+                        "e2e_ms": 1e3 * warm, "cold_e2e_ms": 1e3 * cold,
+                        "compressibility_per_pa": res["xt"]}
+    return report
+
+
+def xrism_cpu_seconds(name="nacl02_298"):
+    """One 1D solve of `name` by the CPU oracle on all host cores."""
+    import synthetic as S
+    cores = os.cpu_count() or 1
+    code = r"""
+import sys, time, json
+sys.path.insert(0, %r); sys.path.insert(0, %r)
+import oracle as O, synthetic as S
+atoms = [dict(name=a["name"], spc=a["species"], sym=a["sym"], sig=a["sigma"], eps=a["epsilon"],
+              q=a["charge"], xyz=a["xyz"], den=a["density"]) for a in S.BASELINE_SOLVENTS[%r]()]
+t0 = time.perf_counter()
+xvv, info = O.xrism_solve(atoms, 298.15, 8192, 0.05)
+print(json.dumps({"s": time.perf_counter() - t0, "steps": info["steps"]}))
+"""
+    src = code % (os.path.join(ROOT, "oracle"), PKG, name)
+    out = subprocess.run([sys.executable, "-c", src], capture_output=True, text=True,
+                         timeout=600, env=dict(os.environ, OMP_NUM_THREADS=str(cores)))
+    if out.returncode:
+        return None
+    r = json.loads(out.stdout.strip().splitlines()[-1])
+    return {"solve_s": r["s"], "evaluations": r["steps"], "cores": cores, "kind": "port",
+            "solvent": name}
+
+
+def _solvents(d):
+    """Copies this run's solvent tables into d."""
+    for f in set(SOLV.values()):
+        shutil.copyfile(os.path.join(_SOLVENT_DIR, f), os.path.join(d, f))
+
+
 def make_deck(d, atoms=None, grid=256):
     """The 256^3 deck (default), or for profiling a smaller grid at the same
     0.5 A spacing and/or the first `atoms` atoms of the same globule."""
     import synthetic
-    with gzip.open(os.path.join(ROOT, "tests", "golden", "naclaq_vv.xvk.gz"), "rb") as fi, \
-            open(os.path.join(d, "naclaq_vv.xvk"), "wb") as fo:
-        shutil.copyfileobj(fi, fo)
+    _solvents(d)
+    xvk = os.path.join(d, SOLV["nacl02"])
     if atoms is None and grid == 256:
-        return synthetic.config("c2", d), os.path.join(d, "naclaq_vv.xvk")
+        return synthetic.config("c2", d, solvent=SOLV["nacl02"]), xvk
     sol = synthetic.make_solute(2000, synthetic.SEEDS["c2"])
     sub = {k: v[:atoms or 2000] for k, v in sol.items()}
     p = synthetic.write_inp(os.path.join(d, "c2_sub.inp"), sub, (grid * 0.5,) * 3, (grid,) * 3,
-                            "naclaq_vv.xvk")
-    return p, os.path.join(d, "naclaq_vv.xvk")
+                            SOLV["nacl02"])
+    return p, xvk
 
 
 # --------------------------------------------------------------- CPU oracle
@@ -187,13 +278,15 @@ def run_gpu(args, rank, world, local):
         return float(t.item())
 
     prec = args.precision
+    xrism = prepare_solvents(args.solvent, device=local)
     tmp = tempfile.mkdtemp(prefix=f"r3dbench{rank}_")
     c3 = args.config == "c3"
     custom = (args.grid != 256 or args.atoms != 2000) and not c3
     if c3:  # the large single solve: 512^3, 12,877 atoms, history-10 Anderson
         import synthetic
         _solvents(tmp)
-        inp, xvk = synthetic.config("c3", tmp), os.path.join(tmp, "naclaq_vv.xvk")
+        inp = synthetic.config("c3", tmp, solvent=SOLV["nacl02"])
+        xvk = os.path.join(tmp, SOLV["nacl02"])
     else:
         inp, xvk = make_deck(tmp, atoms=args.atoms if custom else None, grid=args.grid)
 
@@ -298,6 +391,14 @@ def run_gpu(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu and not custom and not c3:
         rate, cores, sample = cpu_oracle_rate(CPU_SAMPLE_ITERS, 1)
         cpu = {"value": rate, "unit": "iter/s", "cores": cores, "kind": "port", "sample": sample}
+        if xrism:
+            xrism["cpu_baseline"] = xrism_cpu_seconds()
+    if xrism:
+        xrism = {"workload": "1D XRISM-KH solves making this run's solvent tables (8192 points "
+                             "at 0.05 A, 298.15 K, RMS 1e-10, DIIS 20 / 0.3, 5-stage charge "
+                             "ladder); device time, and end to end through r3d_xrism_solve "
+                             "(host atoms in, host table out; warm)",
+                 **xrism}
 
     if rank == 0:
         line = {
@@ -305,8 +406,8 @@ def run_gpu(args, rank, world, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_iter,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 grids+transforms, f64 state/reductions" if prec == "mixed" else "f64",
-            "data": "synthetic (seeded %s-atom globule; shipped 0.2 M NaCl .xvk)"
-                    % ("12,877" if c3 else "2000"),
+            "data": "synthetic (seeded %s-atom globule; %s)"
+                    % ("12,877" if c3 else "2000", SOLVENT_DATA[args.solvent]),
             "config": {"workload": WORKLOAD_C3 if c3 else WORKLOAD if not custom else
                        f"PROFILING CASE (not the headline): {args.grid}^3 grid, "
                        f"{args.atoms} atoms, NaCl water, KH, AN2",
@@ -336,11 +437,13 @@ def run_gpu(args, rank, world, local):
             "fp64": fp64,
             "batched_screen": batch,
             "served": serve,
+            "xrism_solvents": xrism,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     shutil.rmtree(tmp, ignore_errors=True)
+    shutil.rmtree(_SOLVENT_DIR, ignore_errors=True)
     if dist:
         dist.destroy_process_group()
 
@@ -353,13 +456,6 @@ def _sfe_kcal(path):
     return None
 
 
-def _solvents(d):
-    for name in ("h2o_vv", "naclaq_vv"):
-        with gzip.open(os.path.join(ROOT, "tests", "golden", name + ".xvk.gz"), "rb") as fi, \
-                open(os.path.join(d, name + ".xvk"), "wb") as fo:
-            shutil.copyfileobj(fi, fo)
-
-
 def run_batch_screen(local):
     """64 seeded drug-like solutes (8-60 atoms) on 48^3-128^3 grids, water,
     PSE-3 reached as KH -> PSE-2 -> PSE-3: mixed precision through one batch
@@ -369,7 +465,7 @@ def run_batch_screen(local):
     import synthetic as S
     d = tempfile.mkdtemp(prefix="r3dc4_")
     _solvents(d)
-    decks = S.c4_decks(d)
+    decks = S.c4_decks(d, solvent=SOLV["water"])
     ladder = [(R.KH, 1), (R.PSE, 2), (R.PSE, 3)]
     # mixed, batched
     t0 = time.perf_counter()
@@ -464,14 +560,14 @@ def run_batch_screen(local):
 
 def run_served(local, rates=(10.0, 30.0, 100.0), count=48):
     """The served stream: Poisson arrivals of seeded solutes (8-500 atoms,
-    64^3-192^3 grids, water or 0.2 M NaCl, KH or PSE-2) into one server
+    64^3-192^3 grids, water or 0.1 M NaCl, KH or PSE-2) into one server
     (r3d_server_*: continuous batching); latency = finish - submit."""
     import numpy as np
     import rism3d as R
     import synthetic as S
     d = tempfile.mkdtemp(prefix="r3dc5_")
     _solvents(d)
-    reqs = S.c5_requests(d, count)
+    reqs = S.c5_requests(d, count, solvents=(SOLV["water"], SOLV["nacl01"]))
 
     def stream(srv, rate, seed):
         gaps = np.random.default_rng(seed).exponential(1.0 / rate, len(reqs))
@@ -533,7 +629,8 @@ def run_served(local, rates=(10.0, 30.0, 100.0), count=48):
         grids[g] = grids.get(g, 0) + 1
     shutil.rmtree(d, ignore_errors=True)
     return {"workload": f"{count} seeded requests per rate: 8-500 atoms (log-uniform), "
-                        "water or 0.2 M NaCl, KH or PSE-2 (via KH), AN2, RMS 1e-6",
+                        "water or 0.1 M NaCl (the shipped 0.2 M table with --solvent shipped), KH or "
+                        "PSE-2 (via KH), AN2, RMS 1e-6",
             "grids": grids, "mixed": lines["mixed"], "fp64": lines["fp64"],
             "sfe_err_kcal": {"max": err[-1] if err else None,
                              "p50": err[len(err) // 2] if err else None, "n": len(err)}}
@@ -543,6 +640,7 @@ def run_served(local, rates=(10.0, 30.0, 100.0), count=48):
 def run_reference(args, rank, world):
     if rank != 0:
         return
+    prepare_solvents(args.solvent)
     k = max(1, min(args.steps, CPU_SAMPLE_ITERS))
     w = max(0, min(args.warmup, 1))
     rate, cores, sample = cpu_oracle_rate(k, w)
@@ -550,7 +648,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": rate * 1.0, "unit": "iter/s",
         "n_gpus": world, "steps": k, "warmup": w, "ms_per_step": 1e3 / rate,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded 2000-atom globule; shipped 0.2 M NaCl .xvk)",
+        "data": "synthetic (seeded 2000-atom globule; %s)" % SOLVENT_DATA[args.solvent],
         "config": {"workload": WORKLOAD, "precision": "fp64", "grid": 256, "sites": 4,
                    "atoms": 2000},
         "e2e": {"value": rate, "unit": "iter/s", "h2d_bytes_per_step": 0,
@@ -580,6 +678,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
+    ap.add_argument("--solvent", choices=["baseline", "shipped"], default="baseline",
+                    help="solvent tables: made by the 1D XRISM solve, or the shipped ones")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

@@ -251,3 +251,24 @@ def xrism_solve(atoms, temper, ntab, dr, closure=CLOS_KH, pse_n=1, tol=1e-10,
         raise OracleError("orc_xrism_solve: bad input (%d)" % rc)
     return xvv, dict(xt=info[0], rms=info[1], steps=int(info[2]),
                      status=STATUS[int(info[3])])
+
+
+def write_xvk(path, atoms, temper, ntab, dr, xvv, xt):
+    """The .xvk layout of solvent_read.cc:31-58 (one table row per line);
+    atoms as read_xvk()["atoms"] (name, spc, sym, sig, eps, q, xyz, den)."""
+    natv = xvv.shape[1]
+    nspec = len({a["spc"] for a in atoms})
+    with open(path, "w") as fh:
+        fh.write("##  reduced xvv(k) data with solvent parameters\n")
+        fh.write("## %9d %7d %7d %15.8f %15.8f\n" % (len(atoms), natv, ntab, dr,
+                                                   np.pi / (ntab * dr)))
+        fh.write("## %4d %16.8f %16.8E\n" % (nspec, temper, xt))
+        fh.write("## ATOM SPC SYM sig[Angs]   eps[J/mol]  charge[e]    ---X---     ---Y---"
+                 "     ---Z---    density[M]\n")
+        for a in atoms:
+            fh.write("## %-6s %3d %3d %12.8f %14.8f %12.8f %12.8f %12.8f %12.8f %14.8f\n"
+                     % (a.get("name", "X"), a["spc"], a["sym"], a["sig"], a["eps"], a["q"],
+                        a["xyz"][0], a["xyz"][1], a["xyz"][2], a["den"]))
+        fh.write("##\n")
+        for row in xvv.reshape(ntab, natv * natv):
+            fh.write("".join(" %23.16E" % v for v in row) + "\n")

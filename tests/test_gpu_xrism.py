@@ -6,6 +6,8 @@ Tolerances: GPU vs oracle 2e-8 absolute on xvv and 1e-7 relative on the
 compressibility (both stop at RMS 1e-10 from different summation orders);
 GPU vs the shipped tables 5e-7 (the tables' own residual, as for the
 oracle in test_xrism.py)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -98,3 +100,25 @@ def test_gpu_table_feeds_the_3d_solve(R, solvents, refcase, tmp_path):
     # 3e-7 table differences move mu_ex (kcal/mol per site) by far less than
     # the 1e-6 kcal/mol of the FP64 parity bar
     assert np.abs(out[0] - out[1]).max() < 1e-5, (out[0], out[1])
+
+
+@pytest.mark.parametrize("name", ["water_298", "nacl01_298", "nacl02_298"])
+def test_gpu_baseline_solvents(R, name, tmp_path):
+    """The configurations' solvents (298.15 K water, 0.1 / 0.2 M NaCl with
+    their ion LJ): GPU against the oracle, and the written table drives a 3D
+    solve of a small deck to convergence."""
+    import synthetic
+    atoms = synthetic.BASELINE_SOLVENTS[name]()
+    oatoms = [dict(spc=a["species"], sym=a["sym"], sig=a["sigma"], eps=a["epsilon"],
+                   q=a["charge"], xyz=a["xyz"], den=a["density"]) for a in atoms]
+    path, res = synthetic.make_solvent(name, str(tmp_path))
+    oxvv, oinfo = oracle.xrism_solve(oatoms, 298.15, 8192, 0.05)
+    assert oinfo["status"] == res["status"] == "converged"
+    tab = oracle.read_xvk(path)["xvv"]
+    assert np.abs(tab - oxvv).max() < GPU_ORACLE_TOL
+    assert abs(res["xt"] / oinfo["xt"] - 1) < GPU_ORACLE_XT
+    inp = synthetic.small(str(tmp_path), nu=10, grid=32, box=16.0, solvent=os.path.basename(path),
+                          name="deck_" + name)
+    s = R.RISM3D(precision="fp64")
+    s.initialize(inp, xvk=path)
+    assert s.iterate()[2] == "converged"

@@ -147,3 +147,31 @@ def test_solve_rejects_bad_input_without_gpu(R):
         R.XRISM(bad).solve()
     with pytest.raises(R.R3DError):
         R.XRISM([dict(water[0], sym=2)]).solve()  # class 1 has no atom
+
+
+def test_oracle_makes_configuration_water(R):
+    """The configurations' 298.15 K water converges in the oracle (the
+    reference ships only 300 K water)."""
+    import synthetic
+    atoms = [dict(spc=a["species"], sym=a["sym"], sig=a["sigma"], eps=a["epsilon"], q=a["charge"],
+                  xyz=a["xyz"], den=a["density"]) for a in synthetic.water_atoms()]
+    xvv, info = oracle.xrism_solve(atoms, 298.15, 8192, 0.05)
+    assert info["status"] == "converged"
+    # compressibility of this water model near 4.8e-10 / Pa, chi(k -> 0) =
+    # rho kT kappa_T for the O-O entry
+    assert 4.5e-10 < info["xt"] < 5.1e-10
+    rho = synthetic.WATER_M * synthetic.AVOGADRO * 1e-27 * 1e30
+    assert abs(xvv[0, 0, 0] / (rho * 1.380649e-23 * 298.15 * info["xt"]) - 1) < 1e-3
+
+
+def test_oracle_writer_matches_library_writer(R, solvents, tmp_path):
+    """The reference arm writes its tables with oracle.write_xvk; the file
+    is the library writer's, byte for byte."""
+    d = oracle.read_xvk(solvents["naclaq_vv"])
+    x = R.XRISM.from_deck(solvents["naclaq_vv"])
+    x.table = d["xvv"].copy()
+    x.result = dict(xt=d["xt"])
+    a, b = str(tmp_path / "lib.xvk"), str(tmp_path / "orc.xvk")
+    x.write_xvk(a)
+    oracle.write_xvk(b, d["atoms"], d["temper"], d["ntab"], d["dr"], d["xvv"], d["xt"])
+    assert open(a).read() == open(b).read()
