@@ -91,6 +91,7 @@ void launch_atom_integrals(const IntAtoms &, const double *, long long, const in
                            const double *, double *, int, double *, cudaStream_t);
 template <typename P>
 void launch_mix_an2(Batch, int, cudaStream_t);
+void launch_t_restore(const void *t, const void *dslot, void *out, long long niv, cudaStream_t s);
 template <typename P>
 void launch_anm(Batch, int, const Desc *, const int *, int, cudaStream_t, int);
 template <typename P>
@@ -211,6 +212,7 @@ struct r3d_ctx {
   void *tw64 = nullptr, *tw32 = nullptr;  // compile-time engine twiddles
   uint32_t *kidx = nullptr;
   double *partials = nullptr, *scratch = nullptr;
+  void *tbuf = nullptr;  // mixed AN2: rebuilt t of the last evaluation (maxstep)
   int npart = 0;  // rows of partials
   size_t scratch_bytes = 0;
   Ctl *ctl = nullptr;
@@ -1123,7 +1125,8 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   // AN2: hist_a = t slots (T), hist_b = residual slots (R);
   // ANM: hist_a = residual ring (R), hist_b = z ring (T)
   const size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
-  const size_t ha = c->mixer == MIX_AN2 ? sizeof(T) : sizeof(R);
+  // (mixed AN2: the t slots hold FP32 differences of successive t)
+  const size_t ha = c->mixer == MIX_AN2 ? (c->fp64 ? sizeof(T) : sizeof(R)) : sizeof(R);
   const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
   if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
   if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
@@ -1545,7 +1548,9 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
     timed("reduce", (double)iter_ix_ctas(c->geo) * kPartials * 8,
           [&] { launch_reduce(c->ddesc, ixc, 1, 1, s); });
     const bool picard = h.count_left > 0;
-    timed("mix_an2", picard ? n * N * (3 * ts + 2 * rs) : n * N * (5 * ts + 4 * rs),
+    const bool diffs = rs < ts;  // mixed: FP32 t differences in the slots
+    timed("mix_an2", picard ? n * N * (diffs ? 2 * ts + 3 * rs : 3 * ts + 2 * rs)
+                            : n * N * (diffs ? 2 * ts + 7 * rs : 5 * ts + 4 * rs),
           [&] { launch_mix_an2<P>(bmx, c->geo.mix_ctas, s); });
   } else {
     timed("anm_dots", n * N * rs * (h.hcount + 1),
@@ -1686,13 +1691,26 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
 // ------------------------------------------------------------ read-back
 // Grid of t that produced the last residual: t itself, unless the last step
 // also mixed (maxstep reached), in which case AN2 left the old t in its
-// history slot (anderson_cuda.cu:11-22).
-static const void *t_of_residual(r3d_ctx *c, const Ctl &h) {
+// history slot (anderson_cuda.cu:11-22) -- in the mixed path as the FP32
+// difference to the new t, so the old t is rebuilt into a buffer of its own.
+static int t_of_residual(r3d_ctx *c, const Ctl &h, const void **out) {
+  *out = c->t;
   if (h.status == MAXSTEP && h.mix_flag && c->mixer == MIX_AN2) {
-    size_t off = (size_t)h.coef[3] * c->desc.n * c->desc.Ns * sizeof(double);
-    return (const char *)c->hist_a + off;
+    const long long niv = (long long)c->desc.n * c->desc.Ns;
+    if (c->fp64) {
+      *out = (const char *)c->hist_a + (size_t)h.coef[3] * niv * sizeof(double);
+      return R3D_OK;
+    }
+    if (!c->tbuf) {
+      int rc = dalloc(c, &c->tbuf, (size_t)niv * sizeof(double));
+      if (rc) return rc;
+    }
+    launch_t_restore(c->t, (const char *)c->hist_a + (size_t)h.coef[3] * niv * sizeof(float),
+                     c->tbuf, niv, c->stream);
+    CK(cudaGetLastError());
+    *out = c->tbuf;
   }
-  return c->t;
+  return R3D_OK;
 }
 
 static int ensure_scratch(r3d_ctx *c, size_t bytes) {
@@ -1721,7 +1739,8 @@ extern "C" int r3d_thermo(r3d_ctx *c, double *xmu, double *xmu2, double *pmv,
   if (rc) return rc;
   Ctl h;
   if ((rc = read_ctl(c, h))) return rc;
-  const void *tg = t_of_residual(c, h);
+  const void *tg = nullptr;
+  if ((rc = t_of_residual(c, h, &tg))) return rc;
   if (c->fp64)
     launch_thermo<P64>(d, tg, c->scratch, ctas, c->stream);
   else
@@ -1811,7 +1830,8 @@ extern "C" int r3d_get_grid(r3d_ctx *c, int which, double *host) {
     case R3D_GRID_G: case R3D_GRID_H: {
       count = niv;
       if ((rc = ensure_scratch(c, count * 8))) return rc;
-      const void *tg = t_of_residual(c, h);
+      const void *tg = nullptr;
+  if ((rc = t_of_residual(c, h, &tg))) return rc;
       double *g = which == R3D_GRID_G ? c->scratch : nullptr;
       double *hh = which == R3D_GRID_H ? c->scratch : nullptr;
       if (c->fp64)
@@ -1939,7 +1959,8 @@ extern "C" int r3d_atom_integrals(r3d_ctx *c, double *grad, double *euv, double 
   int rc = read_ctl(c, h);
   if (rc) return rc;
   if ((rc = ensure_scratch(c, niv * 8))) return rc;  // g, FP64
-  const void *tg = t_of_residual(c, h);
+  const void *tg = nullptr;
+  if ((rc = t_of_residual(c, h, &tg))) return rc;
   if (c->fp64)
     launch_gh<P64>(d, tg, c->scratch, nullptr, s);
   else

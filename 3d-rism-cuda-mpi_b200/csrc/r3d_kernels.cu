@@ -538,13 +538,73 @@ __global__ void __launch_bounds__(kThreads)
   const long long i0 = (long long)(blockIdx.x - b.prefix[si]) * kMixChunk + threadIdx.x;
   T *__restrict__ t = (T *)d.t;
   const R *__restrict__ r = (const R *)d.res;
-  T *__restrict__ tp = (T *)d.hist_a;
   R *__restrict__ rp = (R *)d.hist_b;
   const bool picard = c->coef[2] < 0;
   const long long boff = (long long)c->coef[3] * niv;
   const double s1 = c->coef[0], s2 = c->coef[1], m = d.m;
   T tv[kMixPer];
   R rv[kMixPer];
+  if constexpr (sizeof(R) < sizeof(T)) {
+    // Mixed precision: the t slots hold FP32 differences of successive
+    // states, D_k = t_k - t_{k+1}, written when t_{k+1} is made.  At step k
+    // the newest slot (1 - binary) holds t_{k-1} - t_k and the other
+    // t_{k-2} - t_{k-1}; the mix needs only t_slot - t_k, which is D_new and
+    // D_old + D_new.  Slot traffic halves against FP64 copies of t.
+    R *__restrict__ dd = (R *)d.hist_a;
+    const long long noff = (long long)(1 - (int)c->coef[3]) * niv;
+    if (picard) {  // t_{k+1} = t_k + R_k: D_k = -R_k
+#pragma unroll
+      for (int k = 0; k < kMixPer; ++k) {
+        const long long i = i0 + k * kThreads;
+        if (i < niv) {
+          tv[k] = t[i];
+          rv[k] = r[i];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kMixPer; ++k) {
+        const long long i = i0 + k * kThreads;
+        if (i < niv) {
+          dd[boff + i] = -rv[k];
+          rp[boff + i] = rv[k];
+          t[i] = tv[k] + (T)rv[k];
+        }
+      }
+      return;
+    }
+    R dn[kMixPer], dl[kMixPer], b0[kMixPer], b1[kMixPer];
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) {
+        tv[k] = t[i];
+        rv[k] = r[i];
+        dn[k] = dd[noff + i];
+        dl[k] = dd[boff + i];
+        b0[k] = rp[i];
+        b1[k] = rp[i + niv];
+      }
+    }
+    const bool old0 = boff == 0;  // slot 0 holds the older entry
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) {
+        const double tt = tv[k], rr = rv[k];
+        const double dnew = dn[k], dold = (double)dl[k] + dnew;
+        const double e0 = old0 ? dold : dnew, e1 = old0 ? dnew : dold;  // t_slot - t_k
+        const double rp0 = b0[k], rp1 = b1[k];
+        const double uu = tt + s1 * e0 + s2 * e1;
+        const double vv = tt + rr + s1 * (e0 + rp0 - rr) + s2 * (e1 + rp1 - rr);
+        const double tn = uu + m * (vv - uu);
+        dd[boff + i] = (R)(tt - tn);
+        rp[boff + i] = rv[k];
+        t[i] = (T)tn;
+      }
+    }
+    return;
+  }
+  T *__restrict__ tp = (T *)d.hist_a;
   if (picard) {
 #pragma unroll
     for (int k = 0; k < kMixPer; ++k) {
@@ -1412,6 +1472,17 @@ void launch_ctl_gather(const Desc *d, int ns, double *out, cudaStream_t s) {
 template <typename P>
 void launch_mix_an2(Batch b, int grid, cudaStream_t s) {
   k_mix_an2<P><<<grid, kThreads, 0, s>>>(b);
+}
+// Mixed AN2: the t of the last evaluation when the last step also mixed
+// (maxstep): t_k = t_{k+1} + D_k, D_k in slot `slot` of the t differences.
+__global__ void k_t_restore(const double *t, const float *dslot, double *out, long long niv) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < niv) out[i] = t[i] + (double)dslot[i];
+}
+void launch_t_restore(const void *t, const void *dslot, void *out, long long niv,
+                      cudaStream_t s) {
+  k_t_restore<<<(unsigned)((niv + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+      (const double *)t, (const float *)dslot, (double *)out, niv);
 }
 template <typename P>
 void launch_anm(Batch b, int grid, const Desc *d, const int *ctas, int ns,

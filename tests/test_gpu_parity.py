@@ -130,3 +130,21 @@ def test_mixed_precision_within_tolerance(R, refcase, case, tmp_path):
     # first number is SFE_SC (total), PMV is the third-to-last
     assert abs(got[0] - ref[0]) <= 0.01 * KCAL
     assert abs(got[-3] - ref[-3]) <= 0.1 * A3_PER_LMOL
+
+
+def test_mixed_maxstep_results_are_of_the_last_evaluation(R, refcase):
+    """A solve stopped by maxstep mixes at its last step too, so its results
+    (g, thermo) belong to the t before that mix.  The mixed path keeps the AN2
+    history as FP32 differences of successive t and rebuilds that t; the FP64
+    path keeps it whole.  After a few steps both paths agree to FP32 rounding,
+    while the t after the mix would be a whole mixing step away."""
+    inp, xvk = refcase("s64kh")
+    g = {}
+    for prec in ("fp64", "mixed"):
+        s = _solver(R, inp, xvk, prec=prec)
+        s.set_control(convergence=1e-300, maxstep=6)
+        steps, rms, status = s.iterate()
+        assert status == "maxstep" and steps == 6
+        g[prec] = s.get("g")
+        s.close()
+    assert np.abs(g["mixed"] - g["fp64"]).max() < 1e-4 * max(1.0, np.abs(g["fp64"]).max())
