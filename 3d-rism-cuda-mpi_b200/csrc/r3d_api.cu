@@ -200,7 +200,7 @@ struct r3d_ctx {
   std::vector<void *> allocs;
   size_t bytes = 0;
   void *u = nullptr, *t = nullptr, *fr = nullptr, *res = nullptr, *w = nullptr,
-       *fk = nullptr, *chi = nullptr, *lr = nullptr, *hist_a = nullptr,
+       *fk = nullptr, *chi = nullptr, *lr = nullptr, *gq = nullptr, *hist_a = nullptr,
        *hist_b = nullptr, *cref = nullptr, *chi64 = nullptr;
   double next_refresh = 0;  // mixed path: refresh when rms drops below this
   // mixed path: the refresh's FP64 geometry and work buffer, kept from the
@@ -953,7 +953,7 @@ static int refresh(r3d_ctx *c, bool zero) {
 static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   const size_t R = c->rsz, T = 8, N = (size_t)d.N, n = (size_t)d.n;
   size_t b = 0;
-  b += 3 * n * N * R + n * N * T;  // u, res, lr (grid type), t (state type)
+  b += 3 * n * N * R + 2 * n * N * T;  // u, res, lr (grid type), t, gq (state type)
   b += n * N * R;                  // w (n half spectra)
   b += N * R + N * 8;              // fr, fk (FP64 half spectrum)
   if (!c->fp64) b += n * N * R + (size_t)nshell * n * n * 8;  // cref, chi64
@@ -961,7 +961,8 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   b += (size_t)d.Nh * 4;           // kidx
   b += (size_t)nshell * n * n * R;
   size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
-  b += slots * n * N * (R + T);    // mixer history (residuals, states)
+  // mixer history (residuals, states; mixed AN2: FP32 state differences)
+  b += slots * n * N * (R + (c->mixer == MIX_AN2 && !c->fp64 ? R : T));
   b += (size_t)std::max(max_ix_ctas(c->geo), c->geo.dot_ctas) * kPartials * 8;
   b += (size_t)(c->prob.maxstep + 1) * 8 + sizeof(Ctl) + sizeof(Desc) + 4096;
   return b;
@@ -973,8 +974,8 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
 // inputs the bulk copy engine stages (k_fx_bulk / k_ix_bulk).  Which is
 // faster depends on the row length, the sites and the precision, so the
 // first solve of each geometry times both on its own buffers -- the mode-1 x
-// passes write only w, the residual and the partials, which every iteration
-// rewrites -- and the choice holds for the process.
+// passes write only w, gq, the residual and the partials, which every
+// iteration rewrites -- and the choice holds for the process.
 static std::mutex g_tune_mu;
 // per geometry: the FX and IX variant (0 one tile per CTA, 1 bulk-staged,
 // 2 warp tiles)
@@ -1116,6 +1117,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = dalloc(c, &c->t, n * N * sizeof(T)))) return rc;
   if ((rc = dalloc(c, &c->res, n * N * sizeof(R)))) return rc;
   if ((rc = dalloc(c, &c->lr, n * N * sizeof(R)))) return rc;
+  if ((rc = dalloc(c, &c->gq, n * N * sizeof(T)))) return rc;
   if ((rc = dalloc(c, &c->w, n * Nh * 2 * sizeof(R)))) return rc;
   if ((rc = dalloc(c, &c->fr, d.N * sizeof(R)))) return rc;
   if ((rc = dalloc(c, &c->fk, d.Nh * sizeof(double2)))) return rc;
@@ -1144,6 +1146,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   CK(cudaMemsetAsync(c->u, 0, n * N * sizeof(R), s));
   CK(cudaMemsetAsync(c->t, 0, n * N * sizeof(T), s));
   CK(cudaMemsetAsync(c->lr, 0, n * N * sizeof(R), s));
+  CK(cudaMemsetAsync(c->gq, 0, n * N * sizeof(T), s));
   CK(cudaMemsetAsync(c->w, 0, n * Nh * 2 * sizeof(R), s));
   CK(cudaMemsetAsync(c->fr, 0, d.N * sizeof(R), s));
   CK(cudaMemsetAsync(c->fk, 0, d.Nh * sizeof(double2), s));
@@ -1173,6 +1176,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   d.fk = nullptr;  // phi_L(k) enters through lr (see refresh)
   d.chi = c->chi;
   d.lr = c->lr;
+  d.gq = c->gq;
   d.cref = c->cref;
   d.kidx = c->kidx;
   d.hist_a = c->hist_a;
@@ -1534,7 +1538,8 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
     return R3D_OK;
   };
   const double cref = d.cref ? rs : 0.0;
-  timed("fwd_x", n * N * (ts + rs + cref + rs),
+  // FX: t, u, c_ref in; w (half spectrum: one grid value per voxel) and g out
+  timed("fwd_x", n * N * (ts + rs + cref + rs + ts),
         [&] { pass_fx<P>(d, c->geo, bx, s, 1, nullptr); });
   timed("fft_y_fwd", n * N * 2 * rs,
         [&] { pass_fy_iter<P>(d, c->geo, by, s, -1); });
@@ -1542,7 +1547,8 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
         [&] { pass_zoz_iter<P>(d, c->geo, bz, s); });
   timed("fft_y_inv", n * N * 2 * rs,
         [&] { pass_fy_iter<P>(d, c->geo, by, s, 1); });
-  timed("inv_x", n * N * (rs + ts + rs + rs + rs + (dots ? 2 * rs : 0)),
+  // IX: w, g, lr (and the two AN2 residual slots) in; R out
+  timed("inv_x", n * N * (rs + ts + rs + rs + (dots ? 2 * rs : 0)),
         [&] { pass_ix<P>(d, c->geo, bix, s, 1, nullptr); });
   if (c->mixer == MIX_AN2) {
     timed("reduce", (double)iter_ix_ctas(c->geo) * kPartials * 8,

@@ -148,6 +148,12 @@ struct Desc {
   // fk = beta phi_L(k) in transform units (FP64; subtracted in the OZ step
   // only when non-null, i.e. in the refresh pipeline)
   void *u, *t, *fr, *res, *w, *fk, *chi, *lr, *cref;
+  // gq: g = closure(-u + t) as the iteration's FX evaluated it (state type,
+  // FP64), left for the IX of the same evaluation, which reads it instead of
+  // t and u and evaluates no closure.  (Stored in FP32, as g - 1, it added
+  // enough noise to R near convergence to cost the mixed path 14 % more
+  // iterations at 256^3.)
+  void *gq;
   const uint32_t *kidx;  // [z][y][p] shell index of each half-spectrum point
   // AN2: tp, rp [2][n][N]; ANM: fring, zring [H+1][n][N] (res aliases a slot)
   void *hist_a, *hist_b;

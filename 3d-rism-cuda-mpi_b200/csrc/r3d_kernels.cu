@@ -86,6 +86,8 @@ __global__ void __launch_bounds__(kThreads)
       double t0 = t[base + m], t1 = t[base + m + hx];
       double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
       double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + hx] + t1);
+      ((T *)d.gq)[base + m] = g0;
+      ((T *)d.gq)[base + m + hx] = g1;
       double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
       if (cref) {
         c0 -= (double)cref[base + m];
@@ -300,8 +302,8 @@ __global__ void __launch_bounds__(kThreads)
   for (int k = 0; k < d.nrad_x; ++k) pl.rad[k] = d.rad_x[k];
 
   const bool dots = MODE == 1 && d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
-  const T *t = (const T *)d.t;
-  const R *u = (const R *)d.u, *lr = (const R *)d.lr;
+  const T *gq = (const T *)d.gq;
+  const R *lr = (const R *)d.lr;
   R *res = (R *)d.res;
   const R *rp = (const R *)d.hist_b;
   const long long niv = (long long)n * d.Ns;
@@ -341,9 +343,7 @@ __global__ void __launch_bounds__(kThreads)
           dst[base + m] = h0;
           dst[base + m + hx] = h1;
         } else {
-          double t0 = t[base + m], t1 = t[base + m + hx];
-          double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
-          double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + hx] + t1);
+          const double g0 = gq[base + m], g1 = gq[base + m + hx];
           // tr: R = h + 1 - g with h = h_s - L, evaluated in FP64 and rounded
           // once (R is small near convergence, g need not be)
           R r0 = (R)((double)h0 + (double)lr[base + m] - g0);

@@ -61,6 +61,8 @@ __global__ void __launch_bounds__(kThreads)
       const double t0 = t[base + m], t1 = t[base + m + L];
       const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
       const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + L] + t1);
+      ((T *)d.gq)[base + m] = g0;
+      ((T *)d.gq)[base + m + L] = g1;
       double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
       if (cref) {
         c0 -= (double)cref[base + m];
@@ -336,8 +338,8 @@ __global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
   const int ntile = d.n * tps;
   const bool dots = MODE == 1 && d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
   const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
-  const T *t = (const T *)d.t;
-  const R *u = (const R *)d.u, *lr = (const R *)d.lr;
+  const T *gq = (const T *)d.gq;
+  const R *lr = (const R *)d.lr;
   R *res = (R *)d.res;
   const R *rp = (const R *)d.hist_b;
   const long long niv = (long long)d.n * d.Ns;
@@ -393,9 +395,7 @@ __global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
         dst[base + m] = h0;
         dst[base + m + L] = h1;
       } else {
-        const double t0 = t[base + m], t1 = t[base + m + L];
-        const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m] + t0);
-        const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)u[base + m + L] + t1);
+        const double g0 = gq[base + m], g1 = gq[base + m + L];
         const R r0 = (R)((double)h0 + (double)lr[base + m] - g0);
         const R r1 = (R)((double)h1 + (double)lr[base + m + L] - g1);
         res[base + m] = r0;
@@ -425,15 +425,14 @@ __global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
 // ------------------------------------------------- IX with bulk staging
 // The iteration's IX (MODE 1) with the per-voxel inputs staged by the bulk
 // copy engine: a tile's PC rows of one site are one contiguous block in each
-// of t, u, lr and the two AN2 residual slots, so one cp.async.bulk per array
+// of gq, lr and the two AN2 residual slots, so one cp.async.bulk per array
 // brings the next tile into shared memory while the current one is being
 // transformed and reduced (two stages, one mbarrier each).
 template <typename P, int L, int PC>
 struct IxStage {  // byte layout of one stage of staged inputs
   static constexpr int NX = 2 * L;
-  static constexpr size_t t = 0;
-  static constexpr size_t u = t + (size_t)PC * NX * sizeof(typename P::T);
-  static constexpr size_t lr = u + (size_t)PC * NX * sizeof(typename P::R);
+  static constexpr size_t gq = 0;
+  static constexpr size_t lr = gq + (size_t)PC * NX * sizeof(typename P::T);
   static constexpr size_t r0 = lr + (size_t)PC * NX * sizeof(typename P::R);
   static constexpr size_t r1 = r0 + (size_t)PC * NX * sizeof(typename P::R);
   static constexpr size_t w = r1 + (size_t)PC * NX * sizeof(typename P::R);  // spectrum rows
@@ -442,7 +441,7 @@ struct IxStage {  // byte layout of one stage of staged inputs
 #if R3D_CT_FP64
 size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz) {
   const size_t buf = ((csz * (size_t)L * (PC + 1) + 127) / 128) * 128;
-  const size_t stage = (size_t)PC * 2 * L * (tsz + 4 * rsz) + (size_t)PC * L * csz;
+  const size_t stage = (size_t)PC * 2 * L * (tsz + 3 * rsz) + (size_t)PC * L * csz;
   return buf + 2 * stage;
 }
 #endif
@@ -479,7 +478,7 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
   const long long niv = (long long)d.n * d.Ns;
   const uint32_t tbytes = PC * NX * sizeof(T), rbytes = PC * NX * sizeof(R);
   const uint32_t wbytes = PC * L * sizeof(C);
-  const uint32_t stage_tx = tbytes + 2 * rbytes + wbytes + (dots ? 2 * rbytes : 0);
+  const uint32_t stage_tx = tbytes + rbytes + wbytes + (dots ? 2 * rbytes : 0);
   const Desc *dp = &d;
   char *const stages = smem + BUF;
   uint64_t *const bars = bar;
@@ -492,8 +491,7 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
     uint64_t *br = bars + st;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(br, stage_tx);
-    bulk_g2s(sb + St::t, (const T *)dp->t + base, tbytes, br);
-    bulk_g2s(sb + St::u, (const R *)dp->u + base, rbytes, br);
+    bulk_g2s(sb + St::gq, (const T *)dp->gq + base, tbytes, br);
     bulk_g2s(sb + St::lr, (const R *)dp->lr + base, rbytes, br);
     bulk_g2s(sb + St::w,
              (const C *)dp->w + (long long)v * dp->Nhs + (long long)(tile % tps) * PC * L,
@@ -554,8 +552,8 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
     }
     __syncthreads();
     ct_fft_dif<L, PC, LD, 1>(buf, tw);
-    const T *ts = (const T *)(sb + St::t);
-    const R *us = (const R *)(sb + St::u), *ls = (const R *)(sb + St::lr);
+    const T *gs = (const T *)(sb + St::gq);
+    const R *ls = (const R *)(sb + St::lr);
     const R *q0s = (const R *)(sb + St::r0), *q1s = (const R *)(sb + St::r1);
     const long long gbase = (long long)v * d.Ns + row0 * NX;
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
@@ -565,9 +563,7 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
       if ((m + par[r]) & 1) h0 = -h0;
       if ((m + L + par[r]) & 1) h1 = -h1;
       const int i0 = r * NX + m, i1 = i0 + L;
-      const double t0 = ts[i0], t1 = ts[i1];
-      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)us[i0] + t0);
-      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)us[i1] + t1);
+      const double g0 = gs[i0], g1 = gs[i1];
       const R r0 = (R)((double)h0 + (double)ls[i0] - g0);
       const R r1 = (R)((double)h1 + (double)ls[i1] - g1);
       res[gbase + i0] = r0;
@@ -698,6 +694,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const char *sb = smem + BUF + st * St::bytes;
     const T *ts = (const T *)(sb + St::t);
     const R *us = (const R *)(sb + St::u), *cs = (const R *)(sb + St::cref);
+    T *gqg = (T *)d.gq + (long long)v * d.Ns + row0 * NX;
 #pragma unroll 4
     for (int e = threadIdx.x; e < PC * L; e += kThreads) {
       const int r = e / L, m = e % L;
@@ -706,6 +703,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       const double t0 = ts[i0], t1 = ts[i1];
       const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)us[i0] + t0);
       const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)us[i1] + t1);
+      gqg[i0] = g0;
+      gqg[i1] = g1;
       double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
       if (has_cref) {
         c0 -= (double)cs[i0];
@@ -776,6 +775,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
     const long long base0 = (long long)v * d.Ns + row0 * NX;
     const T *tt = t + base0;
     const R *ut = u + base0, *ct = cref + (has_cref ? base0 : 0);
+    T *gt = (T *)d.gq + base0;
     const int pr0 = (int)((row0 % ny + row0 / ny) & 1);
     const int y0 = (int)(row0 % ny);
 #pragma unroll 1
@@ -788,6 +788,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
       const double t0 = tt[i0], t1 = tt[i1];
       const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i0] + t0);
       const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i1] + t1);
+      gt[i0] = g0;
+      gt[i1] = g1;
       double c0 = g0 - 1.0 - t0, c1 = g1 - 1.0 - t1;
       if (has_cref) {
         c0 -= (double)ct[i0];
@@ -832,8 +834,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
   const int ny = d.ny, tps = (d.ny * d.nz) / PCW, ntile = d.n * tps;
   const bool dots = d.mixer == MIX_AN2 && d.ctl->count_left <= 0;
   const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
-  const T *t = (const T *)d.t;
-  const R *u = (const R *)d.u, *lr = (const R *)d.lr;
+  const T *gq = (const T *)d.gq;
+  const R *lr = (const R *)d.lr;
   const R *rp = (const R *)d.hist_b;
   R *res = (R *)d.res;
   const long long niv = (long long)d.n * d.Ns;
@@ -872,8 +874,8 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
     __syncwarp();
     ct_fft_dif_warp<L, PCW, LD, 1>(buf, tw, lane);
     const long long base0 = (long long)v * d.Ns + row0 * NX;
-    const T *tt = t + base0;
-    const R *ut = u + base0, *lt = lr + base0, *p0t = rp + base0, *q0t = rp + niv + base0;
+    const T *gt = gq + base0;
+    const R *lt = lr + base0, *p0t = rp + base0, *q0t = rp + niv + base0;
     R *rt = res + base0;
     const int pr0 = (int)((row0 % ny + row0 / ny) & 1);
     const int y0 = (int)(row0 % ny);
@@ -886,9 +888,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
       if ((m + par) & 1) h0 = -h0;
       if ((m + L + par) & 1) h1 = -h1;
       const int i0 = r * NX + m, i1 = i0 + L;
-      const double t0 = tt[i0], t1 = tt[i1];
-      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i0] + t0);
-      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)ut[i1] + t1);
+      const double g0 = gt[i0], g1 = gt[i1];
       const R r0 = (R)((double)h0 + (double)lt[i0] - g0);
       const R r1 = (R)((double)h1 + (double)lt[i1] - g1);
       rt[i0] = r0;
