@@ -60,6 +60,7 @@ constexpr int kXNT = 512;     // threads of the per-pair transform CTAs
 constexpr int kXWide = 256;   // threads of the wide kernels
 constexpr int kXMaxN = 16384;
 constexpr int kXRollbacks = 8;
+constexpr int kXChunk = 1024;  // elements per CTA of xr_dots
 
 namespace phys {  // src-cuda-mpi/physical.h:5-14
 constexpr double avogadro = 6.02214076e23;
@@ -594,76 +595,77 @@ __global__ void __launch_bounds__(kXWide) xr_pack_inv(XP p) {
   pack_pair(p.zi + (size_t)pr * p.M, p.N, j, p.E[j].y, t[j], t[p.N - j]);
 }
 
-// bordered DIIS system [G 1; 1^T 0] c = e_n (order m = n + 1 <= 32) in
-// shared memory by the CTA: partial pivoting on the column, one multiplier
-// per row, the row updates spread over the threads, back substitution by
-// one warp (row r on lane r).  G: the Gram matrix of the n entries (oldest
-// first), stride 33.
-__device__ void diis_solve_block(const double *G, int n, double *coef) {
-  __shared__ double A[kXMaxH + 1][kXMaxH + 2];  // [row][col], col m = rhs
-  __shared__ double mult[kXMaxH + 1];
-  __shared__ int piv_row;
-  __shared__ bool ok;
-  const int m = n + 1, tid = threadIdx.x, nt = blockDim.x;
+// bordered DIIS system [G 1; 1^T 0] c = e_n (order m = n + 1 <= 32) by one
+// warp, without block barriers: row r lives in the registers of lane r
+// (columns unrolled, so every index is static); partial pivoting leaves the
+// rows in place and publishes each column's pivot row to shared memory, one
+// reciprocal per column; the back substitution reads the pivot rows there.
+// G: the Gram matrix of the n entries (oldest first), stride 33.  Called by
+// warp 0 (all 32 lanes).
+__device__ void diis_solve_warp(const double *G, int n, double *coef) {
+  __shared__ double Pv[kXMaxH + 1][33];  // pivot row of each column; [32] = rhs
+  const int lane = threadIdx.x & 31;
+  const int m = n + 1;
   double sc = 0.0;
   for (int i = 0; i < n; ++i) sc = fmax(sc, G[i * 33 + i]);
   sc = sc > 0.0 ? 1.0 / sc : 1.0;
-  for (int e = tid; e < 32 * 33; e += nt) {
-    const int r = e / 33, x = e - r * 33;
-    if (r >= m || x > m) continue;
-    double v;
-    if (x == m) v = r == n ? 1.0 : 0.0;
-    else if (r < n && x < n) v = G[r * 33 + x] * sc;
-    else v = (r < n || x < n) ? 1.0 : 0.0;
-    A[r][x] = v;
-  }
-  if (tid == 0) ok = true;
-  __syncthreads();
-  for (int col = 0; col < m; ++col) {
-    if (tid < 32) {  // pivot: largest |A[r][col]|, r >= col; swap; multipliers
-      const int r = tid;
-      double best = (r >= col && r < m) ? fabs(A[r][col]) : -1.0;
-      int bl = r;
+  double row[32];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
-        if (ob > best || (ob == best && ol < bl)) { best = ob; bl = ol; }
-      }
-      if (!(best > 1e-300)) {
-        if (tid == 0) ok = false;
-      } else {
-        if (bl != col)
-          for (int x = tid; x <= m; x += 32) {
-            const double t = A[col][x];
-            A[col][x] = A[bl][x];
-            A[bl][x] = t;
-          }
-        __syncwarp();
-        if (r > col && r < m) mult[r] = A[r][col] / A[col][col];
-      }
+  for (int x = 0; x < 32; ++x) {
+    double v = 0.0;
+    if (lane < m && x < m) {
+      if (lane < n && x < n) v = G[lane * 33 + x] * sc;
+      else if (lane < n || x < n) v = 1.0;  // the border; the corner is 0
     }
-    __syncthreads();
-    if (!ok) break;
-    for (int e = tid; e < 32 * 33; e += nt) {
-      const int r = e / 33, x = e - r * 33;
-      if (r > col && r < m && x > col && x <= m) A[r][x] -= mult[r] * A[col][x];
+    row[x] = v;
+  }
+  double rhs = lane == n ? 1.0 : 0.0;
+  bool used = lane >= m;  // lanes past the system never pivot
+  bool ok = true;
+#pragma unroll
+  for (int col = 0; col < 32; ++col) {
+    if (col >= m) break;
+    double best = used ? -1.0 : fabs(row[col]);
+    int bl = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+      if (ob > best || (ob == best && ol < bl)) { best = ob; bl = ol; }
     }
-    __syncthreads();
+    if (!(best > 1e-300)) {  // the same in every lane
+      ok = false;
+      break;
+    }
+    if (lane == bl) {
+      used = true;
+#pragma unroll
+      for (int x = 0; x < 32; ++x)
+        if (x >= col) Pv[col][x] = row[x];
+      Pv[col][32] = rhs;
+    }
+    __syncwarp();
+    if (!used) {
+      const double mult = row[col] / Pv[col][col];
+#pragma unroll
+      for (int x = 0; x < 32; ++x)
+        if (x > col) row[x] -= mult * Pv[col][x];
+      rhs -= mult * Pv[col][32];
+    }
   }
-  if (tid < 32) {
-    const int r = tid;
-    double rhs = r < m ? A[r][m] : 0.0, sol = 0.0;
-    bool fin = ok;
-    if (ok)
-      for (int col = m - 1; col >= 0; --col) {
-        const double v = __shfl_sync(0xffffffffu, rhs / (r < m ? A[r][r] : 1.0), col);
-        if (r == col) sol = v;
-        if (r < col) rhs -= A[r][col] * v;
-      }
-    fin = __all_sync(0xffffffffu, fin && (r >= n || isfinite(sol)));
-    if (r < n) coef[r] = fin ? sol : (r == n - 1 ? 1.0 : 0.0);
+  __syncwarp();
+  double sol = 0.0;
+  if (ok) {
+    for (int col = m - 1; col >= 0; --col) {
+      double term = (lane > col && lane < m) ? Pv[col][lane] * sol : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
+      const double v = (Pv[col][32] - term) / Pv[col][col];
+      if (lane == col) sol = v;
+    }
   }
+  const bool fin = __all_sync(0xffffffffu, ok && (lane >= n || isfinite(sol)));
+  if (lane < n) coef[lane] = fin ? sol : (lane == n - 1 ? 1.0 : 0.0);
 }
 
 // f = t_new - t of the evaluation into the ring, <f, f_n> against the ring
@@ -678,7 +680,6 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
   __shared__ int s_head, s_nn, s_stage, s_stage_steps, s_rollbacks;
   __shared__ double s_best, s_eta;
   __shared__ int slot[kXMaxH];
-  __shared__ double red[kXWide / 32][kXMaxH];
   __shared__ double G[32 * 33];  // Gram of the nn entries, oldest first
   __shared__ double dots[kXMaxH];
   __shared__ bool last;
@@ -699,34 +700,39 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
     const int a = e / nn, b = e - a * nn;
     G[a * 33 + b] = c->gram[slot[a] * H + slot[b]];
   }
+  // this CTA's chunk of kXChunk elements: f = t_new - t into the ring and
+  // into shared memory, then warp w dots the chunk with entries w, w + 8, ...
+  // (coalesced rows, every load of a lane independent of the others)
   const size_t rows = (size_t)p.P * p.Ns;
+  const size_t e0 = (size_t)blockIdx.x * kXChunk;
   const double *t0 = p.ring_t + (size_t)head * rows;
   double *f0 = p.ring_f + (size_t)head * rows;
-  double acc[kXMaxH];
-#pragma unroll
-  for (int n = 0; n < kXMaxH; ++n) acc[n] = 0.0;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < rows;
-       e += (size_t)gridDim.x * blockDim.x) {
-    const double f = p.tn[e] - t0[e];  // zero on the unused row elements
-    f0[e] = f;
-#pragma unroll
-    for (int n = 0; n < kXMaxH; ++n)
-      if (n < nn) acc[n] += f * (n == nn - 1 ? f : p.ring_f[(size_t)slot[n] * rows + e]);
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int n = 0; n < kXMaxH; ++n) {
-    if (n >= nn) break;
-    double v = acc[n];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) red[wid][n] = v;
+  __shared__ double fs[kXChunk];
+  for (int k = threadIdx.x; k < kXChunk; k += blockDim.x) {
+    const size_t e = e0 + k;
+    double f = 0.0;
+    if (e < rows) {
+      f = p.tn[e] - t0[e];  // zero on the unused row elements
+      f0[e] = f;
+    }
+    fs[k] = f;
   }
   __syncthreads();
-  if (threadIdx.x < nn) {
-    double s = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w][threadIdx.x];
-    p.partials[(size_t)blockIdx.x * 32 + threadIdx.x] = s;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int n = wid; n < nn; n += kXWide / 32) {
+    const double *fn = p.ring_f + (size_t)slot[n] * rows + e0;
+    double acc = 0.0;
+    if (n == nn - 1) {  // the newest entry is this evaluation's f
+#pragma unroll 8
+      for (int k = lane; k < kXChunk; k += 32) acc += fs[k] * fs[k];
+    } else {
+#pragma unroll 8
+      for (int k = lane; k < kXChunk; k += 32)
+        if (e0 + k < rows) acc += fs[k] * fn[k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) p.partials[(size_t)blockIdx.x * 32 + n] = acc;
   }
   __threadfence();
   __syncthreads();
@@ -813,9 +819,9 @@ __global__ void __launch_bounds__(kXWide) xr_dots(XP p) {
     decide = dcs;
   }
   __syncthreads();
-  if (decide == 3) {
+  if (decide == 3 && threadIdx.x < 32) {
     if (threadIdx.x < nn) c->src[threadIdx.x] = slot[threadIdx.x];
-    diis_solve_block(G, nn, c->coef);
+    diis_solve_warp(G, nn, c->coef);
   }
 }
 
@@ -1035,7 +1041,7 @@ int r3d_xrism_solve(const r3d_xrism_opts *opts, const r3d_xrism_atom *atoms, int
   char *dmem = nullptr;
   XCtl *hctl = nullptr;
   const int nblk_dots =
-      std::max(1, std::min(296, (int)(((size_t)P * Ns + 4 * kXWide - 1) / (4 * kXWide))));
+      std::max(1, (int)(((size_t)P * Ns + kXChunk - 1) / kXChunk));
   const size_t rowsz = (size_t)P * Ns * sizeof(double);
   const size_t zsz = (size_t)P * M * sizeof(double2);
   size_t off = 0;
