@@ -1131,8 +1131,6 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
   if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
   if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
-  // after the mixer's arrays: placed between them it moved their relative
-  // DRAM offsets and cost the AN2 mix 12 % of its bandwidth at 256^3
   if ((rc = dalloc(c, &c->gq, n * N * sizeof(T)))) return rc;
   const int npart = std::max(max_ix_ctas(c->geo), c->geo.dot_ctas);
   if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;

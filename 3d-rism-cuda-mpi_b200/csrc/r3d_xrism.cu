@@ -1066,6 +1066,8 @@ int r3d_xrism_solve(const r3d_xrism_opts *opts, const r3d_xrism_atom *atoms, int
   const int per_graph = 8;
   long long max_evals = (long long)o.maxstep * o.nladder;
 
+  int prev_device = -1;
+  XCK(cudaGetDevice(&prev_device));
   XCK(cudaSetDevice(o.device));
   XCK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   XCK(cudaMalloc(&dmem, off));
@@ -1185,6 +1187,7 @@ done:
   if (dmem) cudaFree(dmem);
   if (hctl) cudaFreeHost(hctl);
   if (st) cudaStreamDestroy(st);
+  if (prev_device >= 0) cudaSetDevice(prev_device);  // the caller's current device
   return rc;
 }
 
