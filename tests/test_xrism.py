@@ -175,3 +175,30 @@ def test_oracle_writer_matches_library_writer(R, solvents, tmp_path):
     x.write_xvk(a)
     oracle.write_xvk(b, d["atoms"], d["temper"], d["ntab"], d["dr"], d["xvv"], d["xt"])
     assert open(a).read() == open(b).read()
+
+
+def test_bench_solvent_tables_without_gpu(tmp_path):
+    """bench.py's reference arm makes the configurations' tables with the CPU
+    oracle (no GPU); the decks of every configuration then name files that
+    exist and parse as .xvk with the configuration's temperature."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    try:
+        bench.prepare_solvents("baseline")
+        assert sorted(bench.SOLV) == ["nacl01", "nacl02", "water"]
+        inp, xvk = bench.make_deck(str(tmp_path), atoms=20, grid=64)
+        d = oracle.read_xvk(xvk)
+        assert d["temper"] == 298.15 and d["natv"] == 4
+        assert [a["name"] for a in d["atoms"]] == ["O", "H", "H", "Na", "Cl"]
+        assert abs(d["atoms"][4]["sig"] - 4.40) < 1e-9
+        bench.prepare_solvents("shipped")
+        assert bench.SOLV["nacl02"] == "naclaq_vv.xvk"
+        os.makedirs(str(tmp_path / "s"))
+        inp, xvk = bench.make_deck(str(tmp_path / "s"), atoms=20, grid=64)
+        assert oracle.read_xvk(xvk)["temper"] == 300.0
+    finally:
+        import shutil
+        if bench._SOLVENT_DIR:
+            shutil.rmtree(bench._SOLVENT_DIR, ignore_errors=True)
