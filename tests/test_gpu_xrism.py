@@ -122,3 +122,24 @@ def test_gpu_baseline_solvents(R, name, tmp_path):
     s = R.RISM3D(precision="fp64")
     s.initialize(inp, xvk=path)
     assert s.iterate()[2] == "converged"
+
+
+def test_gpu_seven_site_classes(R):
+    """More than six site classes take the runtime-sized OZ kernel and the
+    separate packing launch: water with five ions (Na, Cl, K, Br, Li; 0.15 M
+    of each charge), 2048 points, against the oracle."""
+    import synthetic
+    atoms = [dict(spc=a["species"], sym=a["sym"], sig=a["sigma"], eps=a["epsilon"],
+                  q=a["charge"], xyz=a["xyz"], den=a["density"], name=a["name"])
+             for a in synthetic.water_atoms(55.0)]
+    ions = [("Na", 2.43, 0.0874, 1.0, 0.05), ("Cl", 4.40, 0.1, -1.0, 0.1),
+            ("K", 3.14, 0.087, 1.0, 0.05), ("Br", 4.62, 0.09, -1.0, 0.05),
+            ("Li", 2.13, 0.018, 1.0, 0.05)]
+    for i, (nm, s, e, q, c) in enumerate(ions):
+        atoms.append(dict(spc=2 + i, sym=3 + i, sig=s, eps=e * 4184.0, q=q, xyz=(0.0, 0.0, 0.0),
+                          den=c, name=nm))
+    x, tab, oxvv, oinfo = _solve_both(R, atoms, 298.15, 2048, 0.05)
+    assert x.result["natv"] == 7
+    assert x.result["status"] == oinfo["status"] == "converged", (x.result, oinfo)
+    assert np.abs(tab - oxvv).max() < GPU_ORACLE_TOL, np.abs(tab - oxvv).max()
+    assert abs(x.result["xt"] / oinfo["xt"] - 1) < GPU_ORACLE_XT
