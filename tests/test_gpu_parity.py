@@ -148,3 +148,31 @@ def test_mixed_maxstep_results_are_of_the_last_evaluation(R, refcase):
         g[prec] = s.get("g")
         s.close()
     assert np.abs(g["mixed"] - g["fp64"]).max() < 1e-4 * max(1.0, np.abs(g["fp64"]).max())
+
+
+def test_runtime_length_x_engine_matches_oracle(R, solvents, tmp_path):
+    """nx = 72 (an x transform of 36 complex points, not a compile-time
+    length) runs the runtime-length x passes, which also write and read the
+    g grid: FP64 against the oracle on the same deck, mixed within its
+    tolerance of FP64."""
+    import shutil
+    import synthetic
+    shutil.copyfile(solvents["h2o_vv"], str(tmp_path / "h2o_vv.xvk"))
+    inp = synthetic.small(str(tmp_path), nu=8, grid=(72, 64, 64), box=(36.0, 32.0, 32.0),
+                          name="rt72")
+    xvk = str(tmp_path / "h2o_vv.xvk")
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = _solver(R, inp, xvk, prec=prec)
+        steps, rms, status = s.iterate()
+        assert status == "converged"
+        out[prec] = (steps, np.array(s.thermo()[0]))
+        s.close()
+    o = O.Oracle(inp, xvk=xvk)
+    o.initialize()
+    osteps, orms, ostatus = o.iterate()
+    assert ostatus == "converged"
+    oxmu = np.array(o.thermo()[0])
+    assert abs(out["fp64"][0] - osteps) <= 1
+    assert np.abs(out["fp64"][1] - oxmu).max() < 1e-6
+    assert np.abs(out["mixed"][1] - out["fp64"][1]).max() < 0.02
