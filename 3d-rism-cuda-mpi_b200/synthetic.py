@@ -214,16 +214,16 @@ def nacl_atoms(conc_m):
              xyz=(0.0, 0.0, 0.0), density=conc_m)]
 
 
-BASELINE_SOLVENTS = {"water_298": lambda: water_atoms(),
+CONFIG_SOLVENTS = {"water_298": lambda: water_atoms(),
                      "nacl02_298": lambda: nacl_atoms(0.2),
                      "nacl01_298": lambda: nacl_atoms(0.1)}
 
 
 def make_solvent(name, outdir, device=0, ntab=8192, dr=0.05, temperature=298.15):
-    """Solve one of BASELINE_SOLVENTS with the 1D XRISM solver and write
+    """Solve one of CONFIG_SOLVENTS with the 1D XRISM solver and write
     <outdir>/<name>.xvk; returns (path, result dict)."""
     import rism3d
-    x = rism3d.XRISM(BASELINE_SOLVENTS[name](), device=device, ntab=ntab, dr=dr,
+    x = rism3d.XRISM(CONFIG_SOLVENTS[name](), device=device, ntab=ntab, dr=dr,
                      temperature=temperature)
     x.solve()
     if x.result["status"] != "converged":

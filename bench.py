@@ -48,26 +48,26 @@ FALLBACK_HBM_GBS = 6650.0
 # The configurations name 298.15 K water and 0.1 / 0.2 M NaCl with their own
 # ion LJ parameters; the reference ships water at 300 K and 0.2 M NaCl with
 # other ion parameters.  By default the run makes the named tables with the
-# 1D XRISM solve (synthetic.BASELINE_SOLVENTS; on the GPU, or with the CPU
+# 1D XRISM solve (synthetic.CONFIG_SOLVENTS; on the GPU, or with the CPU
 # oracle on the reference arm); --solvent shipped uses the reference's files.
 SOLVENT_FILES = {
     "shipped": {"water": "h2o_vv.xvk", "nacl02": "naclaq_vv.xvk", "nacl01": "naclaq_vv.xvk"},
-    "baseline": {"water": "water_298.xvk", "nacl02": "nacl02_298.xvk",
+    "configuration": {"water": "water_298.xvk", "nacl02": "nacl02_298.xvk",
                  "nacl01": "nacl01_298.xvk"},
 }
 SOLVENT_DATA = {
     "shipped": "the reference's shipped .xvk tables (water 300 K, 0.2 M NaCl)",
-    "baseline": "298.15 K water and 0.1 / 0.2 M NaCl of the configuration, tables made by "
+    "configuration": "298.15 K water and 0.1 / 0.2 M NaCl of the configuration, tables made by "
                 "this repository's 1D XRISM solve",
 }
-SOLV = dict(SOLVENT_FILES["baseline"])
+SOLV = dict(SOLVENT_FILES["configuration"])
 _SOLVENT_DIR = None
 
 
 def prepare_solvents(kind, device=None):
     """Makes this run's solvent tables once.  device: the GPU for the 1D
     solves (None: the CPU oracle, for the reference arm).  Returns the 1D
-    solves' measurements (baseline tables made on the GPU) or None."""
+    solves' measurements (configuration tables made on the GPU) or None."""
     global _SOLVENT_DIR
     SOLV.clear()
     SOLV.update(SOLVENT_FILES[kind])
@@ -83,7 +83,7 @@ def prepare_solvents(kind, device=None):
     if device is None:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
-        for name, make in S.BASELINE_SOLVENTS.items():
+        for name, make in S.CONFIG_SOLVENTS.items():
             atoms = [dict(name=a["name"], spc=a["species"], sym=a["sym"], sig=a["sigma"],
                           eps=a["epsilon"], q=a["charge"], xyz=a["xyz"], den=a["density"])
                      for a in make()]
@@ -92,7 +92,7 @@ def prepare_solvents(kind, device=None):
                         info["xt"])
         return None
     report = {}
-    for name in S.BASELINE_SOLVENTS:
+    for name in S.CONFIG_SOLVENTS:
         runs = []
         for _ in range(2):  # the first also pays the CUDA context
             t0 = time.perf_counter()
@@ -115,7 +115,7 @@ import sys, time, json
 sys.path.insert(0, %r); sys.path.insert(0, %r)
 import oracle as O, synthetic as S
 atoms = [dict(name=a["name"], spc=a["species"], sym=a["sym"], sig=a["sigma"], eps=a["epsilon"],
-              q=a["charge"], xyz=a["xyz"], den=a["density"]) for a in S.BASELINE_SOLVENTS[%r]()]
+              q=a["charge"], xyz=a["xyz"], den=a["density"]) for a in S.CONFIG_SOLVENTS[%r]()]
 t0 = time.perf_counter()
 xvv, info = O.xrism_solve(atoms, 298.15, 8192, 0.05)
 print(json.dumps({"s": time.perf_counter() - t0, "steps": info["steps"]}))
@@ -678,7 +678,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
-    ap.add_argument("--solvent", choices=["baseline", "shipped"], default="baseline",
+    ap.add_argument("--solvent", choices=["configuration", "shipped"], default="configuration",
                     help="solvent tables: made by the 1D XRISM solve, or the shipped ones")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":

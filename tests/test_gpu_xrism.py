@@ -103,12 +103,12 @@ def test_gpu_table_feeds_the_3d_solve(R, solvents, refcase, tmp_path):
 
 
 @pytest.mark.parametrize("name", ["water_298", "nacl01_298", "nacl02_298"])
-def test_gpu_baseline_solvents(R, name, tmp_path):
+def test_gpu_configuration_solvents(R, name, tmp_path):
     """The configurations' solvents (298.15 K water, 0.1 / 0.2 M NaCl with
     their ion LJ): GPU against the oracle, and the written table drives a 3D
     solve of a small deck to convergence."""
     import synthetic
-    atoms = synthetic.BASELINE_SOLVENTS[name]()
+    atoms = synthetic.CONFIG_SOLVENTS[name]()
     oatoms = [dict(spc=a["species"], sym=a["sym"], sig=a["sigma"], eps=a["epsilon"],
                    q=a["charge"], xyz=a["xyz"], den=a["density"]) for a in atoms]
     path, res = synthetic.make_solvent(name, str(tmp_path))

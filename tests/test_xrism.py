@@ -186,7 +186,7 @@ def test_bench_solvent_tables_without_gpu(tmp_path):
     sys.path.insert(0, root)
     import bench
     try:
-        bench.prepare_solvents("baseline")
+        bench.prepare_solvents("configuration")
         assert sorted(bench.SOLV) == ["nacl01", "nacl02", "water"]
         inp, xvk = bench.make_deck(str(tmp_path), atoms=20, grid=64)
         d = oracle.read_xvk(xvk)
