@@ -18,8 +18,11 @@
  * the form of Kovalenko, Ten-no and Hirata (J. Comput. Chem. 20, 928
  * (1999)).  Pinned: with the reference's physical constants
  * (src-cuda-mpi/physical.h:5-14) and a Coulomb split erf(r/1 A)/r it
- * reproduces the shipped water and 0.2 M NaCl tables to ~2e-7 and their
- * compressibility column to ~4e-7 relative (tests/test_xrism.py).
+ * re-makes the four shipped tables from their own atom tables -- water and
+ * 0.2 M NaCl / KCl at 300 K to 1.3-3.1e-7, their compressibility column to
+ * 2-5e-7 relative, and the 298.15 K ctip3p water to 1.2e-7 once its H
+ * positions (printed to 5 decimals) are recovered from the table's own
+ * large-k rows (tests/test_xrism.py).
  *
  * Sites are reduced to the reader's classes (|sym|): rep(A) is the first
  * atom of class A, n_B rho_B = rhov[B] the summed site density, and
