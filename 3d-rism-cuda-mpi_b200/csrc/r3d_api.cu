@@ -225,6 +225,9 @@ struct r3d_ctx {
   cudaGraphExec_t gexec = nullptr;
   double ms_per_iter = 0;
   int kernels_per_iter = 0;
+  // CUDA-event times of the last initialize: potential pair sums, k-space
+  // Coulomb sum, long-range h term (refresh), whole initialize (host clock)
+  double setup_ms[4] = {0, 0, 0, 0};
   unsigned long long h2d = 0, d2h = 0;  // bytes copied each way
 };
 
@@ -1261,6 +1264,9 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     cudaError_t e = cudaMalloc((void **)&tabs, ntab * sizeof(double2));
     if (e != cudaSuccess) return fail(c, R3D_ENOMEM, "setup scratch");
     double *fr64 = nullptr;
+    cudaEvent_t ev[4];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(ev[0], s));
     if (nu > 0) {
       if (natom != (size_t)nu) return fail(c, R3D_EINVAL, "internal: atom stride");
       launch_potential<P>(d, at, ikbt, ubeta, dr, coulomb, fr64, s);
@@ -1269,6 +1275,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
       CK(cudaMemsetAsync(c->u, 0, n * N * sizeof(R), s));
       CK(cudaMemsetAsync(c->t, 0, n * N * sizeof(T), s));
     }
+    CK(cudaEventRecord(ev[1], s));
     if (coulomb && nu > 0) {
       double2 *ex = tabs, *ey = tabs + (size_t)nu * d.hx, *ez = ey + (size_t)nu * d.ny;
       launch_phase_tables(ex, ey, ez, dx, dy, dz, nu, d.nx, d.ny, d.nz, p.box, s);
@@ -1276,10 +1283,25 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
       launch_fk(d, (double2 *)c->fk, ex, ey, ez, dq, nu, ubeta, p.box, dv, s);
       CK(cudaGetLastError());
     }
+    CK(cudaEventRecord(ev[2], s));
     CK(cudaStreamSynchronize(s));
     cudaFree(tabs);
     // long-range h term: lr = 1 - F^-1[chi q phi_L(k)]  (refresh, c_ref = 0)
+    CK(cudaEventRecord(ev[3], s));
     if ((rc = refresh<P>(c, true))) return rc;
+    cudaEvent_t ev4;
+    CK(cudaEventCreate(&ev4));
+    CK(cudaEventRecord(ev4, s));
+    CK(cudaEventSynchronize(ev4));
+    float t01 = 0, t12 = 0, t34 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t12, ev[1], ev[2]);
+    cudaEventElapsedTime(&t34, ev[3], ev4);
+    c->setup_ms[0] = t01;
+    c->setup_ms[1] = t12;
+    c->setup_ms[2] = t34;
+    for (auto &e : ev) cudaEventDestroy(e);
+    cudaEventDestroy(ev4);
   }
   // control block and descriptor
   {
@@ -1332,12 +1354,22 @@ extern "C" int r3d_initialize(r3d_ctx *c) {
   if (need > fre) return fail(c, R3D_ENOMEM, "problem needs " + std::to_string(need) +
                                                  " device bytes, " + std::to_string(fre) + " free");
   c->desc = d;
+  const auto t0 = std::chrono::steady_clock::now();
   rc = c->fp64 ? init_typed<P64>(c, st) : init_typed<PMix>(c, st);
   if (rc) {
     free_all(c);
     return rc;
   }
+  c->setup_ms[3] =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   c->initialized = true;
+  return R3D_OK;
+}
+
+extern "C" int r3d_setup_timing(const r3d_ctx *c, double *ms) {
+  if (!c || !ms) return fail(nullptr, R3D_EINVAL, "bad arguments");
+  if (!c->initialized) return fail(nullptr, R3D_ESTATE, "setup timing before initialize");
+  for (int i = 0; i < 4; ++i) ms[i] = c->setup_ms[i];
   return R3D_OK;
 }
 

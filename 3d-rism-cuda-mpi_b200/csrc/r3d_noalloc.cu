@@ -3,9 +3,8 @@
 //
 // Who needs this: callers that cannot call cudaMalloc -- code that runs
 // while another framework owns the device's memory pool (and forbids or
-// cannot afford foreign allocations), real-time loops that must not take
-// the allocator's locks or risk an out-of-memory failure in mid-run, and
-// code recorded once and replayed where an allocation would not be replayed.
+// cannot afford foreign allocations), and real-time loops that must not
+// take the allocator's locks or risk an out-of-memory failure in mid-run.
 // They pass device pointers for the input and the output; the only working
 // storage is the fixed array below, which every GPU that loads this library
 // holds until the process exits.
@@ -14,11 +13,15 @@
 // contents of the last call.  Calls that overlap on the GPU (concurrent
 // streams or threads) race on it and must be serialised by the caller.  The
 // first call on each device looks up the array's device address (with that
-// device current); make that first call before any stream capture.
+// device current); make that first call before any stream capture.  That
+// look-up is made under a lock, so host threads whose first calls coincide
+// do not race on it.  The caller's current device is restored on return.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/rism3d_b200.h"
@@ -53,7 +56,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 namespace r3d {
 void set_last_error(const std::string &m);  // r3d_last_error(NULL) reports it
 }
-static void *g_noalloc_ptr[64];  // device address of the array, per ordinal
+// device address of the array, per ordinal (set once, under g_noalloc_mu)
+static std::atomic<void *> g_noalloc_ptr[64];
+static std::mutex g_noalloc_mu;
 
 static int noalloc_fail(int code, const std::string &m) {
   set_last_error("r3d_fft3d_noalloc: " + m);
@@ -79,6 +84,23 @@ __global__ void k_noalloc_scale_inv_in(const double *in, double2 *raw, long long
     const int p = (int)(i % hx), y = (int)((i / hx) % ny), z = (int)(i / ((long long)hx * ny));
     const double sg = ((2 * p + y + z + par0) & 1) ? -1.0 : 1.0;
     raw[i] = make_double2(-in[2 * i + 1] * sg / dv, in[2 * i] * sg / dv);
+  }
+}
+// The descriptor (as plain 8-byte words), a cleared control block and the
+// launch prefixes, written from kernel parameters (no host staging buffer is
+// involved).
+static_assert(sizeof(Desc) % 8 == 0, "descriptor words");
+struct DescWords {
+  unsigned long long w[sizeof(Desc) / 8];
+};
+__global__ void k_noalloc_setup(DescWords d, Desc *dd, Ctl *ctl, int4 pa, int4 pb, int *pre) {
+  for (int i = threadIdx.x; i < (int)(sizeof(Desc) / 8); i += blockDim.x)
+    ((unsigned long long *)dd)[i] = d.w[i];
+  for (int i = threadIdx.x; i < (int)(sizeof(Ctl) / sizeof(int)); i += blockDim.x)
+    ((int *)ctl)[i] = 0;
+  if (threadIdx.x == 0) {
+    pre[0] = pa.x, pre[1] = pa.y, pre[2] = pa.z, pre[3] = pa.w;
+    pre[4] = pb.x, pre[5] = pb.y, pre[6] = pb.z, pre[7] = pb.w;
   }
 }
 __global__ void k_noalloc_scale(double *x, long long n, double s) {
@@ -132,17 +154,34 @@ extern "C" int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const doubl
   d.tiles_y = nz * (hx / Py);
   d.tiles_z = ny * (hx / Pz);
 
-  cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) return noalloc_fail(R3D_ECUDA, cudaGetErrorString(e));
-  if (!g_noalloc_ptr[device]) {  // first call on this device: find the array
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return noalloc_fail(R3D_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_noalloc_ptr[device] = p;
-    kernels_set_smem(true, 220 * 1024);
+  // an error left pending by earlier work of the process is not this call's:
+  // report it without clearing it
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return noalloc_fail(R3D_ECUDA, std::string("a CUDA error was pending before the call: ") +
+                                       cudaGetErrorString(e));
+  int caller = -1;
+  if ((e = cudaGetDevice(&caller)) != cudaSuccess)
+    return noalloc_fail(R3D_ECUDA, cudaGetErrorString(e));
+  struct Restore {  // the caller's current device, on every return path
+    int dev;
+    ~Restore() { cudaSetDevice(dev); }
+  } restore{caller};
+  if ((e = cudaSetDevice(device)) != cudaSuccess)
+    return noalloc_fail(R3D_ECUDA, cudaGetErrorString(e));
+  if (!g_noalloc_ptr[device].load()) {  // first call on this device: find the array
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device].load()) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return noalloc_fail(R3D_ECUDA,
+                            std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      kernels_set_smem(true, 220 * 1024);
+      g_noalloc_ptr[device].store(p);
+    }
   }
-  unsigned char *base = (unsigned char *)g_noalloc_ptr[device];
+  unsigned char *base = (unsigned char *)g_noalloc_ptr[device].load();
   Desc *dd = (Desc *)base;
   Ctl *ctl = (Ctl *)(base + kOffCtl);
   int *pre = (int *)(base + kOffPre);
@@ -150,13 +189,12 @@ extern "C" int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const doubl
   d.w = w;
   d.ctl = ctl;
   const int ix_ctas = d.tiles_x;
-  int pf[8] = {0, d.tiles_x, 0, d.tiles_y, 0, d.tiles_z, 0, ix_ctas};
-  Ctl hctl{};  // cleared each call: nothing of the previous call is reused
   cudaStream_t s = (cudaStream_t)stream;
-  if ((e = cudaMemcpyAsync(dd, &d, sizeof(Desc), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(ctl, &hctl, sizeof(Ctl), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(pre, pf, sizeof(pf), cudaMemcpyHostToDevice, s)) != cudaSuccess)
-    return noalloc_fail(R3D_ECUDA, cudaGetErrorString(e));
+  // control block cleared each call: nothing of the previous call is reused
+  DescWords dw;
+  std::memcpy(dw.w, &d, sizeof(Desc));
+  k_noalloc_setup<<<1, 128, 0, s>>>(dw, dd, ctl, make_int4(0, d.tiles_x, 0, d.tiles_y),
+                                    make_int4(0, d.tiles_z, 0, ix_ctas), pre);
   const double dv = box[0] * box[1] * box[2] / (double)N;
   const int par0 = ((nx + ny + nz) / 2) & 1;
   Batch bx{dd, pre, 1}, by{dd, pre + 2, 1}, bz{dd, pre + 4, 1}, bix{dd, pre + 6, 1};

@@ -8,17 +8,29 @@
 A step is one iteration of the solve (evaluate + RMS + mixing).  Printed as
 one JSON line on rank 0:
   value        whole-job iterations/s with all state resident in HBM (each GPU
-               runs its own solve: weak scaling, no data-path collective)
+               runs its own solve: weak scaling, no data-path collective);
+               K steps are timed per measurement, and measurements of K
+               steps repeat until they cover at least one second
   e2e          iterations/s of complete solves through the C-ABI from host
                files to host results (parse, upload, setup, iterate, thermo,
                g(r) read-back), plus solves/s
+  fp64         the plain FP64 path on the same workload: ms/iteration, and a
+               complete solve (iterations to converge, solves/s)
+  mixed_vs_fp64  excess chemical potential and partial molar volume of the
+               mixed solve against the FP64 solve
+  reference_cuda the reference's own CUDA build (one rank, oracle/_ref) on
+               the same deck: its -DTEST timers, ms/iteration
   roofline     the dominant kernel's algorithmic bytes / its CUDA-event time
+  setup        the one-time potential kernels as pair terms/s against the
+               FP64 (or FP32) FMA rate
   cpu_baseline the FP64 CPU oracle on the same grid and solvent
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
-                  [--impl b200|reference]
-`--impl reference` times the CPU restatement of the reference's solve (the
-reference ships no CPU path) on the host cores for the same workload.
+                  [--impl b200|reference] [--config c2|c3]
+With --gpus N > 1 and no outer launcher, the script starts its own N ranks
+(torch.distributed.run on 127.0.0.1).  `--impl reference` times the CPU
+restatement of the reference's solve (the reference ships no CPU path) on the
+host cores for the same workload.
 """
 import argparse
 import gzip
@@ -34,6 +46,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "3d-rism-cuda-mpi_b200")
 sys.path.insert(0, PKG)
+import replicas  # noqa: E402
 
 METRIC = "ms/iter & solves/s at RMS<1e-6, mixed vs FP64, 1 B200; served p50/p99 latency"
 WORKLOAD = ("256^3 grid, 128 A cell, 2000-atom seeded globule, 0.2 M NaCl water "
@@ -254,29 +267,100 @@ def ncu_traffic(kernel):
         return None
 
 
+# ------------------------------------------------------- measurement helpers
+MIN_TIMED_MS = 1000.0   # the timed measurements of K steps cover at least this
+N_A = 6.02214076e23
+KCAL = 4184.0
+NUM_SM = 148
+# FP64 / FP32 lanes per SM per clock (B200: 64 FP64 and 128 FP32 units per SM)
+LANES = {"fp64": 64, "fp32": 128}
+
+
+def timed_steps(group, s, k, max_reps=500):
+    """Measurements of exactly k iterations (barrier, CUDA events around the
+    k graph replays, barrier; max over ranks), repeated until they cover
+    MIN_TIMED_MS.  Returns (total ms, k * repetitions, repetitions); every
+    rank takes the same decisions (the totals are maxima over ranks)."""
+    total, reps = 0.0, 0
+    while True:
+        ms, _ = group.timed(lambda: (s.step(k), k))
+        total += ms
+        reps += 1
+        if total >= MIN_TIMED_MS or reps >= max_reps:
+            return total, k * reps, reps
+
+
+def pmv_a3(pmv_m3_per_mol):
+    """Partial molar volume in A^3 per molecule from m^3/mol."""
+    return pmv_m3_per_mol * 1e30 / N_A
+
+
+def sec8d_bytes(N, n, b, m):
+    """Algorithmic bytes of one iteration of an idealised slab-FFT design:
+    A_iter = N b (n (14 + 3 m) + 2), and the per-stage arrays of N b bytes
+    (stage A: closure + forward slab pass 3n + 1, B: pencil pass + OZ 2n + 1,
+    C: inverse pass + residual + dots (4 + m) n, D: mixing (5 + 2 m) n)."""
+    arr = N * b
+    return {"iteration": arr * (n * (14 + 3 * m) + 2), "A": arr * (3 * n + 1),
+            "B": arr * (2 * n + 1), "C": arr * (4 + m) * n, "D": arr * (5 + 2 * m) * n}
+
+
+# which stage of that count each of this design's kernels does (a kernel that
+# has no stage there -- the separate y passes -- is counted by its own bytes)
+KERNEL_STAGE = {"fwd_x": "A", "zoz": "B", "inv_x": "C", "mix_an2": "D", "mix_anm": "D"}
+
+
+def reference_cuda(deck, xvk, maxstep=None, timeout=1800):
+    """The reference's own CUDA build (oracle/ref/build_ref.sh: its sources at
+    one rank, cuFFT, FP64) on the same deck and solvent table, timed by its
+    -DTEST timers (iterate.cu:96-105): ms/iteration = Iteration / steps.
+    maxstep caps the iterations (the per-iteration cost does not change)."""
+    import re
+    binp = os.path.join(ROOT, "oracle", "_ref", "3drism-cuda-mpi")
+    if not os.path.exists(binp):
+        return {"unavailable": "oracle/_ref/3drism-cuda-mpi is not built"}
+    d = tempfile.mkdtemp(prefix="r3dref_")
+    try:
+        lines = open(deck).read().split("\n")
+        if maxstep is not None:  # line 4: tolerance and maxstep (read_input.cu:48-52)
+            tol = lines[3].split()[0]
+            lines[3] = f" {tol}   {maxstep}"
+        name = os.path.basename(deck)
+        open(os.path.join(d, name), "w").write("\n".join(lines))
+        shutil.copyfile(xvk, os.path.join(d, lines[2].strip()))
+        env = dict(os.environ, OMPI_COMM_WORLD_LOCAL_RANK="0")
+        t0 = time.perf_counter()
+        out = subprocess.run([binp, name], cwd=d, env=env, capture_output=True, text=True,
+                             timeout=timeout)
+        wall = time.perf_counter() - t0
+        log = out.stdout
+        steps = re.findall(r"Step = (\d+) Reside = (\S+)", log)
+        timers = {k.strip(): float(v)
+                  for k, v in re.findall(r"^(\w[\w ]*?)\s*:\t([0-9.]+) sec", log, re.M)}
+        if out.returncode or not steps or "Iteration" not in timers:
+            return {"unavailable": f"reference run failed (rc {out.returncode}): "
+                                   + (out.stderr or log)[-300:]}
+        n = int(steps[-1][0])
+        res = {"ms_per_iter": 1e3 * timers["Iteration"] / n, "iterations": n,
+               "status": "converged" if maxstep is None and "reached limit" not in log
+               else "maxstep", "wall_s": wall, "timers_s": timers,
+               "precision": "fp64", "transforms": "cuFFT Z2Z (the reference's fft3d.cu)",
+               "binary": "oracle/_ref/3drism-cuda-mpi (oracle/ref/build_ref.sh, one rank)"}
+        stem = os.path.splitext(name)[0]
+        xmu = os.path.join(d, stem + ".xmu")
+        if os.path.exists(xmu):
+            res["sfe_sc_kcal_per_mol"] = _sfe_kcal(xmu)
+        return res
+    except (OSError, subprocess.TimeoutExpired) as e:
+        return {"unavailable": f"reference run failed: {e}"}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 # -------------------------------------------------------------- GPU arm
-def run_gpu(args, rank, world, local):
+def run_gpu(args, group):
     import rism3d as R
-    dist = None
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if dist:
-            dist.barrier()
-
-    def allmax(x):
-        if not dist:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
+    rank, world, local = group.rank, group.world, group.local
     prec = args.precision
     xrism = prepare_solvents(args.solvent, device=local)
     tmp = tempfile.mkdtemp(prefix=f"r3dbench{rank}_")
@@ -300,10 +384,10 @@ def run_gpu(args, rank, world, local):
     # and copies g back to host memory.  The first solve of the process also
     # pays the CUDA runtime's start-up; it is reported as cold_solve_s and
     # the warm solves give the e2e rate.
-    def one_solve(tag):
+    def one_solve(tag, p):
         ph = {}
         t0 = time.perf_counter()
-        s = R.RISM3D(device=local, precision=prec)
+        s = R.RISM3D(device=local, precision=p)
         ph["create_s"] = time.perf_counter() - t0
         t1 = time.perf_counter()
         s.load(inp, xvk=xvk)
@@ -316,69 +400,116 @@ def run_gpu(args, rank, world, local):
         steps, rms, status = s.iterate()
         ph["iterate_s"] = time.perf_counter() - t1
         t1 = time.perf_counter()
-        xmu_path = os.path.join(tmp, f"c2_{tag}.xmu")
+        xmu_path = os.path.join(tmp, f"solve_{tag}.xmu")
         s.output(xmu_path)
         g = s.get("g")
         ph["output_s"] = time.perf_counter() - t1
         total = time.perf_counter() - t0
         h2d, d2h = s.transfer_bytes()
+        pmv = s.thermo()[2]
+        setup = s.setup_timing()
         s.close()
         del g
-        return total, ph, steps, rms, status, h2d, d2h, xmu_path
+        return dict(total=total, phases=ph, steps=steps, rms=rms, status=status, h2d=h2d,
+                    d2h=d2h, sfe=_sfe_kcal(xmu_path), pmv=pmv, setup=setup)
 
-    barrier()
-    cold_s = allmax(one_solve("cold")[0])
+    group.barrier()
+    cold_s = group.allmax(one_solve("cold", prec)["total"])
     warm = []
     for r in range(max(1, args.e2e_reps)):
-        barrier()
-        out = one_solve(f"w{r}")
-        warm.append((allmax(out[0]),) + out[1:])
-    e2e_s = sum(w[0] for w in warm) / len(warm)
-    _, phases, steps, rms, status, h2d, d2h, xmu_path = warm[-1]
-    sfe_kcal = None
-    for ln in open(xmu_path):
-        if ln.startswith("SFE_SC="):
-            sfe_kcal = float(ln.split()[1]) / 4184.0
+        group.barrier()
+        out = one_solve(f"w{r}", prec)
+        out["total"] = group.allmax(out["total"])
+        warm.append(out)
+    e2e_s = sum(w["total"] for w in warm) / len(warm)
+    last = warm[-1]
 
     # ---- device-resident iteration throughput --------------------------
     s = R.RISM3D(device=local, precision=prec)
     s.load(inp, xvk=xvk)
     configure(s)
-    s.set_control(convergence=1e-300, maxstep=10 ** 8)
+    s.set_control(convergence=1e-300, maxstep=10 ** 9)
     s.initialize()
     s.step(args.warmup)
-    barrier()
     with ClockSampler(local) as clk:
-        ms = s.step(args.steps)
-    ms = allmax(ms)
+        ms, timed, reps = timed_steps(group, s, args.steps)
     _, kpi = s.timing()
     st = s.status()
     if st[2] != "running":
         raise RuntimeError(f"solve left the running state during timing: {st}")
     prof = s.profile_kernels(reps=10)
     s.close()  # before the FP64 run: at 512^3 the two do not fit together
-    ms_iter = ms / args.steps
-    value = world * args.steps / (ms * 1e-3)
+    ms_iter = ms / timed
+    value = world * timed / (ms * 1e-3)
 
-    # FP64 comparison on the same workload (a shorter timed run)
-    fp64 = None
+    # ---- the plain FP64 path on the same workload ------------------------
+    fp64 = mvf = None
     if prec == "mixed" and not args.no_fp64:
         s64 = R.RISM3D(device=local, precision="fp64")
         s64.load(inp, xvk=xvk)
         configure(s64)
-        s64.set_control(convergence=1e-300, maxstep=10 ** 8)
+        s64.set_control(convergence=1e-300, maxstep=10 ** 9)
         s64.initialize()
         s64.step(args.warmup)
         k64 = max(10, args.steps // 4)
-        ms64 = allmax(s64.step(k64))
-        fp64 = {"ms_per_iter": ms64 / k64, "iter_per_s": world * k64 / (ms64 * 1e-3)}
+        ms64, timed64, _ = timed_steps(group, s64, k64)
         s64.close()
+        fp64 = {"ms_per_iter": ms64 / timed64, "iter_per_s": world * timed64 / (ms64 * 1e-3),
+                "steps_timed": timed64}
+        # complete FP64 solves (the first also loads the FP64 kernels)
+        solves64 = []
+        for r in range(1 if c3 else 2):
+            group.barrier()
+            o = one_solve(f"f{r}", "fp64")
+            o["total"] = group.allmax(o["total"])
+            solves64.append(o)
+        f = solves64[-1]
+        fp64.update({"iters_to_converge": f["steps"], "solve_status": f["status"],
+                     "final_rms": f["rms"], "solve_s": f["total"],
+                     "solves_per_s": world / f["total"], "phases_s": f["phases"],
+                     "sfe_sc_kcal_per_mol": f["sfe"], "pmv_A3": pmv_a3(f["pmv"])})
+        if f["status"] == "converged" and last["status"] == "converged":
+            mvf = {"sfe_err_kcal": abs(last["sfe"] - f["sfe"]),
+                   "pmv_err_A3": abs(pmv_a3(last["pmv"]) - pmv_a3(f["pmv"])),
+                   "bars": {"sfe_kcal": 0.01, "pmv_A3": 0.1},
+                   "iterations": {"mixed": last["steps"], "fp64": f["steps"]}}
 
-    # dominant kernel roofline
-    name, kms, kbytes = max(prof, key=lambda x: x[1])
+    # ---- roofline of the dominant kernel --------------------------------
     peak, peak_kind = peak_hbm()
-    achieved = kbytes / (kms * 1e-3) / 1e9
-    iter_bytes = sum(b for _, _, b in prof)
+    name, kms, kbytes = max(prof, key=lambda x: x[1])
+    b = 8 if prec == "fp64" else 4
+    m = 10 if c3 else 2
+    N = (512 if c3 else args.grid) ** 3
+    sec8 = sec8d_bytes(N, 4, b, m)
+    stage = KERNEL_STAGE.get(name)
+    alg = sec8[stage] if stage else kbytes
+    achieved = alg / (kms * 1e-3) / 1e9
+    iter_bytes = sum(bb for _, _, bb in prof)
+
+    # ---- one-time setup kernels against the FMA rate --------------------
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    atoms = 12877 if c3 else args.atoms
+    su = last["setup"]
+    pairs = N * atoms * (4 + 1)  # LJ n N Nu + real-space Coulomb N Nu
+    # FP64 operations per atom-voxel pair as written in k_potential (each +,
+    # *, fma, fmin, compare, rsqrt and exp counted once): 12.5 shared + 6 per
+    # site -> a lower bound on the work, so the fraction is a lower bound too
+    ops = N * atoms * (12.5 + 6 * 4)
+    lanes = LANES["fp64"]
+    peak_ops = NUM_SM * lanes * sm_mhz * 1e6
+    setup = {
+        "potential": {"ms": su["potential_ms"], "pair_terms": pairs,
+                      "pair_terms_per_s": pairs / (su["potential_ms"] * 1e-3),
+                      "ops_per_pair_as_written": 12.5 + 6 * 4,
+                      "ops_per_s": ops / (su["potential_ms"] * 1e-3),
+                      "peak_ops_per_s": peak_ops, "arith": "fp64",
+                      "peak": f"{NUM_SM} SMs x {lanes} FP64 lanes x {sm_mhz:.0f} MHz (nominal)",
+                      "frac": ops / (su["potential_ms"] * 1e-3) / peak_ops},
+        "fk": {"ms": su["fk_ms"], "complex_terms": N // 2 * atoms,
+               "complex_terms_per_s": N // 2 * atoms / max(su["fk_ms"] * 1e-3, 1e-12)},
+        "long_range_ms": su["long_range_ms"], "initialize_ms": su["initialize_ms"],
+        "precision": prec}
 
     batch = serve = None
     if rank == 0 and world == 1 and not custom and not c3:
@@ -386,6 +517,14 @@ def run_gpu(args, rank, world, local):
             batch = run_batch_screen(local)
         if not args.no_serve:
             serve = run_served(local)
+
+    refcuda = None
+    if rank == 0 and world == 1 and not custom and not args.no_reference_cuda:
+        refcuda = reference_cuda(inp, xvk, maxstep=30 if c3 else None)
+        if "ms_per_iter" in refcuda:
+            refcuda["vs_this_fp64_ms_per_iter"] = (refcuda["ms_per_iter"] / fp64["ms_per_iter"]
+                                                   if fp64 else None)
+            refcuda["vs_this_mixed_ms_per_iter"] = refcuda["ms_per_iter"] / ms_iter
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and not custom and not c3:
@@ -412,40 +551,54 @@ def run_gpu(args, rank, world, local):
                        f"PROFILING CASE (not the headline): {args.grid}^3 grid, "
                        f"{args.atoms} atoms, NaCl water, KH, AN2",
                        "precision": prec, "grid": 512 if c3 else args.grid, "sites": 4,
-                       "atoms": 12877 if c3 else args.atoms, "replicas": world,
+                       "atoms": atoms, "replicas": world,
+                       "timing": f"{reps} measurements of exactly {args.steps} steps "
+                                 f"({timed} steps, {ms:.0f} ms), each bracketed by barrier + "
+                                 "CUDA-event sync, max over ranks",
                        "l2": "inputs larger than L2 (>8 GB touched per iteration)"},
+            "steps_timed": timed, "timed_repeats": reps,
             "ms_per_iter": ms_iter,
-            "iters_to_converge": steps, "solve_status": status, "final_rms": rms,
-            "solves_per_s": world / e2e_s, "sfe_sc_kcal_per_mol": sfe_kcal,
-            "e2e": {"value": world * steps / e2e_s, "unit": "iter/s",
-                    "h2d_bytes_per_step": h2d / max(steps, 1),
-                    "d2h_bytes_per_step": d2h / max(steps, 1),
+            "iters_to_converge": last["steps"], "solve_status": last["status"],
+            "final_rms": last["rms"],
+            "solves_per_s": world / e2e_s, "sfe_sc_kcal_per_mol": last["sfe"],
+            "pmv_A3": pmv_a3(last["pmv"]),
+            "e2e": {"value": world * last["steps"] / e2e_s, "unit": "iter/s",
+                    "h2d_bytes_per_step": last["h2d"] / max(last["steps"], 1),
+                    "d2h_bytes_per_step": last["d2h"] / max(last["steps"], 1),
                     "solve_s": e2e_s, "solves_per_s": world / e2e_s,
                     "solves_timed": len(warm), "cold_solve_s": cold_s,
-                    "warm_solves_s": [w[0] for w in warm],
-                    "phases_s": phases},
-            "gpu_launches": kpi * args.steps,
+                    "warm_solves_s": [w["total"] for w in warm],
+                    "phases_s": last["phases"]},
+            "gpu_launches": kpi * timed,
             "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": ncu_traffic(name), "algorithmic_bytes": kbytes,
+                         "traffic": ncu_traffic(name), "algorithmic_bytes": alg,
+                         "bytes_count": (f"stage {stage} of A_iter = N b (n (14 + 3m) + 2)"
+                                         if stage else "this design's own count"),
+                         "design_bytes": kbytes, "design_frac": kbytes / (kms * 1e-3) / 1e9 / peak,
                          "launch_ms": kms,
-                         "iteration": {"algorithmic_bytes": iter_bytes,
-                                       "achieved_gbs": iter_bytes / (ms_iter * 1e-3) / 1e9,
-                                       "frac": iter_bytes / (ms_iter * 1e-3) / 1e9 / peak}},
-            "kernels": [{"name": n, "ms": m, "bytes": b, "gbs": b / (m * 1e-3) / 1e9}
-                        for n, m, b in prof],
+                         "iteration": {"algorithmic_bytes": sec8["iteration"],
+                                       "achieved_gbs": sec8["iteration"] / (ms_iter * 1e-3) / 1e9,
+                                       "frac": sec8["iteration"] / (ms_iter * 1e-3) / 1e9 / peak,
+                                       "bytes_count": f"A_iter = N b (n (14 + 3m) + 2), n 4, "
+                                                      f"b {b}, m {m}",
+                                       "design_bytes": iter_bytes,
+                                       "design_frac": iter_bytes / (ms_iter * 1e-3) / 1e9 / peak}},
+            "kernels": [{"name": n_, "ms": m_, "bytes": b_, "gbs": b_ / (m_ * 1e-3) / 1e9}
+                        for n_, m_, b_ in prof],
             "fp64": fp64,
+            "mixed_vs_fp64": mvf,
+            "reference_cuda": refcuda,
+            "setup": setup,
             "batched_screen": batch,
             "served": serve,
             "xrism_solvents": xrism,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     shutil.rmtree(tmp, ignore_errors=True)
     shutil.rmtree(_SOLVENT_DIR, ignore_errors=True)
-    if dist:
-        dist.destroy_process_group()
 
 
 # ------------------------------------------------- batched and served solves
@@ -678,19 +831,37 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip the reference's own CUDA build")
     ap.add_argument("--solvent", choices=["configuration", "shipped"], default="configuration",
                     help="solvent tables: made by the 1D XRISM solve, or the shipped ones")
+    ap.add_argument("--print-launch", action="store_true",
+                    help="print the rank launch --gpus N > 1 would make, and exit")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1 and args.impl == "b200":
+        # no outer launcher: start one rank per GPU (replicas, 127.0.0.1)
+        argv = [os.path.abspath(__file__)] + [a for a in sys.argv[1:] if a != "--print-launch"]
+        if args.print_launch:
+            print(json.dumps({"nproc": args.gpus, "argv": argv}))
+            return 0
+        return replicas.launch(args.gpus, argv)
+    if args.print_launch:
+        print(json.dumps({"nproc": 1, "argv": [os.path.abspath(__file__)] + sys.argv[1:]}))
+        return 0
     rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         run_reference(args, rank, world)
-    else:
-        run_gpu(args, rank, world, local)
+        return 0
+    group = replicas.Group("nccl" if world > 1 else "none")
+    try:
+        run_gpu(args, group)
+    finally:
+        group.close()
+    return 0
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

@@ -154,6 +154,14 @@ int r3d_device_bytes(const r3d_ctx *ctx, unsigned long long *bytes);
 int r3d_iter_timing(const r3d_ctx *ctx, double *ms_per_iter,
                     int *kernels_per_iter);
 
+/* Times of the last r3d_initialize, ms: [0] the grid potentials (LJ and
+ * real-space Coulomb pair sums, cal_LJ.cu / cal_Coulomb.cu's real-space
+ * part), [1] the k-space Coulomb sum (cal_Coulomb.cu's fk), [2] the
+ * long-range h term, all CUDA-event times, and [3] the whole initialize
+ * (host clock, shells and uploads included).  No counterpart in the
+ * reference beyond its -DTEST timers (initialize.cu). */
+int r3d_setup_timing(const r3d_ctx *ctx, double *ms);
+
 /* Advance the solve by exactly `nsteps` iterations (graph replays, no
  * convergence polling; converged or diverged solves do no further work) and
  * return their CUDA-event time in *ms.  No counterpart in the reference: the
@@ -226,18 +234,22 @@ int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
 
 /* No counterpart in the reference.  r3d_fft3d (FP64) for callers that
  * cannot allocate device memory: code running while another framework owns
- * the device's memory pool, real-time loops that must not enter the
- * allocator, or work recorded once and replayed.  d_in / d_out are the
- * caller's device buffers, in the layouts of r3d_fft3d; the only working
- * storage is one fixed array of R3D_NOALLOC_SCRATCH_BYTES that every GPU
- * loading this library holds until the process exits.  Grids with
- * nx/2*ny*nz above (R3D_NOALLOC_SCRATCH_BYTES - 16384) / 16 points (about
- * 2.1 million: 160^3) are rejected with R3D_EBUDGET.  All calls on a device share the array: calls
- * that overlap on the GPU race and must be serialised by the caller.  The
- * first call on each device looks up the array's address; make it before
- * any stream capture.  stream may be NULL (the default stream); the call
- * returns after its work on that stream has finished.  Errors are reported
- * by r3d_last_error(NULL). */
+ * the device's memory pool, and real-time loops that must not enter the
+ * allocator.  d_in / d_out are the caller's device buffers, in the layouts
+ * of r3d_fft3d; the only working storage is one fixed array of
+ * R3D_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
+ * the process exits.  Grids with nx/2*ny*nz above
+ * (R3D_NOALLOC_SCRATCH_BYTES - 16384) / 16 points (about 2.1 million:
+ * 160^3) are rejected with R3D_EBUDGET.  All calls on a device share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller.  The first call on each device looks up the array's address (under
+ * a lock, so concurrent first calls from several host threads are safe); make
+ * it before any stream capture.  stream may be NULL (the default stream);
+ * the work is ordered after what the caller queued on that stream, and the
+ * call returns after it has finished.  The caller's current device is
+ * restored on return.  A CUDA error already pending in the process is
+ * reported (R3D_ECUDA) and left pending.  Errors are reported by
+ * r3d_last_error(NULL). */
 #define R3D_NOALLOC_SCRATCH_BYTES (32u << 20)
 int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
                       int dir, const double *d_in, double *d_out, void *stream);

@@ -3,9 +3,16 @@
 # at one rank for sm_100a, straight from its sources under the reference
 # tree, against the single-rank mpi.h beside this script.  Output goes to
 # oracle/_ref/ only (git-ignored; the binary travels to the GPU machine).
-# Usage: oracle/ref/build_ref.sh [/root/reference]
+# Usage: oracle/ref/build_ref.sh REFERENCE_TREE
+#   (or R3D_REFERENCE_SRC=REFERENCE_TREE oracle/ref/build_ref.sh), where
+#   REFERENCE_TREE is the directory that holds src-cuda-mpi/.
 set -euo pipefail
-REF=${1:-/root/reference}/src-cuda-mpi
+TREE=${1:-${R3D_REFERENCE_SRC:-}}
+if [ -z "$TREE" ]; then
+  echo "usage: $0 REFERENCE_TREE (the directory holding src-cuda-mpi/)" >&2
+  exit 2
+fi
+REF=$TREE/src-cuda-mpi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT=$HERE/../_ref
 OBJ=$OUT/obj

@@ -5,6 +5,7 @@ import os
 import shutil
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -58,3 +59,26 @@ def refcase(tmp_path_factory, solvents):
         raise KeyError(case)
 
     return make
+
+
+KCAL = 4184.0  # J per kcal
+A3_PER_LMOL = 1e-27 * 6.02214076e23  # 1 A^3 per molecule in L/mol (6.02e-4)
+PMV_TOL = 0.1 * A3_PER_LMOL  # the 0.1 A^3 bar, in the .xmu's L/mol
+
+
+def assert_xmu_fp64(got, ref):
+    """FP64 bar on the numbers of an .xmu (output_xmu.cu's order): every
+    free-energy number (J/mol) within 1e-6 kcal/mol, PMV (L/mol, third from
+    the end) within 0.1 A^3 on its own, the pressure to 1e-9 relative."""
+    assert len(got) == len(ref)
+    pmv = len(ref) - 3
+    rest = [i for i in range(len(ref)) if i != pmv]
+    np.testing.assert_allclose(np.take(got, rest), np.take(ref, rest), rtol=1e-9, atol=1e-6 * KCAL)
+    assert abs(got[pmv] - ref[pmv]) <= PMV_TOL, (got[pmv], ref[pmv])
+
+
+def assert_xmu_mixed(got, ref):
+    """Mixed-precision bar: SFE_SC (the first number) within 0.01 kcal/mol,
+    PMV within 0.1 A^3."""
+    assert abs(got[0] - ref[0]) <= 0.01 * KCAL, ("SFE kcal/mol", (got[0] - ref[0]) / KCAL)
+    assert abs(got[-3] - ref[-3]) <= PMV_TOL, ("PMV A^3", (got[-3] - ref[-3]) / A3_PER_LMOL)

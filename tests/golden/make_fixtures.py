@@ -2,7 +2,7 @@
 outputs into tests/golden/ (gzip-compressed) so the tests run without the
 reference tree.  Run once in a checkout that has the reference mounted:
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py REFERENCE_TREE
 """
 import gzip
 import os
@@ -45,4 +45,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    tree = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("R3D_REFERENCE_SRC", "")
+    if not tree:
+        sys.exit("usage: make_fixtures.py REFERENCE_TREE (or set R3D_REFERENCE_SRC)")
+    main(tree)

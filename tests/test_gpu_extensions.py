@@ -14,8 +14,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "oracle")
 CASES = sorted(f[:-5] for f in os.listdir(GOLD) if f.endswith(".json"))
-KCAL = 4184.0
-A3_PER_LMOL = 1e-27 * 6.02214076e23 * 1e3
+from conftest import assert_xmu_fp64, assert_xmu_mixed  # noqa: E402
 
 
 def _numbers(text):
@@ -56,8 +55,7 @@ def test_fp64_matches_oracle(refcase, case, tmp_path):
     s.output(str(out))
     ref = _numbers(open(os.path.join(GOLD, case + ".xmu")).read())
     got = _numbers(out.read_text())
-    assert len(got) == len(ref)
-    np.testing.assert_allclose(got, ref, rtol=1e-9, atol=1e-6 * KCAL)
+    assert_xmu_fp64(got, ref)
     gz = np.load(os.path.join(GOLD, case + "_guv.npz"))
     g = s.get("g").reshape(len(gz["sum"]), -1)
     np.testing.assert_allclose(g[:, gz["idx"]], gz["g"], rtol=1e-8, atol=1e-9)
@@ -72,5 +70,4 @@ def test_mixed_within_tolerance(refcase, case, tmp_path):
     s.output(str(out))
     ref = _numbers(open(os.path.join(GOLD, case + ".xmu")).read())
     got = _numbers(out.read_text())
-    assert abs(got[0] - ref[0]) <= 0.01 * KCAL      # SFE_SC (total), J/mol
-    assert abs(got[-3] - ref[-3]) <= 0.1 * A3_PER_LMOL  # PMV, L/mol
+    assert_xmu_mixed(got, ref)

@@ -13,8 +13,7 @@ import oracle as O
 
 pytestmark = pytest.mark.gpu
 GOLD_REF = os.path.join(os.path.dirname(__file__), "golden", "ref")
-KCAL = 4184.0
-A3_PER_LMOL = 1e-27 * 6.02214076e23 * 1e3  # 1 A^3 per molecule in L/mol
+from conftest import A3_PER_LMOL, KCAL, PMV_TOL, assert_xmu_fp64, assert_xmu_mixed  # noqa: E402
 
 
 @pytest.fixture(scope="module")
@@ -31,20 +30,30 @@ def _meta(case):
     return json.load(open(os.path.join(GOLD_REF, case + ".json")))
 
 
-@pytest.mark.parametrize("shape", [(8, 12, 16), (16, 8, 20), (12, 12, 12), (24, 10, 32)])
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("mixed", 2e-5)])
-def test_fft_forward_matches_oracle(R, shape, prec, tol):
-    """The closed-form shifted DFT for every even n; the oracle (= the
-    reference's fft3d.cu) agrees with it only when every n = 0 mod 4, since
-    the reference drops the constant phase e^{-i pi n/2} of each axis."""
-    from test_oracle import _direct_shifted_dft
-    rng = np.random.default_rng(5)
+def _dft1(v, length):
+    """1D shifted DFT: sum_i v_i e^{-i k_j r_i}, r = (i - n/2) dr,
+    k = 2 pi (j - n/2 + 1/2) / L (the per-axis factor of fft3d.cu)."""
+    n = len(v)
+    r = (np.arange(n) - n // 2) * (length / n)
+    k = 2 * np.pi * (np.arange(n) - n / 2 + 0.5) / length
+    return np.exp(-1j * np.outer(k, r)) @ v
+
+
+@pytest.mark.parametrize("shape", [(8, 512, 512), (16, 16, 1024), (512, 8, 64)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("mixed", 3e-5)])
+def test_fft_length_512_separable(R, shape, prec, tol):
+    """The 256- and 512-point engines (x rows of 512 and 1024 reals: packed
+    256/512-point complex transforms; y and z columns of 512) on a separable
+    grid f = a(x) b(y) c(z), whose shifted transform is the product of three
+    1D transforms: F = dv A(k_x) B(k_y) C(k_z)."""
+    rng = np.random.default_rng(17)
     nz, ny, nx = shape
-    box = (nx * 0.5, ny * 0.45, nz * 0.55)
-    f = rng.standard_normal(shape)
-    ref = _direct_shifted_dft(f, box)[:, :, 0::2]  # kept k_x indices 2p
-    if all(n % 4 == 0 for n in shape):
-        np.testing.assert_allclose(O.fft3d(f, box, -1)[:, :, 0::2], ref, atol=1e-11 * np.abs(ref).max())
+    box = (nx * 0.5, ny * 0.5, nz * 0.5)
+    a, b, c = rng.standard_normal(nx), rng.standard_normal(ny), rng.standard_normal(nz)
+    f = c[:, None, None] * b[None, :, None] * a[None, None, :]
+    dv = box[0] * box[1] * box[2] / f.size
+    A, B, C = _dft1(a, box[0])[0::2], _dft1(b, box[1]), _dft1(c, box[2])
+    ref = dv * C[:, None, None] * B[None, :, None] * A[None, None, :]
     got = R.fft3d(f, box, -1, precision=prec)
     scale = np.abs(ref).max()
     np.testing.assert_allclose(got, ref, atol=tol * scale)
@@ -87,8 +96,11 @@ def test_one_evaluation_matches_oracle(R, refcase):
         np.testing.assert_allclose(s.get("t"), o.get("t"), atol=1e-10)
 
 
-@pytest.mark.parametrize("case", ["s64kh", "s_rect", "c1", "s64nacl", "test1"])
+@pytest.mark.parametrize("case", ["s64kh", "s_rect", "c1", "s64nacl", "test1", "c2"])
 def test_fp64_solve_matches_reference(R, refcase, case, tmp_path):
+    """c2 is the headline configuration (256^3, 2000-atom globule, 0.2 M NaCl,
+    KH, AN2 2 0.6 0.2), solved by the same 256-point engine instances the
+    benchmark times, against the reference's own 240-step run."""
     inp, xvk = refcase(case)
     meta = _meta(case)
     s = _solver(R, inp, xvk)
@@ -99,9 +111,7 @@ def test_fp64_solve_matches_reference(R, refcase, case, tmp_path):
     s.output(str(out))
     ref = _xmu_numbers(open(os.path.join(GOLD_REF, case + ".xmu")).read())
     got = _xmu_numbers(out.read_text())
-    assert len(got) == len(ref)
-    # SFE terms in J/mol: 1e-6 kcal/mol; PMV in L/mol; pressure is input-only
-    np.testing.assert_allclose(got, ref, rtol=1e-9, atol=1e-6 * KCAL)
+    assert_xmu_fp64(got, ref)
     gp = os.path.join(GOLD_REF, case + "_guv.npz")
     if os.path.exists(gp):
         g = np.load(gp)
@@ -116,8 +126,11 @@ def test_divergence_detected(R, refcase):
     assert status == "diverged" and steps == 2
 
 
-@pytest.mark.parametrize("case", ["s64kh", "c1", "s64nacl"])
+@pytest.mark.parametrize("case", ["s64kh", "c1", "s64nacl", "c2"])
 def test_mixed_precision_within_tolerance(R, refcase, case, tmp_path):
+    """Mixed path against the reference's FP64 run: SFE_SC (the first
+    number) within 0.01 kcal/mol, PMV (third from the end) within 0.1 A^3.
+    c2 is the headline 256^3 configuration."""
     inp, xvk = refcase(case)
     s = _solver(R, inp, xvk, prec="mixed")
     steps, rms, status = s.iterate()
@@ -126,10 +139,7 @@ def test_mixed_precision_within_tolerance(R, refcase, case, tmp_path):
     s.output(str(out))
     ref = _xmu_numbers(open(os.path.join(GOLD_REF, case + ".xmu")).read())
     got = _xmu_numbers(out.read_text())
-    sfe = [i for i, l in enumerate(open(os.path.join(GOLD_REF, case + ".xmu")).read().split("\n"))]
-    # first number is SFE_SC (total), PMV is the third-to-last
-    assert abs(got[0] - ref[0]) <= 0.01 * KCAL
-    assert abs(got[-3] - ref[-3]) <= 0.1 * A3_PER_LMOL
+    assert_xmu_mixed(got, ref)
 
 
 def test_mixed_maxstep_results_are_of_the_last_evaluation(R, refcase):
