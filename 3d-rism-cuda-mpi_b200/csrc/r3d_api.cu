@@ -77,6 +77,24 @@ int tma_occupancy(int which, int L, size_t smem);
 template <typename P>
 void tma_allow_smem_all();
 size_t ct_smem_ixb(int L, int PC, size_t csz, size_t rsz, size_t tsz);
+// register-pass Stockham y/z passes (r3d_passes_sr.cu)
+size_t sr_smem_y(int L, int PC, size_t csz);
+size_t sr_smem_z(int L, int PC, int ns, size_t csz);
+bool sr_length_supported(int L);
+template <typename P>
+bool sr_launch_fy(int L, int dir, Batch b, int grid, size_t smem, cudaStream_t s);
+template <typename P>
+bool sr_launch_zoz(int L, int ns, bool ozreg, Batch b, int grid, size_t smem, cudaStream_t s);
+template <typename P>
+int sr_pc_y_of();
+template <typename P>
+int sr_pc_z_of(int L, int ns);
+int sr_pc_x_of(int L);
+size_t sr_smem_x(int L, int PC, size_t csz);
+template <typename P>
+bool sr_launch_fx(int L, Batch b, int grid, size_t smem, cudaStream_t s);
+template <typename P>
+bool sr_launch_ix(int L, Batch b, int grid, size_t smem, cudaStream_t s, int per);
 template <typename P>
 void launch_fwd_x(Batch, int, size_t, cudaStream_t, int, const void *);
 template <typename P>
@@ -179,9 +197,18 @@ struct Geo {
   size_t smxw = 0;
   // the iteration's y and z passes on the tensor copy engine (yz_tma = 0:
   // the tile-per-CTA kernels): CTAs per solve, tiles per CTA, stages, smem
+  // (yz_tma also carries the chosen y/z variant: 3 and 4 are the register-
+  // pass Stockham y and z passes, with the OZ on registers / as a pass of
+  // its own; yz_sr = 1 where those kernels cover the lengths and sites)
   int yz_tma = 0, fyt_pc = 0, fyt_ctas = 0, fyt_per = 1, fyt_nst = 0, zt_pc = 0, zt_ctas = 0,
       zt_per = 1, zt_nst = 0;
   size_t smfyt = 0, smzt = 0;
+  int yz_sr = 0, fys_ctas = 0, zs_ctas = 0;
+  size_t smfys = 0, smzs = 0;
+  // the iteration's FX / IX on the Stockham engine (fxs_pc / ixs_pc = 0: not used;
+  // x variant 4): rows per tile, CTAs (FX one tile each; IX ixs_per tiles)
+  int fxs_pc = 0, ixs_pc = 0, fxs_ctas = 0, ixs_ctas = 0, ixs_per = 1;
+  size_t smxs = 0;
   size_t smx = 0, smy = 0, smz = 0;
 };
 
@@ -626,6 +653,33 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
       g.zt_ctas = (tz + g.zt_per - 1) / g.zt_per;
     }
   }
+  g.fxs_pc = g.ixs_pc = 0;
+  if (c->opts.device >= 0 && sr_length_supported(d.hx)) {  // Stockham x passes
+    const int pc = sr_pc_x_of(d.hx);
+    const size_t sm = sr_smem_x(d.hx, pc, cs);
+    if (pc > 0 && rowsN % pc == 0 && sm <= kSmemMax) {
+      g.fxs_pc = g.ixs_pc = pc;
+      g.smxs = sm;
+      g.fxs_ctas = d.n * (rowsN / pc);
+      g.ixs_ctas = std::min(g.fxs_ctas, 4 * kNumSM);
+      g.ixs_per = (g.fxs_ctas + g.ixs_ctas - 1) / g.ixs_ctas;
+      g.ixs_ctas = (g.fxs_ctas + g.ixs_per - 1) / g.ixs_per;
+    }
+  }
+  g.yz_sr = 0;
+  if (c->opts.device >= 0 && sr_length_supported(d.ny) && sr_length_supported(d.nz) &&
+      d.n >= 1 && d.n <= 4) {  // register-pass Stockham y and z passes
+    const int pcy = fp64 ? sr_pc_y_of<P64>() : sr_pc_y_of<PMix>();
+    const int pcz = fp64 ? sr_pc_z_of<P64>(d.nz, d.n) : sr_pc_z_of<PMix>(d.nz, d.n);
+    const size_t smy = sr_smem_y(d.ny, pcy, cs), smz = sr_smem_z(d.nz, pcz, d.n, cs);
+    if (pcz > 0 && d.hx % pcy == 0 && d.hx % pcz == 0 && smy <= kSmemMax && smz <= kSmemMax) {
+      g.yz_sr = 1;
+      g.fys_ctas = d.n * d.nz * (d.hx / pcy);
+      g.zs_ctas = d.ny * (d.hx / pcz);
+      g.smfys = smy;
+      g.smzs = smz;
+    }
+  }
   // mixers: one chunk of mix_chunk() elements per CTA; ANM dots: one full
   // wave of a grid-stride reduction
   const long long niv = (long long)d.n * d.Ns;
@@ -664,6 +718,7 @@ static bool ixb_config(int device, const Desc &d, bool fp64, int pcb, Geo &g) {
 template <typename P>
 static void pass_fx(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode,
                     const void *src) {
+  if (mode == 1 && g.fxs_pc && sr_launch_fx<P>(d.hx, b, g.fxs_ctas, g.smxs, s)) return;
   if (mode == 1 && g.fxw_pc && ct_launch_xw<P>(0, d.hx, g.fxw_pc, b, g.fxw_ctas, g.smxw, s))
     return;
   if (mode == 1 && g.fxb_pc &&
@@ -685,6 +740,7 @@ static void pass_zoz(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int m
 }
 template <typename P>
 static void pass_ix(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode, void *dst) {
+  if (mode == 1 && g.ixs_pc && sr_launch_ix<P>(d.hx, b, g.ixs_ctas, g.smxs, s, g.ixs_per)) return;
   if (mode == 1 && g.ixw_pc && ct_launch_xw<P>(1, d.hx, g.ixw_pc, b, g.ixw_ctas, g.smxw, s))
     return;
   if (mode == 1 && g.ixb_pc &&
@@ -698,12 +754,16 @@ static void pass_ix(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mo
 // else the tile-per-CTA kernels.
 template <typename P>
 static void pass_fy_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int dir) {
-  if (g.yz_tma && tma_launch_fy<P>(d.ny, dir, b, g.fyt_ctas, g.smfyt, s, g.fyt_per, g.fyt_nst))
+  if (g.yz_tma >= 3 && sr_launch_fy<P>(d.ny, dir, b, g.fys_ctas, g.smfys, s)) return;
+  if ((g.yz_tma == 1 || g.yz_tma == 2) &&
+      tma_launch_fy<P>(d.ny, dir, b, g.fyt_ctas, g.smfyt, s, g.fyt_per, g.fyt_nst))
     return;
   pass_fy<P>(d, g, b, s, dir, 1);
 }
 template <typename P>
 static void pass_zoz_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s) {
+  if (g.yz_tma >= 3 && sr_launch_zoz<P>(d.nz, d.n, g.yz_tma == 3, b, g.zs_ctas, g.smzs, s))
+    return;
   if (g.yz_tma == 2 && tma_launch_zoz<P>(d.nz, b, g.zt_ctas, g.smzt, s, g.zt_per, g.zt_nst))
     return;
   if (g.yz_tma == 1 && ct_launch_zoz<P>(d.nz, d.ct_z, b, g.tiles_z, g.smz, s, 1 | 2)) return;
@@ -712,17 +772,18 @@ static void pass_zoz_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s) 
 
 // CTAs of the iteration's IX (each writes one row of the partials k_reduce sums)
 static int iter_ix_ctas(const Geo &g) {
-  return g.ixw_pc ? g.ixw_ctas : g.ixb_pc ? g.ixb_ctas : g.ix_ctas;
+  return g.ixs_pc ? g.ixs_ctas : g.ixw_pc ? g.ixw_ctas : g.ixb_pc ? g.ixb_ctas : g.ix_ctas;
 }
 // rows of partials the iteration's IX may need, whichever variant runs
 static int max_ix_ctas(const Geo &g) {
-  return std::max(std::max(std::max(g.ix_ctas, g.ixb_pc ? g.ixb_ctas : 0),
-                           g.ixw_pc ? g.ixw_ctas : 0),
-                  g.ixh_ctas);
+  return std::max(std::max(std::max(std::max(g.ix_ctas, g.ixb_pc ? g.ixb_ctas : 0),
+                                    g.ixw_pc ? g.ixw_ctas : 0),
+                           g.ixh_ctas),
+                  g.ixs_pc ? g.ixs_ctas : 0);
 }
 // CTAs of the iteration's FX
 static int iter_fx_ctas(const Geo &g) {
-  return g.fxw_pc ? g.fxw_ctas : g.fxb_pc ? g.fxb_ctas : g.tiles_x;
+  return g.fxs_pc ? g.fxs_ctas : g.fxw_pc ? g.fxw_ctas : g.fxb_pc ? g.fxb_ctas : g.tiles_x;
 }
 
 // Launch prefixes of ns solves that share one geometry (a device int block):
@@ -736,9 +797,10 @@ static int pf_off(int ns, int k) {
 static int pf_len(int ns) { return PF_IXC * (ns + 1) + 2 * ns; }
 static std::vector<int> make_prefix(const Geo &g, int ns) {
   std::vector<int> v(pf_len(ns));
-  const int per[6] = {iter_fx_ctas(g), g.yz_tma ? g.fyt_ctas : g.tiles_y,
-                      g.yz_tma == 2 ? g.zt_ctas : g.tiles_z, iter_ix_ctas(g), g.mix_ctas,
-                      g.dot_ctas};
+  const int per[6] = {iter_fx_ctas(g),
+                      g.yz_tma >= 3 ? g.fys_ctas : g.yz_tma ? g.fyt_ctas : g.tiles_y,
+                      g.yz_tma >= 3 ? g.zs_ctas : g.yz_tma == 2 ? g.zt_ctas : g.tiles_z,
+                      iter_ix_ctas(g), g.mix_ctas, g.dot_ctas};
   for (int k = 0; k < 6; ++k)
     for (int i = 0; i <= ns; ++i) v[pf_off(ns, k) + i] = i * per[k];
   for (int i = 0; i < ns; ++i) {
@@ -760,6 +822,10 @@ static Geo scaled(const Geo &g, int ns) {
   s.ixw_ctas *= ns;
   s.fyt_ctas *= ns;
   s.zt_ctas *= ns;
+  s.fys_ctas *= ns;
+  s.zs_ctas *= ns;
+  s.fxs_ctas *= ns;
+  s.ixs_ctas *= ns;
   s.mix_ctas *= ns;
   s.dot_ctas *= ns;
   return s;
@@ -964,8 +1030,10 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
   b += (size_t)d.Nh * 4;           // kidx
   b += (size_t)nshell * n * n * R;
   size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
-  // mixer history (residuals, states; mixed AN2: FP32 state differences)
-  b += slots * n * N * (R + (c->mixer == MIX_AN2 && !c->fp64 ? R : T));
+  // mixer history (residuals, states; mixed: FP32 differences of states, and
+  // for ANM one more FP32 array)
+  b += slots * n * N * (R + (!c->fp64 ? R : T));
+  if (c->mixer == MIX_ANM && !c->fp64) b += n * N * R;
   b += (size_t)std::max(max_ix_ctas(c->geo), c->geo.dot_ctas) * kPartials * 8;
   b += (size_t)(c->prob.maxstep + 1) * 8 + sizeof(Ctl) + sizeof(Desc) + 4096;
   return b;
@@ -981,14 +1049,47 @@ static size_t plan_bytes(const r3d_ctx *c, const Desc &d, int nshell) {
 // iteration rewrites -- and the choice holds for the process.
 static std::mutex g_tune_mu;
 // per geometry: the FX and IX variant (0 one tile per CTA, 1 bulk-staged,
-// 2 warp tiles)
+// 2 warp tiles, 3 (IX) bulk-staged with half-size tiles)
 static std::map<std::array<int, 5>, std::array<int, 3>> g_tune;  // + y/z on TMA
+
+// The committed choice per geometry.  Results of a solve depend (in their
+// last bits, which the Anderson iteration amplifies over hundreds of steps)
+// on the variant: each one sums the residual and its dots in its own order.
+// So the variant is a fixed function of the geometry -- this table, filled
+// from timings taken on a B200 with R3D_AUTOTUNE=1 (which times every
+// candidate and prints the row), else the rule in tune_rule -- and a solve
+// gives the same iterations and results on every box and every run.
+struct TuneRow {
+  int nx, ny, nz, n, fp64;
+  int fx, ix, yz;
+};
+static const TuneRow kTuneTable[] = {
+#include "r3d_tune_table.inc"
+};
+
+// Variants for a geometry with no row in the table: bulk-staged x passes
+// where they exist (warp tiles for short rows), the copy-engine y passes
+// with the tile-per-CTA z pass where the engine covers the lengths.
+static std::array<int, 3> tune_rule(const Geo &g, const Desc &d) {
+  std::array<int, 3> u{0, 0, 0};
+  if (d.hx <= 32 && g.fxw_pc) u[0] = 2;
+  else if (g.fxb_pc) u[0] = 1;
+  if (d.hx <= 32 && g.ixw_pc) u[1] = 2;
+  else if (g.ixb_pc) u[1] = 1;
+  if (g.fxs_pc) u[0] = u[1] = 4;
+  if (g.yz_sr)
+    u[2] = 4;
+  else if (g.yz_tma)
+    u[2] = d.ct_z ? 1 : 2;
+  return u;
+}
 
 template <typename P>
 static int autotune_x(r3d_ctx *c) {
   Geo &g = c->geo;
   const Desc &d = c->desc;
-  if (!g.fxb_pc && !g.ixb_pc && !g.fxw_pc && !g.ixw_pc && !g.yz_tma) return R3D_OK;
+  if (!g.fxb_pc && !g.ixb_pc && !g.fxw_pc && !g.ixw_pc && !g.fxs_pc && !g.yz_tma && !g.yz_sr)
+    return R3D_OK;
   const std::array<int, 5> key{d.nx, d.ny, d.nz, d.n, c->fp64 ? 1 : 0};
   std::array<int, 3> use{0, 0, g.yz_tma};
   bool known = false;
@@ -996,13 +1097,32 @@ static int autotune_x(r3d_ctx *c) {
   // (diagnostics and the per-variant parity tests)
   if (const char *ev = getenv("R3D_X_VARIANT")) {
     const int k = std::atoi(ev);
-    const bool fx = k == 0 || (k == 1 && g.fxb_pc) || (k == 2 && g.fxw_pc);
-    const bool ix = k == 0 || ((k == 1 || k == 3) && g.ixb_pc) || (k == 2 && g.ixw_pc);
-    use = {fx ? std::min(k, 2) : 0, ix ? k : 0, g.yz_tma};
+    const bool fx = k == 0 || ((k == 1 || k == 3) && g.fxb_pc) || (k == 2 && g.fxw_pc) ||
+                    (k == 4 && g.fxs_pc);
+    const bool ix = k == 0 || ((k == 1 || k == 3) && g.ixb_pc) || (k == 2 && g.ixw_pc) ||
+                    (k == 4 && g.ixs_pc);
+    use = {fx ? (k == 3 ? 1 : k) : 0, ix ? k : 0, g.yz_tma};
     if (const char *ey = getenv("R3D_YZ_VARIANT")) {
       const int k = std::atoi(ey);
-      use[2] = (k == 1 && !d.ct_z) ? 0 : std::min(k, g.yz_tma);
+      use[2] = (k >= 3) ? (g.yz_sr ? std::min(k, 4) : 0)
+                        : (k == 1 && !d.ct_z) ? 0 : std::min(k, g.yz_tma);
     }
+    known = true;
+  } else if (!getenv("R3D_AUTOTUNE")) {  // the committed table, else the fixed rule
+    use = tune_rule(g, d);
+    for (const TuneRow &r : kTuneTable)
+      if (r.nx == d.nx && r.ny == d.ny && r.nz == d.nz && r.n == d.n && r.fp64 == (c->fp64 ? 1 : 0)) {
+        use = {r.fx, r.ix, r.yz};
+        break;
+      }
+    // a row naming a variant this geometry does not offer falls back to the rule
+    const bool ok = (use[0] == 0 || (use[0] == 1 && g.fxb_pc) || (use[0] == 2 && g.fxw_pc) ||
+                     (use[0] == 4 && g.fxs_pc)) &&
+                    (use[1] == 0 || ((use[1] == 1 || use[1] == 3) && g.ixb_pc) ||
+                     (use[1] == 2 && g.ixw_pc) || (use[1] == 4 && g.ixs_pc)) &&
+                    (use[2] >= 3 ? (g.yz_sr && use[2] <= 4)
+                                 : (use[2] <= g.yz_tma && !(use[2] == 1 && !d.ct_z)));
+    if (!ok) use = tune_rule(g, d);
     known = true;
   } else {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1017,6 +1137,7 @@ static int autotune_x(r3d_ctx *c) {
     Geo o = g;
     if (k != 1) o.fxb_pc = o.ixb_pc = 0;
     if (k != 2) o.fxw_pc = o.ixw_pc = 0;
+    if (k != 4) o.fxs_pc = o.ixs_pc = 0;
     return o;
   };
   if (!known) {
@@ -1027,10 +1148,11 @@ static int autotune_x(r3d_ctx *c) {
     const bool has_half = g.ixb_pc >= 2 &&
                           ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, half) &&
                           half.ixb_ctas <= c->npart;
-    CK(cudaMalloc((void **)&pf, 22 * sizeof(int)));
-    const int pre[22] = {0, d.tiles_x, 0, g.fxb_ctas, 0, g.fxw_ctas, 0, g.ix_ctas,
+    CK(cudaMalloc((void **)&pf, 30 * sizeof(int)));
+    const int pre[30] = {0, d.tiles_x, 0, g.fxb_ctas, 0, g.fxw_ctas, 0, g.ix_ctas,
                          0, g.ixb_ctas, 0, g.ixw_ctas, 0, g.tiles_y, 0, g.tiles_z,
-                         0, g.fyt_ctas, 0, g.zt_ctas, 0, half.ixb_ctas};
+                         0, g.fyt_ctas, 0, g.zt_ctas, 0, half.ixb_ctas, 0, g.fys_ctas,
+                         0, g.zs_ctas, 0, g.fxs_ctas, 0, g.ixs_ctas};
     CK(copy_h2d(c, pf, pre, sizeof(pre), s));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -1038,7 +1160,7 @@ static int autotune_x(r3d_ctx *c) {
     auto time = [&](auto &&launch) {
       launch();
       cudaEventRecord(e0, s);
-      for (int i = 0; i < 3; ++i) launch();
+      for (int i = 0; i < 10; ++i) launch();
       cudaEventRecord(e1, s);
       cudaEventSynchronize(e1);
       float ms = 0;
@@ -1046,18 +1168,34 @@ static int autotune_x(r3d_ctx *c) {
       return ms;
     };
     float best[2] = {0, 0};
+    std::string report;  // candidate times, us per launch
+    auto note = [&](const char *what, int k, float ms) {
+      report += " " + std::string(what) + std::to_string(k) + "=" +
+                std::to_string((int)(ms * 100.0f)) ;  // 10 launches: ms*100 = us/launch
+    };
     for (int k = 0; k < 3; ++k) {
       const Geo o = only(k);
       const bool fx = k == 0 || (k == 1 ? g.fxb_pc : g.fxw_pc);
       const bool ix = k == 0 || (k == 1 ? g.ixb_pc : g.ixw_pc);
       if (fx) {
         const float ms = time([&] { pass_fx<P>(d, o, Batch{c->ddesc, pf + 2 * k, 1}, s, 1, nullptr); });
+        note("fx", k, ms);
         if (k == 0 || ms < best[0]) best[0] = ms, use[0] = k;
       }
       if (ix) {
         const float ms =
             time([&] { pass_ix<P>(d, o, Batch{c->ddesc, pf + 6 + 2 * k, 1}, s, 1, nullptr); });
+        note("ix", k, ms);
         if (k == 0 || ms < best[1]) best[1] = ms, use[1] = k;
+      }
+      if (k == 2 && g.fxs_pc) {  // variant 4: the Stockham engine
+        const Geo o4 = only(4);
+        const float mf = time([&] { pass_fx<P>(d, o4, Batch{c->ddesc, pf + 26, 1}, s, 1, nullptr); });
+        note("fx", 4, mf);
+        if (mf < best[0]) best[0] = mf, use[0] = 4;
+        const float mi = time([&] { pass_ix<P>(d, o4, Batch{c->ddesc, pf + 28, 1}, s, 1, nullptr); });
+        note("ix", 4, mi);
+        if (mi < best[1]) best[1] = mi, use[1] = 4;
       }
       if (k == 1 && has_half) {  // variant 3: bulk IX, half the rows per tile
         Geo o3 = only(1);
@@ -1066,22 +1204,27 @@ static int autotune_x(r3d_ctx *c) {
         o3.ixb_ctas = half.ixb_ctas;
         o3.ixb_per = half.ixb_per;
         const float ms = time([&] { pass_ix<P>(d, o3, Batch{c->ddesc, pf + 20, 1}, s, 1, nullptr); });
+        note("ix", 3, ms);
         if (ms < best[1]) best[1] = ms, use[1] = 3;
       }
     }
-    if (g.yz_tma) {  // the y/z trio: tile-per-CTA, copy-engine y, copy-engine y and z
+    if (g.yz_tma || g.yz_sr) {  // the y/z trio: tile-per-CTA, copy-engine y, copy-engine
+                                // y and z, register-pass Stockham (OZ on registers / shared)
       float best2 = 0;
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < 5; ++k) {
         if (k == 1 && !d.ct_z) continue;
+        if ((k == 1 || k == 2) && !g.yz_tma) continue;
+        if (k >= 3 && !g.yz_sr) continue;
         Geo o = g;
         o.yz_tma = k;
-        const Batch by{c->ddesc, pf + (k ? 16 : 12), 1},
-            bz{c->ddesc, pf + (k == 2 ? 18 : 14), 1};
+        const Batch by{c->ddesc, pf + (k >= 3 ? 22 : k ? 16 : 12), 1},
+            bz{c->ddesc, pf + (k >= 3 ? 24 : k == 2 ? 18 : 14), 1};
         const float ms = time([&] {
           pass_fy_iter<P>(d, o, by, s, -1);
           pass_zoz_iter<P>(d, o, bz, s);
           pass_fy_iter<P>(d, o, by, s, 1);
         });
+        note("yz", k, ms);
         if (k == 0 || ms < best2) best2 = ms, use[2] = k;
       }
     }
@@ -1090,11 +1233,15 @@ static int autotune_x(r3d_ctx *c) {
     cudaError_t e = cudaGetLastError();
     cudaFree(pf);
     if (e != cudaSuccess) return fail(c, R3D_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    std::fprintf(stderr, "r3d-tune row: {%d, %d, %d, %d, %d, %d, %d, %d},  // us:%s\n", d.nx,
+                 d.ny, d.nz, d.n, c->fp64 ? 1 : 0, use[0], use[1], use[2], report.c_str());
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = use;
   }
   if (use[0] != 1) g.fxb_pc = 0;
   if (use[0] != 2) g.fxw_pc = 0;
+  if (use[0] != 4) g.fxs_pc = 0;
+  if (use[1] != 4) g.ixs_pc = 0;
   if (use[1] == 3) {
     if (!(g.ixb_pc >= 2 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, g))) g.ixb_pc = 0;
   } else if (use[1] != 1) {
@@ -1129,11 +1276,14 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   // AN2: hist_a = t slots (T), hist_b = residual slots (R);
   // ANM: hist_a = residual ring (R), hist_b = z ring (T)
   const size_t slots = c->mixer == MIX_AN2 ? 2 : (size_t)c->history + 1;
-  // (mixed AN2: the t slots hold FP32 differences of successive t)
+  // (mixed AN2: the t slots hold FP32 differences of successive t; mixed
+  // ANM: hist_b holds FP32 differences of successive z and, after the ring,
+  // the last mix's t difference)
   const size_t ha = c->mixer == MIX_AN2 ? (c->fp64 ? sizeof(T) : sizeof(R)) : sizeof(R);
-  const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : sizeof(T);
+  const size_t hb = c->mixer == MIX_AN2 ? sizeof(R) : (c->fp64 ? sizeof(T) : sizeof(R));
+  const size_t bslots = slots + (c->mixer == MIX_ANM && !c->fp64 ? 1 : 0);
   if ((rc = dalloc(c, &c->hist_a, slots * n * N * ha))) return rc;
-  if ((rc = dalloc(c, &c->hist_b, slots * n * N * hb))) return rc;
+  if ((rc = dalloc(c, &c->hist_b, bslots * n * N * hb))) return rc;
   if ((rc = dalloc(c, &c->gq, n * N * sizeof(T)))) return rc;
   const int npart = std::max(max_ix_ctas(c->geo), c->geo.dot_ctas);
   if ((rc = dalloc(c, (void **)&c->partials, (size_t)npart * kPartials * 8))) return rc;
@@ -1144,7 +1294,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = dalloc(c, (void **)&c->ddesc, sizeof(Desc)))) return rc;
   if ((rc = dalloc(c, (void **)&c->dprefix, pf_len(1) * sizeof(int)))) return rc;
   CK(cudaMemsetAsync(c->hist_a, 0, slots * n * N * ha, s));
-  CK(cudaMemsetAsync(c->hist_b, 0, slots * n * N * hb, s));
+  CK(cudaMemsetAsync(c->hist_b, 0, bslots * n * N * hb, s));
   CK(cudaMemsetAsync(c->res, 0, n * N * sizeof(R), s));
   CK(cudaMemsetAsync(c->u, 0, n * N * sizeof(R), s));
   CK(cudaMemsetAsync(c->t, 0, n * N * sizeof(T), s));
@@ -1190,6 +1340,11 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
   if ((rc = make_tmaps(c, d))) return rc;
   d.partial_base = 0;
   d.rmslog = rmslog;
+  // Test hook of the error path of the staged passes: R3D_WAIT_POLLS=k makes
+  // their bounded waits for staged copies give up after k polls, so that a
+  // solve fails with R3D_ECUDA and the device stays usable.
+  d.wait_polls = 0;
+  if (const char *ew = getenv("R3D_WAIT_POLLS")) d.wait_polls = std::atoi(ew);
 
   // chi shell table, scaled by 2/N (the unnormalised transforms' factor)
   d.cubic = st.cubic ? 1 : 0;
@@ -1435,6 +1590,7 @@ static void enqueue(r3d_ctx *c, int stage) {
 static int read_ctl(r3d_ctx *c, Ctl &h) {
   CK(copy_d2h(c, &h, c->ctl, sizeof(Ctl), c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (h.err & 2) return fail(c, R3D_ECUDA, "a kernel's index check failed (debug build)");
   if (h.err) return fail(c, R3D_ECUDA, "a kernel's bounded wait for a staged copy ran out");
   return R3D_OK;
 }
@@ -1597,7 +1753,11 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
           [&] { launch_reduce(c->ddesc, ixc, 1, 1, s); });
     timed("anm_coef", 0, [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, dotc, 1, s, 1); });
     const int m = std::min(h.hcount, c->history);
-    timed("mix_anm", n * N * (rs + ts + m * ts + rs + ts + ts),
+    // FP64: R_k, t_k, m z entries in; R_k, z_k, t out.  Mixed: R_k, t_k, the
+    // last t difference, R_{k-1}, m - 1 z differences in; R_k, the new z
+    // difference, the t difference and t out
+    timed("mix_anm", rs < ts ? n * N * (rs + ts + rs + rs + (m - 1) * rs + rs + rs + rs + ts)
+                             : n * N * (rs + ts + m * ts + rs + ts + ts),
           [&] { launch_anm<P>(bmx, c->geo.mix_ctas, c->ddesc, dotc, 1, s, 2); });
   }
   CK(cudaGetLastError());

@@ -27,8 +27,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 // Bounded wait for phase `parity` of `bar`; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+// polls <= 0: the default limit (2^22 polls, far beyond any copy's latency).
+constexpr int kWaitPolls = 1 << 22;
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int polls = kWaitPolls) {
+  const int limit = polls > 0 ? polls : kWaitPolls;
+  for (int it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"

@@ -10,6 +10,22 @@
 
 namespace r3d {
 
+// Debug builds (-DR3D_DEBUG_BOUNDS, the library's `debug` target): the
+// iteration kernels check the index of each global access against its
+// array's extent; a failed check sets bit 2 of the solve's error word and
+// skips the access, and the host reports R3D_ECUDA.  Release builds compile
+// the checks away.
+#ifdef R3D_DEBUG_BOUNDS
+__device__ __forceinline__ bool r3d_in_bounds(int *err, long long i, long long n) {
+  if (i >= 0 && i < n) return true;
+  atomicOr(err, 2);
+  return false;
+}
+#define R3D_IN(d, i, n) r3d_in_bounds(&(d).ctl->err, (long long)(i), (long long)(n))
+#else
+#define R3D_IN(d, i, n) true
+#endif
+
 // ------------------------------------------------------------------ helpers
 struct Batch {
   const Desc *d;       // [ns]

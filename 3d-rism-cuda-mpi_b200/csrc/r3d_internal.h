@@ -170,6 +170,10 @@ struct Desc {
   Tmap tm_y, tm_z;
   int tma_pc_y, tma_pc_z;
   const int *yrev;  // [ny]: ky index of each digit-reversed y row of w
+  // polls of a staged pass's bounded wait for its copies before it gives up
+  // (sets the error word); <= 0: the default, far beyond any copy's latency.
+  // Set smaller only to exercise that error path (R3D_WAIT_POLLS).
+  int wait_polls;
 };
 
 constexpr int kPartials = 1 + 5 * kMaxSites;  // sum R^2 + per-site dots

@@ -541,6 +541,7 @@ __global__ void __launch_bounds__(kThreads)
   R *__restrict__ rp = (R *)d.hist_b;
   const bool picard = c->coef[2] < 0;
   const long long boff = (long long)c->coef[3] * niv;
+  if (!R3D_IN(d, boff, 2 * niv)) return;  // the ping-pong slot is 0 or 1
   const double s1 = c->coef[0], s2 = c->coef[1], m = d.m;
   T tv[kMixPer];
   R rv[kMixPer];
@@ -801,8 +802,86 @@ __global__ void __launch_bounds__(kThreads)
   T *__restrict__ t = (T *)d.t;
   const R *__restrict__ res = (const R *)d.res;
   R *__restrict__ f = (R *)d.hist_a;
-  T *__restrict__ zr = (T *)d.hist_b;
   const double beta = d.beta, w0 = c->coef[0];
+  if (!R3D_IN(d, head, d.history + 1) || !R3D_IN(d, m, d.history + 1)) return;
+#ifdef R3D_DEBUG_BOUNDS
+  for (int q = 0; q < m; ++q)
+    if (!R3D_IN(d, c->mix_slots[q], d.history + 1)) return;
+#endif
+  if constexpr (sizeof(R) < sizeof(T)) {
+    // Mixed precision: the history of z_i = t_i + beta R_i is kept as FP32
+    // differences of successive entries, E_i = z_i - z_{i+1} (stored under
+    // entry i's slot), plus D = t_k - t_{k+1} of the last mix.  With w0 =
+    // 1 - sum alpha_i,
+    //   t_{k+1} = z_k + sum_i alpha_i (z_i - z_k) = z_k + sum_b C_b E_{k-b},
+    // C_b = sum of alpha over the entries of age >= b; the newest difference
+    // E_{k-1} = D_{k-1} + beta (R_{k-1} - R_k) is formed here.  Against FP64
+    // copies of z this reads 4 instead of 8 bytes per history entry.
+    R *__restrict__ er = (R *)d.hist_b;
+    R *__restrict__ dp = er + (long long)(d.history + 1) * niv;  // D of the last mix
+    double cb[kMaxHistory];
+    {
+      double run = 0;
+      for (int q = m - 1; q >= 0; --q) {
+        run += c->coef[1 + q];
+        cb[q] = run;  // C_{q+1}: entries of age q+1 and older
+      }
+    }
+    double acc[kMixPer], tk[kMixPer];
+    R rk[kMixPer];
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) {
+        rk[k] = res[i];
+        tk[k] = (double)t[i];
+        acc[k] = tk[k] + beta * (double)rk[k];
+      }
+    }
+    if (m >= 1) {
+      const long long s0 = (long long)c->mix_slots[0] * niv;
+#pragma unroll
+      for (int k = 0; k < kMixPer; ++k) {
+        const long long i = i0 + k * kThreads;
+        if (i < niv) {
+          const double e1 = (double)dp[i] + beta * ((double)f[s0 + i] - (double)rk[k]);
+          er[s0 + i] = (R)e1;
+          acc[k] += cb[0] * e1;
+        }
+      }
+    }
+    int q = 1;
+    for (; q + 1 < m; q += 2) {  // two history slots per step
+      const R *__restrict__ ea = er + (long long)c->mix_slots[q] * niv;
+      const R *__restrict__ eb = er + (long long)c->mix_slots[q + 1] * niv;
+      const double ca = cb[q], cc = cb[q + 1];
+#pragma unroll
+      for (int k = 0; k < kMixPer; ++k) {
+        const long long i = i0 + k * kThreads;
+        if (i < niv) acc[k] += ca * (double)ea[i] + cc * (double)eb[i];
+      }
+    }
+    if (q < m) {
+      const R *__restrict__ eq = er + (long long)c->mix_slots[q] * niv;
+      const double cq = cb[q];
+#pragma unroll
+      for (int k = 0; k < kMixPer; ++k) {
+        const long long i = i0 + k * kThreads;
+        if (i < niv) acc[k] += cq * (double)eq[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kMixPer; ++k) {
+      const long long i = i0 + k * kThreads;
+      if (i < niv) {
+        f[(long long)head * niv + i] = rk[k];
+        dp[i] = (R)(tk[k] - acc[k]);
+        t[i] = (T)acc[k];
+      }
+    }
+    return;
+  }
+  T *__restrict__ zr = (T *)d.hist_b;
   double acc[kMixPer], rk[kMixPer], zk[kMixPer];
 #pragma unroll
   for (int k = 0; k < kMixPer; ++k) {
@@ -1395,6 +1474,8 @@ void ct_allow_smem_all();
 
 template <typename P>
 void tma_allow_smem_all();
+template <typename P>
+void sr_allow_smem_all();
 void kernels_set_smem(bool fp64, size_t maxbytes) {
   static bool ct_done[2] = {false, false};
   if (fp64)
@@ -1405,9 +1486,11 @@ void kernels_set_smem(bool fp64, size_t maxbytes) {
     if (fp64) {
       ct_allow_smem_all<P64>();
       tma_allow_smem_all<P64>();
+      sr_allow_smem_all<P64>();
     } else {
       ct_allow_smem_all<PMix>();
       tma_allow_smem_all<PMix>();
+      sr_allow_smem_all<PMix>();
     }
     ct_done[fp64] = true;
   }

@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
       const long long row = row0 + threadIdx.x;
       par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
     }
-    if (!mbar_wait(&bar[st], (phase >> st) & 1)) failed = true;
+    if (!mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls)) failed = true;
     phase ^= 1u << st;
     const char *sb = smem + BUF + st * St::bytes;
     const C *ws = (const C *)(sb + St::w);
@@ -688,7 +688,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const long long row = row0 + threadIdx.x;
       par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
     }
-    if (!mbar_wait(&bar[st], (phase >> st) & 1)) failed = true;
+    if (!mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls)) failed = true;
     phase ^= 1u << st;
     __syncthreads();  // par
     const char *sb = smem + BUF + st * St::bytes;

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kThreads)
   for (int s = 0; s < nst && s < count; ++s) pending |= 1u << s;
   for (int it = 0; it < count; ++it) {
     const int st = it % nst, tile = first + it;
-    const bool ok = mbar_wait(&bar[st], (phase >> st) & 1);
+    const bool ok = mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls);
     if (__syncthreads_or(!ok)) {
       tma_abort(d, bar, nst, pending, phase);
       return;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(kThreads)
   for (int it = 0; it < count; ++it) {
     const int st = it % nst, tile = first + it;
     const int pt = tile % ptiles, y = tile / ptiles;
-    const bool ok = mbar_wait(&bar[st], (phase >> st) & 1);
+    const bool ok = mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls);
     if (__syncthreads_or(!ok)) {
       tma_abort(d, bar, nst, pending, phase);
       return;

@@ -15,7 +15,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "librism3d_b200.so")
+# R3D_LIBRARY may name another build of the same C-ABI (the debug build,
+# lib/librism3d_b200_debug.so, with the kernels' index checks compiled in)
+LIB_PATH = os.environ.get("R3D_LIBRARY") or os.path.join(_HERE, "lib", "librism3d_b200.so")
 
 FP64, MIXED = 0, 1
 KH, HNC, PSE = 0, 1, 2

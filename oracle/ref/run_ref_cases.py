@@ -59,7 +59,8 @@ def deck(case, d):
         return case + ".inp"
     if case in ("c1", "c2", "c3"):
         _xvk("h2o_vv.xvk" if case == "c1" else "naclaq_vv.xvk", d)
-        p = synthetic.config(case, d, outlist="mg" if case == "c1" else "m")
+        # c1 and c2 also write g (.guv) for the 1e-8 g pin; c3 only the .xmu
+        p = synthetic.config(case, d, outlist="mg" if case in ("c1", "c2") else "m")
         return os.path.basename(p)
     # post-solve per-atom integrals: forces (.gra), energies (.euv) and the
     # lambda derivatives of the LJ (-l) or Coulomb (-e) scaling

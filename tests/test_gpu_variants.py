@@ -1,6 +1,7 @@
 """Every implementation of the iteration's x passes (one tile per CTA,
-bulk-copy staged, warp tiles, bulk-copy staged with half-size tiles; the
-autotuner picks one per geometry) and of its y/z passes solves to the
+bulk-copy staged, warp tiles, bulk-copy staged with half-size tiles, the
+register-pass Stockham engine; a committed table picks one per geometry) and
+of its y/z passes solves to the
 reference's results (or the oracle's, for grids the reference cannot run):
 same steps (within 1), .xmu within 1e-6 kcal/mol."""
 import os
@@ -30,7 +31,7 @@ def _numbers(text):
     return [float(x) for x in re.findall(r"=\s*(-?[0-9.]+(?:e[-+]?\d+)?)", text)]
 
 
-@pytest.mark.parametrize("variant", ["0", "1", "2", "3"])
+@pytest.mark.parametrize("variant", ["0", "1", "2", "3", "4"])
 @pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96"])
 def test_x_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, variant, case):
     import rism3d as R
@@ -53,11 +54,13 @@ def test_x_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, varian
         s.close()
 
 
-@pytest.mark.parametrize("yz", ["0", "1", "2"])
+@pytest.mark.parametrize("yz", ["0", "1", "2", "3", "4"])
 @pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96"])
 def test_yz_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, yz, case):
-    """The y/z passes on the tensor copy engine (digit-reversed ky layout of
-    the spectrum between them) against the tile-per-CTA kernels."""
+    """Every y/z trio against the reference: 0 tile-per-CTA kernels, 1 and 2
+    the tensor copy engine (digit-reversed ky layout of the spectrum between
+    the passes), 3 and 4 the register-pass Stockham kernels (natural order;
+    the OZ on registers, or as a shared-memory pass of its own)."""
     import rism3d as R
     monkeypatch.setenv("R3D_X_VARIANT", "0")
     monkeypatch.setenv("R3D_YZ_VARIANT", yz)
