@@ -59,6 +59,12 @@ template <typename P>
 bool ct_launch_ixb(int, int, Batch, int, size_t, cudaStream_t, int);
 template <typename P>
 bool ct_launch_fxb(int, int, Batch, int, size_t, cudaStream_t, int);
+template <typename P>
+bool ct_launch_mfx(int L, Batch b, int grid, size_t smem, cudaStream_t s, int per, int allow_mix);
+template <typename P>
+int ct_occupancy_mfx(int L, size_t smem);
+size_t ct_smem_mfx(int L, int PC);
+int ct_mfx_pc(int L);
 size_t ct_smem_fxb(int L, int PC, size_t csz, size_t rsz, size_t tsz);
 template <typename P>
 int ct_occupancy_bulk(int which, int L, int PC, size_t smem);
@@ -209,6 +215,11 @@ struct Geo {
   // x variant 4): rows per tile, CTAs (FX one tile each; IX ixs_per tiles)
   int fxs_pc = 0, ixs_pc = 0, fxs_ctas = 0, ixs_ctas = 0, ixs_per = 1;
   size_t smxs = 0;
+  // the mixed path's AN2 mix fused into the iteration's FX (mfx_avail: the
+  // kernel covers the geometry; mfx: in use -- the iteration then launches
+  // no separate mix kernel)
+  int mfx_avail = 0, mfx = 0, mfx_ctas = 0, mfx_per = 1;
+  size_t smmfx = 0;
   size_t smx = 0, smy = 0, smz = 0;
 };
 
@@ -230,6 +241,14 @@ struct r3d_ctx {
        *fk = nullptr, *chi = nullptr, *lr = nullptr, *gq = nullptr, *hist_a = nullptr,
        *hist_b = nullptr, *cref = nullptr, *chi64 = nullptr;
   double next_refresh = 0;  // mixed path: refresh when rms drops below this
+  // the refresh schedule: the first at RMS refresh_first, then every time the
+  // RMS has dropped by refresh_factor (R3D_REFRESH="first,factor" overrides).
+  // Measured on the 256^3 NaCl deck: refreshing from 3e-2 on by factors of
+  // 0.3 keeps the FP32 transforms' share of c small enough that the mixed
+  // solve takes the FP64 solve's iterations (260-282 over the pass variants,
+  // against 264-350 with refreshes at 1e-3 and 1e-5 only), for ~9 refreshes
+  // of a few ms each.
+  double refresh_first = 3e-2, refresh_factor = 0.3;
   // mixed path: the refresh's FP64 geometry and work buffer, kept from the
   // first refresh on (the FP64 path refreshes once, at setup, and frees it)
   bool rplanned = false;
@@ -319,6 +338,13 @@ extern "C" int r3d_create(const r3d_opts *opts, r3d_ctx **out) {
   }
   c->fp64 = c->opts.precision == R3D_FP64;
   c->rsz = c->fp64 ? 8 : 4;
+  if (const char *er = getenv("R3D_REFRESH")) {
+    double a = 0, f = 0;
+    if (std::sscanf(er, "%lf,%lf", &a, &f) == 2 && a > 0 && f > 0 && f < 1) {
+      c->refresh_first = a;
+      c->refresh_factor = f;
+    }
+  }
   if (c->opts.device < 0) {  // host-only context: loaders, planning, no GPU
     *out = c;
     return R3D_OK;
@@ -653,6 +679,23 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
       g.zt_ctas = (tz + g.zt_per - 1) / g.zt_per;
     }
   }
+  g.mfx_avail = g.mfx = 0;
+  if (!fp64 && c->mixer == MIX_AN2 && d.ct_x && c->opts.device >= 0) {  // mix-fused FX
+    const int pc = ct_mfx_pc(d.hx);
+    const size_t sm = ct_smem_mfx(d.hx, pc);
+    if (rowsN % pc == 0 && sm <= kSmemMax) {
+      kernels_set_smem(false, kSmemMax);
+      const int per_sm = ct_occupancy_mfx<PMix>(d.hx, sm);
+      if (per_sm > 0) {
+        const int tiles = d.n * (rowsN / pc);
+        g.mfx_avail = 1;
+        g.smmfx = sm;
+        g.mfx_ctas = std::min(tiles, kNumSM * per_sm);
+        g.mfx_per = (tiles + g.mfx_ctas - 1) / g.mfx_ctas;
+        g.mfx_ctas = (tiles + g.mfx_per - 1) / g.mfx_per;
+      }
+    }
+  }
   g.fxs_pc = g.ixs_pc = 0;
   if (c->opts.device >= 0 && sr_length_supported(d.hx)) {  // Stockham x passes
     const int pc = sr_pc_x_of(d.hx);
@@ -715,9 +758,13 @@ static bool ixb_config(int device, const Desc &d, bool fp64, int pcb, Geo &g) {
 // ---------------------------------------------------------- pass dispatch
 // Each pass runs on the compile-time engine when plan_geo chose it for this
 // descriptor (d.ct_* != 0), else on the runtime-length engine.
+// mode 1 with the mix-fused FX in use: allow_mix = 1 applies the mix the
+// last reduce requested (the iteration's graph), 0 is a plain FX (calculate)
 template <typename P>
 static void pass_fx(const Desc &d, const Geo &g, Batch b, cudaStream_t s, int mode,
-                    const void *src) {
+                    const void *src, int allow_mix = 0) {
+  if (mode == 1 && g.mfx && ct_launch_mfx<P>(d.hx, b, g.mfx_ctas, g.smmfx, s, g.mfx_per, allow_mix))
+    return;
   if (mode == 1 && g.fxs_pc && sr_launch_fx<P>(d.hx, b, g.fxs_ctas, g.smxs, s)) return;
   if (mode == 1 && g.fxw_pc && ct_launch_xw<P>(0, d.hx, g.fxw_pc, b, g.fxw_ctas, g.smxw, s))
     return;
@@ -783,7 +830,8 @@ static int max_ix_ctas(const Geo &g) {
 }
 // CTAs of the iteration's FX
 static int iter_fx_ctas(const Geo &g) {
-  return g.fxs_pc ? g.fxs_ctas : g.fxw_pc ? g.fxw_ctas : g.fxb_pc ? g.fxb_ctas : g.tiles_x;
+  return g.mfx ? g.mfx_ctas : g.fxs_pc ? g.fxs_ctas : g.fxw_pc ? g.fxw_ctas
+                                      : g.fxb_pc ? g.fxb_ctas : g.tiles_x;
 }
 
 // Launch prefixes of ns solves that share one geometry (a device int block):
@@ -826,6 +874,7 @@ static Geo scaled(const Geo &g, int ns) {
   s.zs_ctas *= ns;
   s.fxs_ctas *= ns;
   s.ixs_ctas *= ns;
+  s.mfx_ctas *= ns;
   s.mix_ctas *= ns;
   s.dot_ctas *= ns;
   return s;
@@ -1062,21 +1111,23 @@ static std::map<std::array<int, 5>, std::array<int, 3>> g_tune;  // + y/z on TMA
 struct TuneRow {
   int nx, ny, nz, n, fp64;
   int fx, ix, yz;
+  int mfx;  // mixed AN2: 1 = the mix fused into FX (when the geometry has it)
 };
 static const TuneRow kTuneTable[] = {
 #include "r3d_tune_table.inc"
 };
 
-// Variants for a geometry with no row in the table: bulk-staged x passes
-// where they exist (warp tiles for short rows), the copy-engine y passes
-// with the tile-per-CTA z pass where the engine covers the lengths.
+// Variants for a geometry with no row in the table (what the measured rows
+// favour): bulk-staged x passes for rows of 128 or more complex points, else
+// one tile per CTA (warp tiles for the shortest rows); the register-pass
+// Stockham y and z passes where they cover the lengths and sites, else the
+// copy-engine y passes with the tile-per-CTA z pass.
 static std::array<int, 3> tune_rule(const Geo &g, const Desc &d) {
   std::array<int, 3> u{0, 0, 0};
   if (d.hx <= 32 && g.fxw_pc) u[0] = 2;
-  else if (g.fxb_pc) u[0] = 1;
+  else if (d.hx >= 128 && g.fxb_pc) u[0] = 1;
   if (d.hx <= 32 && g.ixw_pc) u[1] = 2;
-  else if (g.ixb_pc) u[1] = 1;
-  if (g.fxs_pc) u[0] = u[1] = 4;
+  else if (d.hx >= 128 && g.ixb_pc) u[1] = 1;
   if (g.yz_sr)
     u[2] = 4;
   else if (g.yz_tma)
@@ -1110,9 +1161,11 @@ static int autotune_x(r3d_ctx *c) {
     known = true;
   } else if (!getenv("R3D_AUTOTUNE")) {  // the committed table, else the fixed rule
     use = tune_rule(g, d);
+    g.mfx = g.mfx_avail;  // the rule: fused where available
     for (const TuneRow &r : kTuneTable)
       if (r.nx == d.nx && r.ny == d.ny && r.nz == d.nz && r.n == d.n && r.fp64 == (c->fp64 ? 1 : 0)) {
         use = {r.fx, r.ix, r.yz};
+        g.mfx = g.mfx_avail && r.mfx;
         break;
       }
     // a row naming a variant this geometry does not offer falls back to the rule
@@ -1238,10 +1291,12 @@ static int autotune_x(r3d_ctx *c) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = use;
   }
+  if (!getenv("R3D_X_VARIANT") && getenv("R3D_AUTOTUNE")) g.mfx = g.mfx_avail;
   if (use[0] != 1) g.fxb_pc = 0;
   if (use[0] != 2) g.fxw_pc = 0;
   if (use[0] != 4) g.fxs_pc = 0;
   if (use[1] != 4) g.ixs_pc = 0;
+  if (const char *em = getenv("R3D_MFX")) g.mfx = g.mfx_avail && std::atoi(em) != 0;
   if (use[1] == 3) {
     if (!(g.ixb_pc >= 2 && ixb_config(c->opts.device, d, c->fp64, g.ixb_pc / 2, g))) g.ixb_pc = 0;
   } else if (use[1] != 1) {
@@ -1553,7 +1608,7 @@ static int enqueue_group(const Group &G, cudaStream_t s, int stage) {
   const int *ixc = G.dpf + pf_off(ns, PF_IXC), *dotc = G.dpf + pf_off(ns, PF_DOTC);
   int k = 0;
   if (stage != 2) {
-    pass_fx<P>(d, g, B(PF_X), s, 1, nullptr);
+    pass_fx<P>(d, g, B(PF_X), s, 1, nullptr, stage == 0 ? 1 : 0);
     pass_fy_iter<P>(d, g, B(PF_Y), s, -1);
     pass_zoz_iter<P>(d, g, B(PF_Z), s);
     pass_fy_iter<P>(d, g, B(PF_Y), s, 1);
@@ -1571,8 +1626,12 @@ static int enqueue_group(const Group &G, cudaStream_t s, int stage) {
   }
   if (stage != 1) {
     if (G.mixer == MIX_AN2) {
-      launch_mix_an2<P>(B(PF_MIX), g.mix_ctas, s);
-      ++k;
+      // (with the mix-fused FX the iteration's mix runs at the start of the
+      // next iteration's FX)
+      if (!(stage == 0 && g.mfx)) {
+        launch_mix_an2<P>(B(PF_MIX), g.mix_ctas, s);
+        ++k;
+      }
     } else {
       launch_anm<P>(B(PF_MIX), g.mix_ctas, G.ddescs, dotc, ns, s, 1);
       launch_anm<P>(B(PF_MIX), g.mix_ctas, G.ddescs, dotc, ns, s, 2);
@@ -1726,9 +1785,18 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
     return R3D_OK;
   };
   const double cref = d.cref ? rs : 0.0;
-  // FX: t, u, c_ref in; w (half spectrum: one grid value per voxel) and g out
-  timed("fwd_x", n * N * (ts + rs + cref + rs + ts),
-        [&] { pass_fx<P>(d, c->geo, bx, s, 1, nullptr); });
+  if (c->geo.mfx) {
+    // the mix fused into FX: t, u, c_ref, and (mixing) the residual and the
+    // four history rows in; t, its two history entries, g and w out
+    const bool mixing = h.mix_flag != 0, picard = h.coef[2] < 0;
+    const double mixb = !mixing ? 0.0 : picard ? rs + ts + 2 * rs : 5 * rs + ts + 2 * rs;
+    timed("mix_fx", n * N * (ts + rs + cref + rs + ts + mixb),
+          [&] { pass_fx<P>(d, c->geo, bx, s, 1, nullptr, 1); });
+  } else {
+    // FX: t, u, c_ref in; w (half spectrum: one grid value per voxel) and g out
+    timed("fwd_x", n * N * (ts + rs + cref + rs + ts),
+          [&] { pass_fx<P>(d, c->geo, bx, s, 1, nullptr); });
+  }
   timed("fft_y_fwd", n * N * 2 * rs,
         [&] { pass_fy_iter<P>(d, c->geo, by, s, -1); });
   timed("zoz", n * N * 2 * rs + (double)d.Nh * 4,
@@ -1743,9 +1811,10 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
           [&] { launch_reduce(c->ddesc, ixc, 1, 1, s); });
     const bool picard = h.count_left > 0;
     const bool diffs = rs < ts;  // mixed: FP32 t differences in the slots
-    timed("mix_an2", picard ? n * N * (diffs ? 2 * ts + 3 * rs : 3 * ts + 2 * rs)
-                            : n * N * (diffs ? 2 * ts + 7 * rs : 5 * ts + 4 * rs),
-          [&] { launch_mix_an2<P>(bmx, c->geo.mix_ctas, s); });
+    if (!c->geo.mfx)
+      timed("mix_an2", picard ? n * N * (diffs ? 2 * ts + 3 * rs : 3 * ts + 2 * rs)
+                              : n * N * (diffs ? 2 * ts + 7 * rs : 5 * ts + 4 * rs),
+            [&] { launch_mix_an2<P>(bmx, c->geo.mix_ctas, s); });
   } else {
     timed("anm_dots", n * N * rs * (h.hcount + 1),
           [&] { launch_anm<P>(bdot, c->geo.dot_ctas, c->ddesc, dotc, 1, s, 0); });
@@ -1835,7 +1904,7 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
   Ctl h{};
   int printed = 0;
   std::vector<double> log;
-  c->next_refresh = 1e-3;
+  c->next_refresh = c->refresh_first;
   const int ksave = c->prob.ksave;  // iterate.cu:63-70: save t every ksave steps / at the end
   for (;;) {
     // chunks end on the multiples of ksave, where t is saved
@@ -1849,7 +1918,7 @@ extern "C" int r3d_iterate(r3d_ctx *c, int *steps, double *rms, int *status) {
     if (!c->fp64 && h.status == RUNNING && h.rms < c->next_refresh) {
       // mixed path: move the converged part of c into the FP64 reference
       if ((rc = refresh<PMix>(c, false))) return rc;
-      c->next_refresh *= 1e-2;
+      c->next_refresh *= c->refresh_factor;
     }
     if (c->opts.verbose && h.step > printed) {
       log.resize(h.step);
@@ -2547,7 +2616,7 @@ static int batch_run(r3d_batch *b, int *iterations, double *ms_out) {
   for (r3d_ctx *c : b->ctxs) {
     int rc = reset_mixer(c);
     if (rc) return bfail(rc, c->err);
-    c->next_refresh = 1e-3;
+    c->next_refresh = c->refresh_first;
   }
   if (b->dirty) {
     int rc = batch_build<P>(b);
@@ -2591,7 +2660,7 @@ static int batch_run(r3d_batch *b, int *iterations, double *ms_out) {
         // mixed path: move the converged part of c into the FP64 reference
         int rc = refresh<PMix>(c, false);
         if (rc) return bfail(rc, c->err);
-        c->next_refresh *= 1e-2;
+        c->next_refresh *= c->refresh_factor;
       }
     }
     if (!running || iters > maxstep + chunk) break;

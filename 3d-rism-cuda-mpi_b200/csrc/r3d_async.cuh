@@ -27,11 +27,26 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 // Bounded wait for phase `parity` of `bar`; false when the limit ran out.
-// polls <= 0: the default limit (2^22 polls, far beyond any copy's latency).
+// polls <= 0: the default, 2^22 polls of try_wait (far beyond any copy's
+// latency).  polls > 0 (the test hook of the error path): that many
+// non-blocking test_wait polls, which a copy issued just before the wait
+// does not satisfy.
 constexpr int kWaitPolls = 1 << 22;
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int polls = kWaitPolls) {
-  const int limit = polls > 0 ? polls : kWaitPolls;
-  for (int it = 0; it < limit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int polls = 0) {
+  if (polls > 0) {
+    for (int it = 0; it < polls; ++it) {
+      uint32_t done;
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+          " selp.u32 %0, 1, 0, p;\n}"
+          : "=r"(done)
+          : "r"(smem_u32(bar)), "r"(parity)
+          : "memory");
+      if (done) return true;
+    }
+    return false;
+  }
+  for (int it = 0; it < kWaitPolls; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"

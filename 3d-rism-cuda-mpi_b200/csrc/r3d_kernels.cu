@@ -487,7 +487,13 @@ __global__ void __launch_bounds__(kThreads)
       c->mix_flag = 0;
       return;
     }
-    if (c->step >= c->maxstep) c->status = MAXSTEP;  // still mixes this step
+    // The last allowed evaluation ends the solve without a mix: t stays the
+    // t of that evaluation, whose g and h the results are computed from.
+    if (c->step >= c->maxstep) {
+      c->status = MAXSTEP;
+      c->mix_flag = 0;
+      return;
+    }
   }
   c->mix_flag = 1;
   if (d.mixer == MIX_AN2) {

@@ -736,6 +736,193 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// -------------------------------------------- AN2 mix fused into FX
+// The mixed path's AN2 update of t (anderson_cuda.cu:1-22, with the t slots
+// as FP32 differences of successive t, as k_mix_an2) fused with the next
+// evaluation's FX: t, the residual and the four history rows of a tile are
+// staged by the bulk copy engine together with u and c_ref; each element's
+// new t is formed, stored with its history entries, and goes straight into
+// the closure and the forward x transform.  Against the separate mix and FX
+// kernels this reads t once instead of twice and saves a launch.  The mix
+// requested by the previous iteration's reduce (mix_flag) is applied; the
+// first evaluation of a solve (mix_flag 0) is a plain FX.
+template <typename P, int L, int PC>
+struct MfxStage {
+  static constexpr int NX = 2 * L;
+  static constexpr size_t t = 0;  // FP64
+  static constexpr size_t u = t + (size_t)PC * NX * 8;
+  static constexpr size_t cref = u + (size_t)PC * NX * 4;
+  static constexpr size_t res = cref + (size_t)PC * NX * 4;
+  static constexpr size_t dn = res + (size_t)PC * NX * 4;   // newest t difference slot
+  static constexpr size_t dl = dn + (size_t)PC * NX * 4;    // the other one
+  static constexpr size_t r0 = dl + (size_t)PC * NX * 4;    // residual slots 0, 1
+  static constexpr size_t r1 = r0 + (size_t)PC * NX * 4;
+  static constexpr size_t bytes = r1 + (size_t)PC * NX * 4;
+};
+#if R3D_CT_FP64
+size_t ct_smem_mfx(int L, int PC) {
+  const size_t buf = ((8 * (size_t)L * (PC + 1) + 127) / 128) * 128;
+  return buf + 2 * (size_t)PC * 2 * L * (8 + 7 * 4);
+}
+#endif
+
+#if !R3D_CT_FP64
+template <int L, int PC>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_mfx_bulk(Batch b, int per, int allow_mix) {
+  using P = PMix;
+  using R = float;
+  using C = float2;
+  using St = MfxStage<P, L, PC>;
+  constexpr int LD = PC + 1, NX = 2 * L;
+  constexpr size_t BUF = ((sizeof(C) * (size_t)L * LD + 127) / 128) * 128;
+  extern __shared__ __align__(128) char smem[];
+  C *buf = (C *)smem;
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ int par[PC];
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  const Ctl *ctl = d.ctl;
+  if (ctl->status != RUNNING) return;
+  const int cta = blockIdx.x - b.prefix[si];
+  const int ny = d.ny;
+  const int tps = (d.ny * d.nz) / PC;
+  const int ntile = d.n * tps;
+  const int first = cta * per;
+  const int count = min(per, ntile - first);
+  if (count <= 0) return;
+  const bool mix = allow_mix && ctl->mix_flag != 0;
+  const bool picard = ctl->coef[2] < 0;
+  const long long niv = (long long)d.n * d.Ns;
+  const long long boff = (long long)ctl->coef[3] * niv, noff = niv - boff;
+  const double s1 = ctl->coef[0], s2 = ctl->coef[1], mm = d.m;
+  const bool old0 = boff == 0;  // slot 0 holds the older entry
+  const bool has_cref = d.cref != nullptr;
+  const C *pw = (const C *)d.pwx, *tw = (const C *)d.twx;
+  const uint32_t tbytes = PC * NX * 8, rbytes = PC * NX * 4;
+  const uint32_t stage_tx = tbytes + rbytes + (has_cref ? rbytes : 0) +
+                            (mix ? (picard ? 1 : 5) * rbytes : 0);
+  const Desc *dp = &d;
+  char *const stages = smem + BUF;
+  uint64_t *const bars = bar;
+  auto issue = [=](int tile, int st) {  // thread 0: the copies of one tile
+    const int v = tile / tps;
+    const long long base = (long long)v * dp->Ns + (long long)(tile % tps) * PC * NX;
+    char *sb = stages + st * St::bytes;
+    uint64_t *br = bars + st;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(br, stage_tx);
+    bulk_g2s(sb + St::t, (const double *)dp->t + base, tbytes, br);
+    bulk_g2s(sb + St::u, (const R *)dp->u + base, rbytes, br);
+    if (has_cref) bulk_g2s(sb + St::cref, (const R *)dp->cref + base, rbytes, br);
+    if (mix) {
+      bulk_g2s(sb + St::res, (const R *)dp->res + base, rbytes, br);
+      if (!picard) {
+        bulk_g2s(sb + St::dn, (const R *)dp->hist_a + noff + base, rbytes, br);
+        bulk_g2s(sb + St::dl, (const R *)dp->hist_a + boff + base, rbytes, br);
+        bulk_g2s(sb + St::r0, (const R *)dp->hist_b + base, rbytes, br);
+        bulk_g2s(sb + St::r1, (const R *)dp->hist_b + niv + base, rbytes, br);
+      }
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) issue(first, 0);
+  uint32_t phase = 0;
+  bool failed = false;
+  int stop = -1;
+  for (int it = 0; it < count; ++it) {
+    const int tile = first + it, st = it & 1;
+    const int v = tile / tps;
+    const long long row0 = (long long)(tile % tps) * PC;
+    if (threadIdx.x == 0 && it + 1 < count) issue(tile + 1, st ^ 1);
+    if (threadIdx.x < PC) {
+      const long long row = row0 + threadIdx.x;
+      par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
+    }
+    if (!mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls)) failed = true;
+    phase ^= 1u << st;
+    __syncthreads();  // par
+    const char *sb = smem + BUF + st * St::bytes;
+    const double *ts = (const double *)(sb + St::t);
+    const R *us = (const R *)(sb + St::u), *cs = (const R *)(sb + St::cref);
+    const R *rs = (const R *)(sb + St::res), *dns = (const R *)(sb + St::dn),
+            *dls = (const R *)(sb + St::dl), *r0s = (const R *)(sb + St::r0),
+            *r1s = (const R *)(sb + St::r1);
+    const long long gbase = (long long)v * d.Ns + row0 * NX;
+    double *tg = (double *)d.t + gbase;
+    R *ddg = (R *)d.hist_a + boff + gbase, *rpg = (R *)d.hist_b + boff + gbase;
+    double *gqg = (double *)d.gq + gbase;
+#pragma unroll 2
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, m = e % L;
+      double tv[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = r * NX + m + h * L;
+        double tt = ts[i];
+        if (mix) {
+          const double rr = rs[i];
+          double tn;
+          if (picard) {  // newdt0: t_{k+1} = t_k + R_k
+            tn = tt + rr;
+          } else {  // newdt
+            const double dnew = dns[i], dold = (double)dls[i] + dnew;
+            const double e0 = old0 ? dold : dnew, e1 = old0 ? dnew : dold;
+            const double rp0 = r0s[i], rp1 = r1s[i];
+            const double uu = tt + s1 * e0 + s2 * e1;
+            const double vv = tt + rr + s1 * (e0 + rp0 - rr) + s2 * (e1 + rp1 - rr);
+            tn = uu + mm * (vv - uu);
+          }
+          ddg[i] = (R)(tt - tn);
+          rpg[i] = (R)rr;
+          tg[i] = tn;
+          tt = tn;
+        }
+        tv[h] = tt;
+      }
+      // trm1mt on the short-range parts (calculate_cuda.cu:18-24)
+      const int i0 = r * NX + m, i1 = i0 + L;
+      const double g0 = closure_g<double>(d.clos, d.pse_n, -(double)us[i0] + tv[0]);
+      const double g1 = closure_g<double>(d.clos, d.pse_n, -(double)us[i1] + tv[1]);
+      gqg[i0] = g0;
+      gqg[i1] = g1;
+      double c0 = g0 - 1.0 - tv[0], c1 = g1 - 1.0 - tv[1];
+      if (has_cref) {
+        c0 -= (double)cs[i0];
+        c1 -= (double)cs[i1];
+      }
+      R f0 = (R)c0, f1 = (R)c1;
+      if ((m + par[r]) & 1) f0 = -f0;
+      if ((m + L + par[r]) & 1) f1 = -f1;
+      buf[digit_rev<L>(m) * LD + r] = cmul(C{f0, -f1}, pw[m]);
+    }
+    __syncthreads();
+    ct_fft_dit<L, PC, LD, -1>(buf, tw);
+    C *w = (C *)d.w + (long long)v * d.Nhs + row0 * L;
+#pragma unroll
+    for (int e = threadIdx.x; e < PC * L; e += kThreads) {
+      const int r = e / L, p = e % L;
+      w[(long long)r * L + p] = buf[p * LD + r];
+    }
+    if (__syncthreads_or(failed)) {  // buf, par and this stage are free again
+      stop = it;
+      break;
+    }
+  }
+  if (stop >= 0) {  // flag the solve, wait (bounded) for the copies in flight, give up
+    if (threadIdx.x == 0) atomicExch(&d.ctl->err, 1);
+    const int st = stop & 1;
+    mbar_wait(&bar[st], ((phase >> st) & 1) ^ 1);
+    if (stop + 1 < count) mbar_wait(&bar[st ^ 1], (phase >> (st ^ 1)) & 1);
+  }
+}
+#endif
+
 // ------------------------------------------------------- warp tiles
 // The iteration's x passes with one tile of PCW rows per warp: each warp
 // loads, transforms (warp-synchronous radix stages) and stores its own tile,
@@ -1069,6 +1256,42 @@ bool ct_launch_fxb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s
   return false;
 }
 
+// The mix-fused FX (mixed precision; false: no kernel for the length).
+// Rows per tile: 4 (2 for rows of 1024 reals).
+constexpr int mfx_pc(int L) { return L >= 512 ? 2 : 4; }
+template <typename P>
+bool ct_launch_mfx(int L, Batch b, int grid, size_t smem, cudaStream_t s, int per,
+                   int allow_mix) {
+#if !R3D_CT_FP64
+#define R3D_MFX(LL)                                                          \
+  if (L == LL) {                                                             \
+    k_mfx_bulk<LL, mfx_pc(LL)><<<grid, kThreads, smem, s>>>(b, per, allow_mix); \
+    return true;                                                             \
+  }
+  R3D_CT_LENGTHS(R3D_MFX)
+#undef R3D_MFX
+#endif
+  return false;
+}
+template <typename P>
+int ct_occupancy_mfx(int L, size_t smem) {
+  int nb = 0;
+#if !R3D_CT_FP64
+#define R3D_OMFX(LL)                                                                        \
+  if (L == LL) {                                                                            \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_mfx_bulk<LL, mfx_pc(LL)>, kThreads, \
+                                                  smem);                                    \
+    return nb;                                                                              \
+  }
+  R3D_CT_LENGTHS(R3D_OMFX)
+#undef R3D_OMFX
+#endif
+  return nb;
+}
+#if R3D_CT_FP64
+int ct_mfx_pc(int L) { return mfx_pc(L); }
+#endif
+
 // Resident CTAs per SM of the bulk-staged FX (which = 0) or IX (1) for
 // length L, PC rows per tile and `smem` dynamic bytes (0: not instantiated).
 template <typename P>
@@ -1181,6 +1404,11 @@ void ct_allow_smem_all() {
   }
   allow_smem(k_fx_warp<P, 256, 2>);
   allow_smem(k_fx_warp<P, 512, 2>);
+#if !R3D_CT_FP64
+#define R3D_AMFX(LL) allow_smem(k_mfx_bulk<LL, mfx_pc(LL)>);
+  R3D_CT_LENGTHS(R3D_AMFX)
+#undef R3D_AMFX
+#endif
   allow_smem(k_ix_warp<P, 256, 2>);
   allow_smem(k_ix_warp<P, 512, 2>);
 }
@@ -1192,6 +1420,8 @@ template bool ct_launch_zoz<PCT>(int, int, Batch, int, size_t, cudaStream_t, int
 template bool ct_launch_ix<PCT>(int, int, Batch, int, size_t, cudaStream_t, int, void *, int);
 template bool ct_launch_ixb<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
 template bool ct_launch_fxb<PCT>(int, int, Batch, int, size_t, cudaStream_t, int);
+template bool ct_launch_mfx<PCT>(int, Batch, int, size_t, cudaStream_t, int, int);
+template int ct_occupancy_mfx<PCT>(int, size_t);
 template int ct_occupancy_bulk<PCT>(int, int, int, size_t);
 template bool ct_launch_xw<PCT>(int, int, int, Batch, int, size_t, cudaStream_t);
 template int ct_occupancy_xw<PCT>(int, int, int, size_t);

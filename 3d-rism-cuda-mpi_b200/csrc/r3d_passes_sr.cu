@@ -417,6 +417,18 @@ __global__ void __launch_bounds__(kThreads) k_ix_sr(Batch b, int per) {
 }
 
 // --------------------------------------------------------------- z pass
+// Position of (site v, z, column p) in the z pass's shared tile: rows of PC
+// columns with one spare row after every 16, so that rows 16 apart (the
+// stride of a radix-16 pass's writes) fall on other banks.
+template <int L>
+__device__ __forceinline__ constexpr int sr_zrows() {
+  return L + L / 16 + 1;
+}
+template <int L, int PC>
+__device__ __forceinline__ int sr_zi(int v, int z, int p) {
+  return (v * sr_zrows<L>() + z + z / 16) * PC + p;
+}
+
 // One Stockham pass in place on the shared-memory tile [site][L][PC] of NS
 // sites: every thread reads and transforms all of its tasks, then (after a
 // barrier, since a pass writes other positions than it reads) writes them.
@@ -430,7 +442,7 @@ __device__ __forceinline__ void sr_tile_pass(C *buf, const C *tw) {
     if (T % NT == 0 || task < T) {
       const int p = task % PC, q = task / PC, j = q % (L / R), v = q / (L / R);
 #pragma unroll
-      for (int m = 0; m < R; ++m) a[k][m] = buf[(v * L + sr_in<L, R>(j, m)) * PC + p];
+      for (int m = 0; m < R; ++m) a[k][m] = buf[sr_zi<L, PC>(v, sr_in<L, R>(j, m), p)];
       sr_pass<L, R, NSs, DIR>(a[k], tw, j);
     }
   }
@@ -441,7 +453,7 @@ __device__ __forceinline__ void sr_tile_pass(C *buf, const C *tw) {
     if (T % NT == 0 || task < T) {
       const int p = task % PC, q = task / PC, j = q % (L / R), v = q / (L / R);
 #pragma unroll
-      for (int m = 0; m < R; ++m) buf[(v * L + sr_out<R, NSs>(j, m)) * PC + p] = a[k][m];
+      for (int m = 0; m < R; ++m) buf[sr_zi<L, PC>(v, sr_out<R, NSs>(j, m), p)] = a[k][m];
     }
   }
   __syncthreads();
@@ -553,8 +565,8 @@ __global__ void __launch_bounds__(NT, (OZREG || NT > 256) ? 1 : 2) k_zoz_sr(Batc
   constexpr int RL = pl.r[pl.n - 1];  // forward last radix = inverse first
   constexpr int NSL = L / RL;         // N of the forward last pass
   extern __shared__ __align__(16) char smem[];
-  C *buf = (C *)smem;  // [site][z][p]
-  C *tw = buf + NS * L * PC;
+  C *buf = (C *)smem;  // [site][z (padded)][p]
+  C *tw = buf + NS * sr_zrows<L>() * PC;
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
   if (d.ctl->status != RUNNING) return;
@@ -570,7 +582,7 @@ __global__ void __launch_bounds__(NT, (OZREG || NT > 256) ? 1 : 2) k_zoz_sr(Batc
   for (int e = threadIdx.x; e < L; e += NT) tw[e] = ((const C *)d.twz)[e];
   const long long ay = 2 * y - d.ny + 1;
   const long long gbase = (long long)y * hx + pt * PC;
-  auto at = [&](int v, int z, int p) -> C & { return buf[(v * L + z) * PC + p]; };
+  auto at = [&](int v, int z, int p) -> C & { return buf[sr_zi<L, PC>(v, z, p)]; };
 
   // forward pass 0: global -> registers -> shared (the loads of up to 16
   // values' worth of tasks are issued together: more loads in flight)
@@ -654,28 +666,55 @@ __global__ void __launch_bounds__(NT, (OZREG || NT > 256) ? 1 : 2) k_zoz_sr(Batc
     __syncthreads();
   } else {
     if constexpr (pl.n > 1) sr_tile_pass<L, RL, NSL, -1, NS, PC, NT>(buf, tw);
-    {  // OZ, in place: k_z and L - 1 - k_z (the same |k| shell) share one
-       // load of the shell's chi row, which is a gather from L2
-      constexpr int T = PC * (L / 2), K = (T + NT - 1) / NT;
+    {  // OZ, in place.  k_z and L - 1 - k_z (the same |k| shell) form a pair;
+       // NS lanes of a warp take one pair, lane q the output site q: it reads
+       // row q of the shell's chi matrix (the group reads the whole row
+       // block at once, a gather from L2 in NS * NS * 4 contiguous bytes),
+       // every site's input (shared-memory broadcast within the group) and
+       // writes its site's outputs after the group has read.
+      constexpr int G = 32 / NS, TP = PC * (L / 2), NW = NT / 32;
+      const int lane = threadIdx.x & 31, q = lane % NS, grp = lane / NS;
+      const bool lane_on = grp < G;
 #pragma unroll 1
-      for (int k = 0; k < K; ++k) {
-        const int task = threadIdx.x + k * NT;
-        if (T % NT == 0 || task < T) {
-          const int p = task % PC, kz = task / PC, kz2 = L - 1 - kz;
-          const R *ch = sr_chi_row<R>(d, 4 * (pt * PC + p) - d.nx + 1, ay, kz, kz * zs + gbase + p);
-          C c1[NS], c2[NS];
+      for (int base = (threadIdx.x >> 5) * G; base < TP; base += NW * G) {
+        const int pair = base + grp;
+        const bool on = lane_on && pair < TP;
+        const int p = pair % PC, kz = pair / PC, kz2 = L - 1 - kz;
+        R x[NS];
+        C c1[NS], c2[NS];
+        if (on) {
+          const R *ch = sr_chi_row<R>(d, 4 * (pt * PC + p) - d.nx + 1, ay, kz,
+                                      (long long)kz * zs + gbase + p) + q * NS;
+          if constexpr (NS == 4 && sizeof(R) == 4) {
+            const float4 v4 = *reinterpret_cast<const float4 *>(ch);
+            x[0] = v4.x, x[1] = v4.y, x[2] = v4.z, x[3] = v4.w;
+          } else if constexpr (NS == 2 && sizeof(R) == 4) {
+            const float2 v2 = *reinterpret_cast<const float2 *>(ch);
+            x[0] = v2.x, x[1] = v2.y;
+          } else {
 #pragma unroll
-          for (int v = 0; v < NS; ++v) {
-            c1[v] = at(v, kz, p);
-            c2[v] = at(v, kz2, p);
+            for (int b = 0; b < NS; ++b) x[b] = ch[b];
           }
-          sr_oz_apply2<R, NS>(c1, c2, ch);
 #pragma unroll
-          for (int v = 0; v < NS; ++v) {
-            at(v, kz, p) = c1[v];
-            at(v, kz2, p) = c2[v];
+          for (int b = 0; b < NS; ++b) {
+            c1[b] = at(b, kz, p);
+            c2[b] = at(b, kz2, p);
           }
         }
+        __syncwarp();
+        if (on) {
+          R h1r = 0, h1i = 0, h2r = 0, h2i = 0;
+#pragma unroll
+          for (int b = 0; b < NS; ++b) {
+            h1r += c1[b].x * x[b];
+            h1i += c1[b].y * x[b];
+            h2r += c2[b].x * x[b];
+            h2i += c2[b].y * x[b];
+          }
+          at(q, kz, p) = C{h1r, h1i};
+          at(q, kz2, p) = C{h2r, h2i};
+        }
+        __syncwarp();
       }
     }
     __syncthreads();
@@ -719,21 +758,23 @@ constexpr int sr_pc_z(int L, int ns) {
 }
 // threads of the z pass: register OZ: one OZ task (all sites) per thread,
 // 64..256; shared OZ: one task of the largest-radix pass per thread, 64..512
+// (a whole number of warps: the OZ pass deals pairs out by warp)
 template <typename P>
 constexpr int sr_threads_z(int L, int ns, bool ozreg) {
-  if (!ozreg) {
-    const int t = ns * sr_pc_z<P>(L, ns) * (L / sr_max_radix(L));
-    return t < 64 ? 64 : (t > 512 ? 512 : t);
-  }
-  const int t = sr_pc_z<P>(L, ns) * (L / sr_plan(L).r[sr_plan(L).n - 1]);
-  return t < 64 ? 64 : (t > 256 ? 256 : t);
+  int t = ozreg ? sr_pc_z<P>(L, ns) * (L / sr_plan(L).r[sr_plan(L).n - 1])
+                : ns * sr_pc_z<P>(L, ns) * (L / sr_max_radix(L));
+  t = (t + 31) / 32 * 32;
+  const int hi = ozreg ? 256 : 512;
+  return t < 64 ? 64 : (t > hi ? hi : t);
 }
 
 #define R3D_SR_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(72) X(80) X(96) X(128) X(144) X(160) X(192) X(256) X(512)
 
 #if R3D_CT_FP64
 size_t sr_smem_y(int L, int PC, size_t csz) { return csz * (size_t)L * (PC + 1); }
-size_t sr_smem_z(int L, int PC, int ns, size_t csz) { return csz * (size_t)L * (ns * PC + 1); }
+size_t sr_smem_z(int L, int PC, int ns, size_t csz) {
+  return csz * ((size_t)ns * (L + L / 16 + 1) * PC + L);
+}
 bool sr_length_supported(int L) { return sr_length_ok(L); }
 #endif
 

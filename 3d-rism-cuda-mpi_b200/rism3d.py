@@ -34,7 +34,7 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
            "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
-           "r3d_fft3d_noalloc", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
+           "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
            "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
            "r3d_server_destroy", "r3d_write_guv", "r3d_write_huv", "r3d_write_cuv",
@@ -120,6 +120,7 @@ def _load():
                                ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
         "r3d_fft3d_noalloc": [ci, ci, ci, ci, dp, ci, vp, vp, vp],
+        "r3d_slab_transform": [ci, ci, ci, ci, ci, vp, vp, vp],
         "r3d_batch_create": [ci, ctypes.POINTER(vp)],
         "r3d_batch_add": [vp, vp],
         "r3d_batch_iterate": [vp, ip, dp],

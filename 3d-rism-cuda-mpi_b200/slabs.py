@@ -1,0 +1,220 @@
+"""A grid split over several GPUs: the slab partition and the distributed
+shifted 3D transform (the reference's FFT3D over MPI ranks, fft3d.cu:81-163,
+with its decomposition of the grid over ranks, cell.cc:30-48).
+
+The reference cuts the grid in pencils over a 2D process grid and moves them
+with MPI_Alltoall between 1D cuFFT passes.  Here the x and y passes run on
+z-slabs (rank r owns the z-planes [z0_r, z0_r + nzl_r), all y and x) and the
+z pass on y-slabs (rank r owns the y-rows [y0_r, y0_r + nyl_r), all z): one
+all-to-all per direction moves the half spectrum between the two layouts.
+With one process per GPU the all-to-all is NCCL's over NVLink (torch.
+distributed); the stages run on the GPU through r3d_slab_transform.  The
+same driver runs on CPU ranks (gloo) with a numpy restatement of the stages,
+which is how the partition and the transposes are tested without GPUs.
+
+Layouts: a z-slab real grid [nzl][ny][nx]; the z-slab half spectrum
+[nzl][ny][hx] complex (hx = nx / 2); the y-slab half spectrum [nz][nyl][hx].
+Transform units as the iteration's passes: unnormalised, the constant phase
+dv C(k) of the full-grid seam left out.
+"""
+import ctypes
+
+import numpy as np
+
+
+class SlabPlan:
+    """z-slabs and y-slabs of an (nz, ny, nx) grid over `world` ranks.  Every
+    z-slab starts on an even plane (the checkerboard sign (-1)^(x+y+z) of the
+    x pass is taken on local z); extents differ by at most 2 (z) / 1 (y)."""
+
+    def __init__(self, nz, ny, nx, world):
+        if nx % 2 or nz % 2:
+            raise ValueError("nx and nz must be even")
+        if world < 1 or nz < 2 * world or ny < world:
+            raise ValueError("need nz >= 2 world and ny >= world")
+        self.nz, self.ny, self.nx, self.world = nz, ny, nx, world
+        self.hx = nx // 2
+        pairs = nz // 2  # z-planes in pairs: every slab starts on an even plane
+        zc = [pairs // world + (1 if r < pairs % world else 0) for r in range(world)]
+        self.z0 = [2 * sum(zc[:r]) for r in range(world)]
+        self.nzl = [2 * c for c in zc]
+        yc = [ny // world + (1 if r < ny % world else 0) for r in range(world)]
+        self.y0 = [sum(yc[:r]) for r in range(world)]
+        self.nyl = yc
+
+    def zslab(self, rank):
+        return slice(self.z0[rank], self.z0[rank] + self.nzl[rank])
+
+    def yslab(self, rank):
+        return slice(self.y0[rank], self.y0[rank] + self.nyl[rank])
+
+    # counts (complex elements) of the all-to-all from z-slabs to y-slabs
+    def send_counts_z2y(self, rank):
+        return [self.nzl[rank] * self.nyl[s] * self.hx for s in range(self.world)]
+
+    def recv_counts_z2y(self, rank):
+        return [self.nzl[s] * self.nyl[rank] * self.hx for s in range(self.world)]
+
+
+# ------------------------------------------------------------- transposes
+def pack_z2y(spec_z, plan):
+    """[nzl][ny][hx] -> the send buffer of the z-to-y all-to-all: for each
+    destination s, its y-rows of every local plane ([nzl][nyl_s][hx])."""
+    return np.concatenate([spec_z[:, plan.yslab(s), :].reshape(-1) for s in range(plan.world)])
+
+
+def unpack_z2y(recv, plan, rank):
+    """Receive buffer (from each source s: [nzl_s][nyl][hx]) -> [nz][nyl][hx]."""
+    out, off = [], 0
+    for s in range(plan.world):
+        n = plan.nzl[s] * plan.nyl[rank] * plan.hx
+        out.append(recv[off:off + n].reshape(plan.nzl[s], plan.nyl[rank], plan.hx))
+        off += n
+    return np.concatenate(out, axis=0)
+
+
+def pack_y2z(spec_y, plan):
+    """[nz][nyl][hx] -> the send buffer of the y-to-z all-to-all: for each
+    destination s, its z-planes of the local y-rows ([nzl_s][nyl][hx])."""
+    return np.concatenate([spec_y[plan.zslab(s)].reshape(-1) for s in range(plan.world)])
+
+
+def unpack_y2z(recv, plan, rank):
+    """Receive buffer (from each source s: [nzl][nyl_s][hx]) -> [nzl][ny][hx]."""
+    out, off = [], 0
+    for s in range(plan.world):
+        n = plan.nzl[rank] * plan.nyl[s] * plan.hx
+        out.append(recv[off:off + n].reshape(plan.nzl[rank], plan.nyl[s], plan.hx))
+        off += n
+    return np.concatenate(out, axis=1)
+
+
+# --------------------------------------------------------- stage backends
+class NumpyStages:
+    """The four stages (r3d_slab_transform's) restated with dense DFT
+    matrices: the packed real x transform at the half-shifted frequencies
+    2p + 1/2 with the checkerboard sign, y and z at k + 1/2."""
+
+    @staticmethod
+    def _mx(nx):
+        x = np.arange(nx)
+        p = np.arange(nx // 2)
+        return ((-1.0) ** x)[None, :] * np.exp(-2j * np.pi * np.outer(2 * p + 0.5, x) / nx)
+
+    @staticmethod
+    def _mk(n):
+        j = np.arange(n)
+        return np.exp(-2j * np.pi * np.outer(j + 0.5, j) / n)
+
+    def forward_xy(self, real, z_parity0=0):
+        nzl, ny, nx = real.shape
+        sgn = ((-1.0) ** (np.arange(nzl)[:, None] + np.arange(ny)[None, :] + z_parity0))
+        a = np.einsum("px,zyx->zyp", self._mx(nx), real * sgn[:, :, None])
+        return np.einsum("ky,zyp->zkp", self._mk(ny), a)
+
+    def forward_z(self, spec):
+        return np.einsum("kz,zyp->kyp", self._mk(spec.shape[0]), spec)
+
+    def inverse_z(self, spec):
+        return np.einsum("kz,kyp->zyp", np.conj(self._mk(spec.shape[0])), spec)
+
+    def inverse_xy(self, spec, z_parity0=0):
+        """The adjoint direction with the kernels' normalisation: the result is
+        the real grid times ny nx / 2 after forward_xy."""
+        nzl, ny, hx = spec.shape
+        nx = 2 * hx
+        a = np.einsum("ky,zkp->zyp", np.conj(self._mk(ny)), spec)
+        # full odd-frequency spectrum of each real row: G[2p] = a_p,
+        # G[nx-1-2p] = conj(a_p); f = Re sum_k G[k] e^{+2 pi i x (k+1/2)/nx} / 2
+        x = np.arange(nx)
+        p = np.arange(hx)
+        e = np.exp(2j * np.pi * np.outer(x, 2 * p + 0.5) / nx)
+        f = np.real(np.einsum("xp,zyp->zyx", e, a))  # half the sum, real part
+        sgn = ((-1.0) ** (np.arange(nzl)[:, None, None] + np.arange(ny)[None, :, None] +
+                          np.arange(nx)[None, None, :] + z_parity0))
+        return f * sgn
+
+
+class CudaStages:
+    """The stages on the GPU through r3d_slab_transform (torch tensors on the
+    rank's device; FP64)."""
+
+    def __init__(self, lib, device=0):
+        self.lib, self.device = lib, device
+
+    def _call(self, stage, nx, ny, nz, spec, real, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        rc = self.lib.r3d_slab_transform(self.device, stage, nx, ny, nz,
+                                         ctypes.c_void_p(spec.data_ptr()),
+                                         ctypes.c_void_p(real.data_ptr()) if real is not None
+                                         else None, ctypes.c_void_p(s))
+        if rc:
+            raise RuntimeError(self.lib.r3d_last_error(None).decode())
+
+    def forward_xy(self, real):
+        import torch
+        nzl, ny, nx = real.shape
+        spec = torch.empty((nzl, ny, nx // 2, 2), dtype=torch.float64, device=real.device)
+        self._call(0, nx, ny, nzl, spec, real.contiguous())
+        return spec
+
+    def forward_z(self, spec):
+        nz, nyl, hx, _ = spec.shape
+        self._call(1, 2 * hx, nyl, nz, spec, None)
+        return spec
+
+    def inverse_z(self, spec):
+        nz, nyl, hx, _ = spec.shape
+        self._call(2, 2 * hx, nyl, nz, spec, None)
+        return spec
+
+    def inverse_xy(self, spec):
+        import torch
+        nzl, ny, hx, _ = spec.shape
+        real = torch.empty((nzl, ny, 2 * hx), dtype=torch.float64, device=spec.device)
+        self._call(3, 2 * hx, ny, nzl, spec, real)
+        return real
+
+
+# ------------------------------------------------------------------ driver
+def all_to_all(send, send_counts, recv_counts, group):
+    """One all-to-all of complex128 numpy buffers (as float64 pairs)."""
+    import torch
+    import torch.distributed as dist
+    s = torch.from_numpy(np.ascontiguousarray(send).view(np.float64))
+    r = torch.empty(2 * sum(recv_counts), dtype=torch.float64)
+    dist.all_to_all_single(r, s, output_split_sizes=[2 * c for c in recv_counts],
+                           input_split_sizes=[2 * c for c in send_counts], group=group)
+    return r.numpy().view(np.complex128)
+
+
+def forward(real_zslab, plan, rank, stages=None, group=None):
+    """Distributed forward transform (CPU ranks, numpy stages): a z-slab real
+    grid -> this rank's y-slab of the transformed half spectrum."""
+    st = stages or NumpyStages()
+    spec_z = st.forward_xy(real_zslab)
+    recv = all_to_all(pack_z2y(spec_z, plan), plan.send_counts_z2y(rank),
+                      plan.recv_counts_z2y(rank), group)
+    return st.forward_z(unpack_z2y(recv, plan, rank))
+
+
+def inverse(spec_yslab, plan, rank, stages=None, group=None):
+    """Distributed inverse: this rank's y-slab of the half spectrum -> its
+    z-slab of the real grid (times nx ny nz / 2)."""
+    st = stages or NumpyStages()
+    spec_y = st.inverse_z(spec_yslab)
+    recv = all_to_all(pack_y2z(spec_y, plan), plan.recv_counts_z2y(rank),
+                      plan.send_counts_z2y(rank), group)
+    return st.inverse_xy(unpack_y2z(recv, plan, rank))
+
+
+def allreduce_sums(values, group=None):
+    """The solve's per-rank partial sums (sum R^2, the AN2 dots) over ranks:
+    every rank then takes the same convergence and mixing decisions
+    (cal_rms.cu:23, anderson.cu:95)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(np.asarray(values, dtype=np.float64))
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.numpy()

@@ -307,7 +307,8 @@ def sec8d_bytes(N, n, b, m):
 
 # which stage of that count each of this design's kernels does (a kernel that
 # has no stage there -- the separate y passes -- is counted by its own bytes)
-KERNEL_STAGE = {"fwd_x": "A", "zoz": "B", "inv_x": "C", "mix_an2": "D", "mix_anm": "D"}
+KERNEL_STAGE = {"fwd_x": "A", "zoz": "B", "inv_x": "C", "mix_an2": "D", "mix_anm": "D",
+                "mix_fx": "AD"}
 
 
 def reference_cuda(deck, xvk, maxstep=None, timeout=1800):
@@ -482,7 +483,7 @@ def run_gpu(args, group):
     N = (512 if c3 else args.grid) ** 3
     sec8 = sec8d_bytes(N, 4, b, m)
     stage = KERNEL_STAGE.get(name)
-    alg = sec8[stage] if stage else kbytes
+    alg = sum(sec8[x] for x in stage) if stage else kbytes
     achieved = alg / (kms * 1e-3) / 1e9
     iter_bytes = sum(bb for _, _, bb in prof)
 
@@ -573,7 +574,7 @@ def run_gpu(args, group):
             "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": ncu_traffic(name), "algorithmic_bytes": alg,
-                         "bytes_count": (f"stage {stage} of A_iter = N b (n (14 + 3m) + 2)"
+                         "bytes_count": (f"stage(s) {stage} of A_iter = N b (n (14 + 3m) + 2)"
                                          if stage else "this design's own count"),
                          "design_bytes": kbytes, "design_frac": kbytes / (kms * 1e-3) / 1e9 / peak,
                          "launch_ms": kms,

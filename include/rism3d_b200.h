@@ -254,6 +254,23 @@ int r3d_fft3d(int device, int precision, int nx, int ny, int nz,
 int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
                       int dir, const double *d_in, double *d_out, void *stream);
 
+/* One rank's stages of the shifted 3D transform when a grid is split over
+ * several GPUs (the reference's distributed FFT3D, fft3d.cu:81-163, with the
+ * pencil decomposition of cell.cc:30-48; here z-slabs for the x and y passes
+ * and y-slabs for the z pass, moved between by one all-to-all per direction,
+ * which the caller runs -- slabs.py with NCCL).  Device buffers, FP64, on
+ * `device` and `stream` (NULL: the default stream); the call returns when the
+ * stage has finished.  (nx, ny, nz) are the slab's own extents:
+ *   stage 0  d_real [nz][ny][nx] (a z-slab; it must start on an even global
+ *            plane) -> d_spec [nz][ny][nx/2] complex: x and y transforms
+ *   stage 1  d_spec [nz][ny][nx/2] (a y-slab, all z) -> z transform, in place
+ *   stage 2  the inverse z transform, in place
+ *   stage 3  d_spec (z-slab; destroyed) -> d_real: inverse y and x transforms
+ * in unnormalised transform units (the constant phase dv C(k) of r3d_fft3d
+ * left out; stages 0-1 then 2-3 return the grid times nx ny nz / 2). */
+int r3d_slab_transform(int device, int stage, int nx, int ny, int nz, double *d_spec,
+                       double *d_real, void *stream);
+
 /* ---- batches of independent solves --------------------------------------
  * The reference runs one solve per process (main.cu:63-65).  A batch iterates
  * many initialized contexts together: the solves of one geometry (grid,

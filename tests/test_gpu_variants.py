@@ -32,7 +32,7 @@ def _numbers(text):
 
 
 @pytest.mark.parametrize("variant", ["0", "1", "2", "3", "4"])
-@pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96"])
+@pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96", "g80kh"])
 def test_x_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, variant, case):
     import rism3d as R
     monkeypatch.setenv("R3D_X_VARIANT", variant)
@@ -55,7 +55,7 @@ def test_x_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, varian
 
 
 @pytest.mark.parametrize("yz", ["0", "1", "2", "3", "4"])
-@pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96"])
+@pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96", "g80kh"])
 def test_yz_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, yz, case):
     """Every y/z trio against the reference: 0 tile-per-CTA kernels, 1 and 2
     the tensor copy engine (digit-reversed ky layout of the spectrum between

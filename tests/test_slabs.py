@@ -1,0 +1,157 @@
+"""A grid split over several GPUs (slabs.py): the z-slab / y-slab partition,
+the all-to-all transposes between them and the distributed shifted 3D
+transform, run as world-size-2 gloo groups on the CPU with the numpy stages,
+against the single-process transform and the closed-form shifted DFT (the
+semantics of the reference's fft3d.cu:81-163).  The GPU stages
+(r3d_slab_transform) are checked against the same numbers with the ranks
+emulated one after the other on one device (test marked gpu)."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "3d-rism-cuda-mpi_b200")
+sys.path.insert(0, PKG)
+import slabs  # noqa: E402
+
+SHAPE = (12, 10, 8)  # nz, ny, nx
+BOX = (4.0, 5.0, 6.5)
+
+
+def _grid(seed=3):
+    return np.random.default_rng(seed).standard_normal(SHAPE)
+
+
+def _full_raw(f):
+    st = slabs.NumpyStages()
+    return st.forward_z(st.forward_xy(f))
+
+
+def test_partition_covers_the_grid_with_even_z_starts():
+    for world in (1, 2, 3, 5):
+        p = slabs.SlabPlan(14, 9, 8, world) if world < 5 else slabs.SlabPlan(20, 7, 8, world)
+        assert sum(p.nzl) == p.nz and sum(p.nyl) == p.ny
+        assert all(z0 % 2 == 0 for z0 in p.z0)
+        assert all(p.z0[r] + p.nzl[r] == (p.z0[r + 1] if r + 1 < world else p.nz)
+                   for r in range(world))
+        assert max(p.nzl) - min(p.nzl) <= 2 and max(p.nyl) - min(p.nyl) <= 1
+        for r in range(world):  # what r sends is what the others receive
+            assert sum(p.send_counts_z2y(r)) == p.nzl[r] * p.ny * p.hx
+            assert sum(p.recv_counts_z2y(r)) == p.nz * p.nyl[r] * p.hx
+    with pytest.raises(ValueError):
+        slabs.SlabPlan(6, 4, 8, 4)  # fewer than two z-planes per rank
+
+
+def test_numpy_stages_are_the_shifted_transform():
+    """raw = i sigma F / dv with F the closed-form shifted DFT (k_x index 2p)
+    and sigma = (-1)^(2p + ky + kz + (nx + ny + nz) / 2): the constant phase
+    the full-grid seam r3d_fft3d applies."""
+    from test_oracle import _direct_shifted_dft
+    f = _grid()
+    nz, ny, nx = SHAPE
+    F = _direct_shifted_dft(f, BOX)[:, :, 0::2]
+    dv = BOX[0] * BOX[1] * BOX[2] / f.size
+    par0 = ((nx + ny + nz) // 2) & 1
+    kz, ky, p = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx // 2), indexing="ij")
+    sigma = (-1.0) ** (2 * p + ky + kz + par0)
+    np.testing.assert_allclose(_full_raw(f), 1j * sigma * F / dv, atol=1e-10 * np.abs(F).max() / dv)
+
+
+def test_numpy_stages_round_trip():
+    f = _grid(5)
+    st = slabs.NumpyStages()
+    back = st.inverse_xy(st.inverse_z(_full_raw(f)))
+    np.testing.assert_allclose(back, f * f.size / 2, atol=1e-9 * f.size)
+
+
+RANK_SCRIPT = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, %(pkg)r)
+import replicas, slabs
+g = replicas.Group("gloo", timeout_s=60)
+nz, ny, nx = %(shape)r
+f = np.random.default_rng(3).standard_normal((nz, ny, nx))
+plan = slabs.SlabPlan(nz, ny, nx, g.world)
+mine = slabs.forward(f[plan.zslab(g.rank)], plan, g.rank)
+back = slabs.inverse(mine.copy(), plan, g.rank)
+sums = slabs.allreduce_sums([float(np.sum(np.abs(mine) ** 2)), 1.0])
+print(json.dumps({"rank": g.rank, "y": [plan.y0[g.rank], plan.nyl[g.rank]],
+                  "z": [plan.z0[g.rank], plan.nzl[g.rank]],
+                  "spec": [mine.real.tolist(), mine.imag.tolist()], "back": back.tolist(),
+                  "sums": sums.tolist()}), flush=True)
+g.close()
+"""
+
+
+def test_distributed_transform_on_two_gloo_ranks(tmp_path):
+    """Each rank transforms its z-slab; after the z-to-y all-to-all and the z
+    pass it holds its y-slab of the full transform.  The inverse brings back
+    its z-slab (times N/2).  The partial-sum all-reduce sums over ranks."""
+    script = tmp_path / "rank.py"
+    script.write_text(RANK_SCRIPT % {"pkg": PKG, "shape": SHAPE})
+    code = (f"import sys; sys.path.insert(0, {PKG!r}); import replicas; "
+            f"sys.exit(replicas.launch(2, [{str(script)!r}], timeout_s=120))")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    res = sorted((json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")),
+                 key=lambda r: r["rank"])
+    assert len(res) == 2
+    f = _grid()
+    raw = _full_raw(f)
+    total = 0.0
+    for r in res:
+        y0, nyl = r["y"]
+        z0, nzl = r["z"]
+        spec = np.array(r["spec"][0]) + 1j * np.array(r["spec"][1])
+        np.testing.assert_allclose(spec, raw[:, y0:y0 + nyl, :], atol=1e-9 * np.abs(raw).max())
+        np.testing.assert_allclose(np.array(r["back"]), f[z0:z0 + nzl] * f.size / 2,
+                                   atol=1e-8 * f.size)
+        total += np.sum(np.abs(spec) ** 2)
+    for r in res:
+        assert r["sums"][1] == 2.0
+        assert r["sums"][0] == pytest.approx(total, rel=1e-12)
+
+
+@pytest.mark.gpu
+def test_gpu_stages_match_with_two_emulated_ranks():
+    """r3d_slab_transform's four stages for two ranks, run one after the other
+    on one device (the all-to-all done by packing on the host), against the
+    numpy stages; forward then inverse returns the grid times N/2."""
+    import torch
+    import rism3d as R
+    nz, ny, nx = 16, 12, 32
+    f = np.random.default_rng(9).standard_normal((nz, ny, nx))
+    plan = slabs.SlabPlan(nz, ny, nx, 2)
+    cs = slabs.CudaStages(R.lib, 0)
+    to_c = lambda t: t.cpu().numpy()[..., 0] + 1j * t.cpu().numpy()[..., 1]  # noqa: E731
+    to_t = lambda a: torch.from_numpy(np.stack([a.real, a.imag], -1).copy()).cuda()  # noqa: E731
+    spec_z = [to_c(cs.forward_xy(torch.from_numpy(f[plan.zslab(r)].copy()).cuda()))
+              for r in range(2)]
+    sends = [slabs.pack_z2y(spec_z[r], plan) for r in range(2)]
+    spec_y = []
+    for r in range(2):  # what rank r receives from each source
+        parts = []
+        for s in range(2):
+            off = sum(plan.send_counts_z2y(s)[:r])
+            parts.append(sends[s][off:off + plan.send_counts_z2y(s)[r]])
+        spec_y.append(to_c(cs.forward_z(to_t(slabs.unpack_z2y(np.concatenate(parts), plan, r)))))
+    raw = _full_raw(f)
+    for r in range(2):
+        np.testing.assert_allclose(spec_y[r], raw[:, plan.yslab(r), :], atol=1e-10 * np.abs(raw).max())
+    # inverse
+    inv_y = [to_c(cs.inverse_z(to_t(spec_y[r]))) for r in range(2)]
+    sends = [slabs.pack_y2z(inv_y[r], plan) for r in range(2)]
+    for r in range(2):
+        parts = []
+        for s in range(2):
+            counts = plan.recv_counts_z2y(s)  # what s sends to each destination
+            off = sum(counts[:r])
+            parts.append(sends[s][off:off + counts[r]])
+        back = cs.inverse_xy(to_t(slabs.unpack_y2z(np.concatenate(parts), plan, r))).cpu().numpy()
+        np.testing.assert_allclose(back, f[plan.zslab(r)] * f.size / 2, atol=1e-9 * f.size)
