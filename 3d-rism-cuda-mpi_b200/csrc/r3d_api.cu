@@ -95,6 +95,8 @@ template <typename P>
 int sr_pc_y_of();
 template <typename P>
 int sr_pc_z_of(int L, int ns);
+template <typename P>
+void sr_allow_geometry(int hx, int ny, int nz, int ns);
 int sr_pc_x_of(int L);
 size_t sr_smem_x(int L, int PC, size_t csz);
 template <typename P>
@@ -303,23 +305,84 @@ static cudaError_t copy_d2h(r3d_ctx *c, void *dst, const void *src, size_t n,
   return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s);
 }
 
+// A solve's device memory comes from one stream-ordered pool per device,
+// allocated and freed on the solve's stream, and the pool keeps what is
+// freed for the next solve.  cudaMalloc / cudaFree of a solve's gigabytes
+// would synchronise the whole device -- a server's admissions would wait
+// for the iterations in flight -- and returning and re-mapping the pages of
+// every solve costs from milliseconds to a second per solve.  Memory the
+// pool holds unused is counted as free by the admission checks and given
+// back (trimmed) when an allocation does not fit.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64];
+
+static cudaMemPool_t solve_pool(int dev) {
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = dev;
+    cudaMemPool_t mp = nullptr;
+    if (cudaMemPoolCreate(&mp, &pp) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    unsigned long long keep = ~0ull;  // never give memory back at a sync
+    cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pool[dev] = mp;
+  }
+  return g_pool[dev];
+}
+
+// Bytes the device's pool holds but no solve uses.
+static size_t pool_spare(int dev) {
+  cudaMemPool_t mp = solve_pool(dev);
+  if (!mp) return 0;
+  unsigned long long res = 0, used = 0;
+  cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &res);
+  cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemCurrent, &used);
+  return res > used ? (size_t)(res - used) : 0;
+}
+
+// bytes on stream s from device dev's pool; on a failure the pool's unused
+// memory is released and the allocation tried once more
+static cudaError_t pool_alloc(int dev, void **p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t mp = solve_pool(dev);
+  if (!mp) return cudaErrorMemoryAllocation;
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes, mp, s);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cudaStreamSynchronize(s);
+    cudaMemPoolTrimTo(mp, 0);
+    e = cudaMallocFromPoolAsync(p, bytes, mp, s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+  }
+  return e;
+}
+
 static int dalloc(r3d_ctx *c, void **p, size_t bytes) {
   if (bytes == 0) bytes = 16;
-  cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return fail(c, R3D_ENOMEM, "cudaMalloc(" + std::to_string(bytes) +
-                                   ") failed: " + cudaGetErrorString(e));
-  }
+  cudaError_t e = pool_alloc(c->opts.device, p, bytes, c->stream);
+  if (e != cudaSuccess)
+    return fail(c, R3D_ENOMEM, "device allocation of " + std::to_string(bytes) +
+                                   " bytes failed: " + cudaGetErrorString(e));
   c->allocs.push_back(*p);
   c->bytes += bytes;
   return R3D_OK;
 }
 
+// Frees on the solve's stream; every other stream that used the memory (a
+// batch's, a server's) has finished with it when a solve is freed.
 static void free_all(r3d_ctx *c) {
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   c->gexec = nullptr;
-  for (void *p : c->allocs) cudaFree(p);
+  for (void *p : c->allocs) cudaFreeAsync(p, c->stream);
   c->allocs.clear();
   c->bytes = 0;
   c->rtmp = nullptr;
@@ -723,6 +786,14 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
       g.smzs = smz;
     }
   }
+  // large shared memory for the Stockham kernels of this geometry's lengths
+  // (set here, before any capture; loads only the kernels the solve may use)
+  if (g.fxs_pc || g.yz_sr) {
+    if (fp64)
+      sr_allow_geometry<P64>(g.fxs_pc ? d.hx : 0, g.yz_sr ? d.ny : 0, g.yz_sr ? d.nz : 0, d.n);
+    else
+      sr_allow_geometry<PMix>(g.fxs_pc ? d.hx : 0, g.yz_sr ? d.ny : 0, g.yz_sr ? d.nz : 0, d.n);
+  }
   // mixers: one chunk of mix_chunk() elements per CTA; ANM dots: one full
   // wave of a grid-stride reduction
   const long long niv = (long long)d.n * d.Ns;
@@ -1024,7 +1095,7 @@ static int refresh(r3d_ctx *c, bool zero) {
   char *tmp = c->rtmp;
   if (!tmp) {
     if (c->fp64) {
-      CK(cudaMalloc((void **)&tmp, bytes));
+      CK(pool_alloc(c->opts.device, (void **)&tmp, bytes, s));
     } else {
       int rc = dalloc(c, (void **)&c->rtmp, bytes);
       if (rc) return rc;
@@ -1064,7 +1135,7 @@ static int refresh(r3d_ctx *c, bool zero) {
   launch_lr_update<P>(c64, c->lr, (long long)n * N, s);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
-  if (tmp != c->rtmp) cudaFree(tmp);
+  if (tmp != c->rtmp) cudaFreeAsync(tmp, s);
   return R3D_OK;
 }
 
@@ -1471,7 +1542,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     // FP64 phase tables of the k-space Coulomb sum (setup scratch)
     const size_t ntab = (size_t)std::max(nu, 1) * (d.hx + d.ny + d.nz);
     double2 *tabs = nullptr;
-    cudaError_t e = cudaMalloc((void **)&tabs, ntab * sizeof(double2));
+    cudaError_t e = pool_alloc(c->opts.device, (void **)&tabs, ntab * sizeof(double2), s);
     if (e != cudaSuccess) return fail(c, R3D_ENOMEM, "setup scratch");
     double *fr64 = nullptr;
     cudaEvent_t ev[4];
@@ -1495,7 +1566,7 @@ static int init_typed(r3d_ctx *c, const ShellTable &st) {
     }
     CK(cudaEventRecord(ev[2], s));
     CK(cudaStreamSynchronize(s));
-    cudaFree(tabs);
+    cudaFreeAsync(tabs, s);
     // long-range h term: lr = 1 - F^-1[chi q phi_L(k)]  (refresh, c_ref = 0)
     CK(cudaEventRecord(ev[3], s));
     if ((rc = refresh<P>(c, true))) return rc;
@@ -1561,6 +1632,7 @@ extern "C" int r3d_initialize(r3d_ctx *c) {
                                     std::to_string(c->opts.hbm_budget));
   size_t fre = 0, tot = 0;
   CK(cudaMemGetInfo(&fre, &tot));
+  fre += pool_spare(c->opts.device);  // held by the pool for the next solve
   if (need > fre) return fail(c, R3D_ENOMEM, "problem needs " + std::to_string(need) +
                                                  " device bytes, " + std::to_string(fre) + " free");
   c->desc = d;
@@ -1758,7 +1830,7 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   // keep t: the kernels below run out of sequence and overwrite it
   void *tsave = nullptr;
   const size_t tb = (size_t)d.n * d.Ns * sizeof(T);
-  CK(cudaMalloc(&tsave, tb));
+  CK(pool_alloc(c->opts.device, &tsave, tb, s));
   CK(cudaMemcpyAsync(tsave, c->t, tb, cudaMemcpyDeviceToDevice, s));
   Ctl h;
   int rc = read_ctl(c, h);
@@ -1832,7 +1904,7 @@ static int profile_typed(r3d_ctx *c, int reps, std::string &names, double *ms,
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(c->t, tsave, tb, cudaMemcpyDeviceToDevice, s));
   CK(cudaStreamSynchronize(s));
-  cudaFree(tsave);
+  cudaFreeAsync(tsave, s);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *nk = std::min(k, 16);
@@ -1983,7 +2055,7 @@ static int t_of_residual(r3d_ctx *c, const Ctl &h, const void **out) {
 static int ensure_scratch(r3d_ctx *c, size_t bytes) {
   if (c->scratch_bytes >= bytes) return R3D_OK;
   if (c->scratch) {
-    cudaFree(c->scratch);
+    cudaFreeAsync(c->scratch, c->stream);
     c->allocs.erase(std::find(c->allocs.begin(), c->allocs.end(), (void *)c->scratch));
     c->bytes -= c->scratch_bytes;
   }
@@ -2248,7 +2320,7 @@ extern "C" int r3d_atom_integrals(r3d_ctx *c, double *grad, double *euv, double 
   const long long nk = (long long)nu * (4 + n);
   double *buf = nullptr;
   const size_t bytes = (tab.size() + (size_t)nchunk * nk + nk) * sizeof(double);
-  CK(cudaMalloc((void **)&buf, std::max<size_t>(bytes, 16)));
+  CK(pool_alloc(c->opts.device, (void **)&buf, std::max<size_t>(bytes, 16), s));
   double *dtab = buf, *part = buf + tab.size(), *out = part + (size_t)nchunk * nk;
   int rcc = R3D_OK;
   std::vector<double> host(nk);
@@ -2281,7 +2353,7 @@ extern "C" int r3d_atom_integrals(r3d_ctx *c, double *grad, double *euv, double 
     c->d2h += nk * 8;
     c->h2d += tab.size() * 8;
   }
-  cudaFree(buf);
+  cudaFreeAsync(buf, s);
   if (rcc) return rcc;
   const double dv = p.box[0] * p.box[1] * p.box[2] / (double)N, kcal2J = 4184.0;
   for (int a = 0; a < nu; ++a) {

@@ -1480,8 +1480,6 @@ void ct_allow_smem_all();
 
 template <typename P>
 void tma_allow_smem_all();
-template <typename P>
-void sr_allow_smem_all();
 void kernels_set_smem(bool fp64, size_t maxbytes) {
   static bool ct_done[2] = {false, false};
   if (fp64)
@@ -1492,11 +1490,9 @@ void kernels_set_smem(bool fp64, size_t maxbytes) {
     if (fp64) {
       ct_allow_smem_all<P64>();
       tma_allow_smem_all<P64>();
-      sr_allow_smem_all<P64>();
     } else {
       ct_allow_smem_all<PMix>();
       tma_allow_smem_all<PMix>();
-      sr_allow_smem_all<PMix>();
     }
     ct_done[fp64] = true;
   }

@@ -833,32 +833,10 @@ bool sr_launch_zoz(int L, int ns, bool ozreg, Batch b, int grid, size_t smem, cu
   }
 }
 
-template <typename P, int NS, bool OZREG>
-static void sr_allow_ns() {
-#define R3D_SRA(LL)                                                                       \
-  sr_allow(k_zoz_sr<P, LL, sr_pc_z<P>(LL, NS), NS, sr_threads_z<P>(LL, NS, OZREG), OZREG>);
-  R3D_SR_LENGTHS(R3D_SRA)
-#undef R3D_SRA
-}
-template <typename P>
-void sr_allow_x();
-template <typename P>
-void sr_allow_smem_all() {
-  constexpr int PC = sr_pc_y<P>();
-#define R3D_SRA(LL)                       \
-  sr_allow(k_fy_sr<P, LL, PC, -1>);       \
-  sr_allow(k_fy_sr<P, LL, PC, 1>);
-  R3D_SR_LENGTHS(R3D_SRA)
-#undef R3D_SRA
-  sr_allow_x<P>();
-  sr_allow_ns<P, 1, false>();
-  sr_allow_ns<P, 1, true>();
-  sr_allow_ns<P, 2, false>();
-  sr_allow_ns<P, 2, true>();
-  sr_allow_ns<P, 3, false>();
-  sr_allow_ns<P, 3, true>();
-  sr_allow_ns<P, 4, false>();
-  sr_allow_ns<P, 4, true>();
+template <typename P, int LL, int NS>
+static void sr_allow_zoz() {
+  sr_allow(k_zoz_sr<P, LL, sr_pc_z<P>(LL, NS), NS, sr_threads_z<P>(LL, NS, false), false>);
+  sr_allow(k_zoz_sr<P, LL, sr_pc_z<P>(LL, NS), NS, sr_threads_z<P>(LL, NS, true), true>);
 }
 
 // x passes: PC rows per tile, PC * (L / R_0) tasks filling the CTA
@@ -903,20 +881,37 @@ bool sr_launch_ix(int L, Batch b, int grid, size_t smem, cudaStream_t s, int per
 #undef R3D_SRX
   return false;
 }
+
+// The kernels of one geometry: x passes of length hx, y of ny, z with its
+// OZ over ns sites of nz (both OZ forms).  Setting the attribute loads the
+// kernel, so a solve loads only the lengths it uses.
 template <typename P>
-void sr_allow_x() {
-#define R3D_SRAX(LL)                                \
-  sr_allow(k_fx_sr<P, LL, sr_pc_x<LL>()>);          \
-  sr_allow(k_ix_sr<P, LL, sr_pc_x<LL>()>);
-  R3D_SR_LENGTHS(R3D_SRAX)
-#undef R3D_SRAX
+void sr_allow_geometry(int hx, int ny, int nz, int ns) {
+  constexpr int PC = sr_pc_y<P>();
+#define R3D_SRG(LL)                                                   \
+  if (hx == LL) {                                                     \
+    sr_allow(k_fx_sr<P, LL, sr_pc_x<LL>()>);                          \
+    sr_allow(k_ix_sr<P, LL, sr_pc_x<LL>()>);                          \
+  }                                                                   \
+  if (ny == LL) {                                                     \
+    sr_allow(k_fy_sr<P, LL, PC, -1>);                                 \
+    sr_allow(k_fy_sr<P, LL, PC, 1>);                                  \
+  }                                                                   \
+  if (nz == LL) {                                                     \
+    if (ns == 1) sr_allow_zoz<P, LL, 1>();                            \
+    if (ns == 2) sr_allow_zoz<P, LL, 2>();                            \
+    if (ns == 3) sr_allow_zoz<P, LL, 3>();                            \
+    if (ns == 4) sr_allow_zoz<P, LL, 4>();                            \
+  }
+  R3D_SR_LENGTHS(R3D_SRG)
+#undef R3D_SRG
 }
 
 template bool sr_launch_fx<PSR>(int, Batch, int, size_t, cudaStream_t);
 template bool sr_launch_ix<PSR>(int, Batch, int, size_t, cudaStream_t, int);
 template bool sr_launch_fy<PSR>(int, int, Batch, int, size_t, cudaStream_t);
 template bool sr_launch_zoz<PSR>(int, int, bool, Batch, int, size_t, cudaStream_t);
-template void sr_allow_smem_all<PSR>();
+template void sr_allow_geometry<PSR>(int, int, int, int);
 template int sr_pc_y_of<PSR>();
 template int sr_pc_z_of<PSR>(int, int);
 
