@@ -97,6 +97,13 @@ template <typename P>
 int sr_pc_z_of(int L, int ns);
 template <typename P>
 void sr_allow_geometry(int hx, int ny, int nz, int ns);
+template <typename P>
+bool sr_launch_zozp(int L, int ns, Batch b, int ntiles, int grid, size_t smem, cudaStream_t s);
+template <typename P>
+int sr_occupancy_zozp(int L, int ns, size_t smem);
+template <typename P>
+int sr_zp_supported(int L, int ns);
+size_t sr_smem_zp(int L, int PC, int ns, size_t csz);
 int sr_pc_x_of(int L);
 size_t sr_smem_x(int L, int PC, size_t csz);
 template <typename P>
@@ -207,12 +214,14 @@ struct Geo {
   // the tile-per-CTA kernels): CTAs per solve, tiles per CTA, stages, smem
   // (yz_tma also carries the chosen y/z variant: 3 and 4 are the register-
   // pass Stockham y and z passes, with the OZ on registers / as a pass of
-  // its own; yz_sr = 1 where those kernels cover the lengths and sites)
+  // its own; yz_sr = 1 where those kernels cover the lengths and sites;
+  // 5: variant 4 with the persistent z pass that streams its next tile in,
+  // yz_srp = 1 where it exists: zp_ctas CTAs for any number of solves)
   int yz_tma = 0, fyt_pc = 0, fyt_ctas = 0, fyt_per = 1, fyt_nst = 0, zt_pc = 0, zt_ctas = 0,
       zt_per = 1, zt_nst = 0;
   size_t smfyt = 0, smzt = 0;
-  int yz_sr = 0, fys_ctas = 0, zs_ctas = 0;
-  size_t smfys = 0, smzs = 0;
+  int yz_sr = 0, fys_ctas = 0, zs_ctas = 0, yz_srp = 0, zp_ctas = 0;
+  size_t smfys = 0, smzs = 0, smzp = 0;
   // the iteration's FX / IX on the Stockham engine (fxs_pc / ixs_pc = 0: not used;
   // x variant 4): rows per tile, CTAs (FX one tile each; IX ixs_per tiles)
   int fxs_pc = 0, ixs_pc = 0, fxs_ctas = 0, ixs_ctas = 0, ixs_per = 1;
@@ -794,6 +803,25 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
     else
       sr_allow_geometry<PMix>(g.fxs_pc ? d.hx : 0, g.yz_sr ? d.ny : 0, g.yz_sr ? d.nz : 0, d.n);
   }
+  // the persistent z pass: whole 16-byte copies of tile rows (the rows of
+  // the spectrum and the site stride 16-byte aligned), one CTA per SM or more
+  g.yz_srp = g.zp_ctas = 0;
+  g.smzp = 0;
+  if (g.yz_sr && (fp64 ? sr_zp_supported<P64>(d.nz, d.n) : sr_zp_supported<PMix>(d.nz, d.n)) &&
+      ((size_t)d.hx * cs) % 16 == 0 && ((size_t)d.Nhs * cs) % 16 == 0) {
+    const int pcz = fp64 ? sr_pc_z_of<P64>(d.nz, d.n) : sr_pc_z_of<PMix>(d.nz, d.n);
+    const size_t sm = sr_smem_zp(d.nz, pcz, d.n, cs);
+    const int occ = sm > kSmemMax ? 0
+                    : fp64 ? sr_occupancy_zozp<P64>(d.nz, d.n, sm)
+                           : sr_occupancy_zozp<PMix>(d.nz, d.n, sm);
+    if (occ > 0) {
+      int nsm = kNumSM;
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->opts.device);
+      g.yz_srp = 1;
+      g.smzp = sm;
+      g.zp_ctas = occ * nsm;
+    }
+  }
   // mixers: one chunk of mix_chunk() elements per CTA; ANM dots: one full
   // wave of a grid-stride reduction
   const long long niv = (long long)d.n * d.Ns;
@@ -880,6 +908,9 @@ static void pass_fy_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s, i
 }
 template <typename P>
 static void pass_zoz_iter(const Desc &d, const Geo &g, Batch b, cudaStream_t s) {
+  if (g.yz_tma == 5 && g.yz_srp &&
+      sr_launch_zozp<P>(d.nz, d.n, b, g.zs_ctas, g.zp_ctas, g.smzp, s))
+    return;
   if (g.yz_tma >= 3 && sr_launch_zoz<P>(d.nz, d.n, g.yz_tma == 3, b, g.zs_ctas, g.smzs, s))
     return;
   if (g.yz_tma == 2 && tma_launch_zoz<P>(d.nz, b, g.zt_ctas, g.smzt, s, g.zt_per, g.zt_nst))
@@ -1226,7 +1257,7 @@ static int autotune_x(r3d_ctx *c) {
     use = {fx ? (k == 3 ? 1 : k) : 0, ix ? k : 0, g.yz_tma};
     if (const char *ey = getenv("R3D_YZ_VARIANT")) {
       const int k = std::atoi(ey);
-      use[2] = (k >= 3) ? (g.yz_sr ? std::min(k, 4) : 0)
+      use[2] = (k >= 3) ? (g.yz_sr ? (k >= 5 ? (g.yz_srp ? 5 : 4) : k) : 0)
                         : (k == 1 && !d.ct_z) ? 0 : std::min(k, g.yz_tma);
     }
     known = true;
@@ -1244,7 +1275,7 @@ static int autotune_x(r3d_ctx *c) {
                      (use[0] == 4 && g.fxs_pc)) &&
                     (use[1] == 0 || ((use[1] == 1 || use[1] == 3) && g.ixb_pc) ||
                      (use[1] == 2 && g.ixw_pc) || (use[1] == 4 && g.ixs_pc)) &&
-                    (use[2] >= 3 ? (g.yz_sr && use[2] <= 4)
+                    (use[2] >= 3 ? (g.yz_sr && (use[2] <= 4 || (use[2] == 5 && g.yz_srp)))
                                  : (use[2] <= g.yz_tma && !(use[2] == 1 && !d.ct_z)));
     if (!ok) use = tune_rule(g, d);
     known = true;
@@ -1335,10 +1366,11 @@ static int autotune_x(r3d_ctx *c) {
     if (g.yz_tma || g.yz_sr) {  // the y/z trio: tile-per-CTA, copy-engine y, copy-engine
                                 // y and z, register-pass Stockham (OZ on registers / shared)
       float best2 = 0;
-      for (int k = 0; k < 5; ++k) {
+      for (int k = 0; k < 6; ++k) {
         if (k == 1 && !d.ct_z) continue;
         if ((k == 1 || k == 2) && !g.yz_tma) continue;
         if (k >= 3 && !g.yz_sr) continue;
+        if (k == 5 && !g.yz_srp) continue;
         Geo o = g;
         o.yz_tma = k;
         const Batch by{c->ddesc, pf + (k >= 3 ? 22 : k ? 16 : 12), 1},
@@ -1357,8 +1389,9 @@ static int autotune_x(r3d_ctx *c) {
     cudaError_t e = cudaGetLastError();
     cudaFree(pf);
     if (e != cudaSuccess) return fail(c, R3D_ECUDA, std::string("autotune: ") + cudaGetErrorString(e));
-    std::fprintf(stderr, "r3d-tune row: {%d, %d, %d, %d, %d, %d, %d, %d},  // us:%s\n", d.nx,
-                 d.ny, d.nz, d.n, c->fp64 ? 1 : 0, use[0], use[1], use[2], report.c_str());
+    std::fprintf(stderr, "r3d-tune row: {%d, %d, %d, %d, %d, %d, %d, %d, %d},  // us:%s\n", d.nx,
+                 d.ny, d.nz, d.n, c->fp64 ? 1 : 0, use[0], use[1], use[2], g.mfx_avail ? 1 : 0,
+                 report.c_str());
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = use;
   }

@@ -26,6 +26,20 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// 16-byte asynchronous copies global -> shared through L2 (cp.async); they
+// complete by groups: commit after a set of copies, then wait for all
+// committed groups.  A hardware wait on copies already issued (no spin).
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)),
+               "l"(__cvta_generic_to_global(src))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 // Bounded wait for phase `parity` of `bar`; false when the limit ran out.
 // polls <= 0: the default, 2^22 polls of try_wait (far beyond any copy's
 // latency).  polls > 0 (the test hook of the error path): that many

@@ -148,6 +148,30 @@ __device__ __forceinline__ constexpr double rsin_tab_16(int e) {
                             -0.38268343236508977173};
   return s[e];
 }
+__device__ __forceinline__ constexpr double rsin_tab_24(int e) {
+  constexpr double s[24] = {
+      0.0, 0.25881904510252076235, 0.5, 0.70710678118654752440, 0.86602540378443864676,
+      0.96592582628906828675, 1.0, 0.96592582628906828675, 0.86602540378443864676,
+      0.70710678118654752440, 0.5, 0.25881904510252076235, 0.0, -0.25881904510252076235, -0.5,
+      -0.70710678118654752440, -0.86602540378443864676, -0.96592582628906828675, -1.0,
+      -0.96592582628906828675, -0.86602540378443864676, -0.70710678118654752440, -0.5,
+      -0.25881904510252076235};
+  return s[e];
+}
+__device__ __forceinline__ constexpr double rsin_tab_32(int e) {
+  constexpr double s[32] = {
+      0.0, 0.19509032201612826785, 0.38268343236508977173, 0.55557023301960222474,
+      0.70710678118654752440, 0.83146961230254523708, 0.92387953251128675613,
+      0.98078528040323044913, 1.0, 0.98078528040323044913, 0.92387953251128675613,
+      0.83146961230254523708, 0.70710678118654752440, 0.55557023301960222474,
+      0.38268343236508977173, 0.19509032201612826785, 0.0, -0.19509032201612826785,
+      -0.38268343236508977173, -0.55557023301960222474, -0.70710678118654752440,
+      -0.83146961230254523708, -0.92387953251128675613, -0.98078528040323044913, -1.0,
+      -0.98078528040323044913, -0.92387953251128675613, -0.83146961230254523708,
+      -0.70710678118654752440, -0.55557023301960222474, -0.38268343236508977173,
+      -0.19509032201612826785};
+  return s[e];
+}
 R3D_ROOTS(6, 1.0, 0.5, -0.5, -1.0, -0.5, 0.5)
 R3D_ROOTS(9, 1.0, 0.76604444311897803520, 0.17364817766693034885, -0.5,
           -0.93969262078590838405, -0.93969262078590838405, -0.5, 0.17364817766693034885,
@@ -161,7 +185,35 @@ R3D_ROOTS(16, 1.0, 0.92387953251128675613, 0.70710678118654752440, 0.38268343236
           -0.38268343236508977173, -0.70710678118654752440, -0.92387953251128675613, -1.0,
           -0.92387953251128675613, -0.70710678118654752440, -0.38268343236508977173, 0.0,
           0.38268343236508977173, 0.70710678118654752440, 0.92387953251128675613)
+R3D_ROOTS(24, 1.0, 0.96592582628906828675, 0.86602540378443864676, 0.70710678118654752440, 0.5,
+          0.25881904510252076235, 0.0, -0.25881904510252076235, -0.5, -0.70710678118654752440,
+          -0.86602540378443864676, -0.96592582628906828675, -1.0, -0.96592582628906828675,
+          -0.86602540378443864676, -0.70710678118654752440, -0.5, -0.25881904510252076235, 0.0,
+          0.25881904510252076235, 0.5, 0.70710678118654752440, 0.86602540378443864676,
+          0.96592582628906828675)
+R3D_ROOTS(32, 1.0, 0.98078528040323044913, 0.92387953251128675613, 0.83146961230254523708,
+          0.70710678118654752440, 0.55557023301960222474, 0.38268343236508977173,
+          0.19509032201612826785, 0.0, -0.19509032201612826785, -0.38268343236508977173,
+          -0.55557023301960222474, -0.70710678118654752440, -0.83146961230254523708,
+          -0.92387953251128675613, -0.98078528040323044913, -1.0, -0.98078528040323044913,
+          -0.92387953251128675613, -0.83146961230254523708, -0.70710678118654752440,
+          -0.55557023301960222474, -0.38268343236508977173, -0.19509032201612826785, 0.0,
+          0.19509032201612826785, 0.38268343236508977173, 0.55557023301960222474,
+          0.70710678118654752440, 0.83146961230254523708, 0.92387953251128675613,
+          0.98078528040323044913)
 #undef R3D_ROOTS
+
+// The half-sample twiddle over the R elements z = j + m L / R of a task of
+// a first forward (last inverse) pass: e^{-i pi z / L} = e^{-i pi j / L}
+// times the constant e^{-i pi m / R} = W_{2R}^m, so a task reads one table
+// entry (for j) instead of R.  Returns that twiddle from the entry for j.
+template <int R, typename C>
+__device__ __forceinline__ C sr_half_twiddle(C pj, int m) {
+  using Rt = decltype(pj.x);
+  if (m == 0) return pj;
+  const Rt c = (Rt)rcos<2 * R>(m), sn = (Rt)-rsin<2 * R>(m);
+  return C{pj.x * c - pj.y * sn, pj.x * sn + pj.y * c};
+}
 
 // ------------------------------------------------------------ small DFTs
 // In place, natural order in and out.

@@ -833,6 +833,66 @@ __global__ void __launch_bounds__(kThreads)
         cb[q] = run;  // C_{q+1}: entries of age q+1 and older
       }
     }
+    if ((niv & 3) == 0) {
+      // Four consecutive elements per thread (16-byte loads of every FP32
+      // stream, the chunk's elements [4 tid, 4 tid + 4)), and the history
+      // read four slots at a time: 64 bytes of loads in flight per thread in
+      // the sum over the ring.  Every slot and stream starts on a 16-byte
+      // boundary when niv is a multiple of 4.
+      const long long iv = (long long)(blockIdx.x - b.prefix[si]) * kMixChunk + 4 * threadIdx.x;
+      if (iv >= niv) return;
+      const float4 r4 = *reinterpret_cast<const float4 *>(res + iv);
+      const double2 ta = *reinterpret_cast<const double2 *>(t + iv);
+      const double2 tb = *reinterpret_cast<const double2 *>(t + iv + 2);
+      const double rk[4] = {r4.x, r4.y, r4.z, r4.w}, tk[4] = {ta.x, ta.y, tb.x, tb.y};
+      double acc[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[e] = tk[e] + beta * rk[e];
+      if (m >= 1) {
+        const long long s0 = (long long)c->mix_slots[0] * niv;
+        const float4 d4 = *reinterpret_cast<const float4 *>(dp + iv);
+        const float4 f4 = *reinterpret_cast<const float4 *>(f + s0 + iv);
+        const double dd[4] = {d4.x, d4.y, d4.z, d4.w}, ff[4] = {f4.x, f4.y, f4.z, f4.w};
+        float e1f[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double e1 = dd[e] + beta * (ff[e] - rk[e]);
+          e1f[e] = (float)e1;
+          acc[e] += cb[0] * e1;
+        }
+        *reinterpret_cast<float4 *>(er + s0 + iv) = make_float4(e1f[0], e1f[1], e1f[2], e1f[3]);
+      }
+      int q = 1;
+      for (; q + 3 < m; q += 4) {
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          v[u] = *reinterpret_cast<const float4 *>(er + (long long)c->mix_slots[q + u] * niv + iv);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double cu = cb[q + u];
+          acc[0] += cu * v[u].x;
+          acc[1] += cu * v[u].y;
+          acc[2] += cu * v[u].z;
+          acc[3] += cu * v[u].w;
+        }
+      }
+      for (; q < m; ++q) {
+        const float4 v = *reinterpret_cast<const float4 *>(er + (long long)c->mix_slots[q] * niv + iv);
+        const double cq = cb[q];
+        acc[0] += cq * v.x;
+        acc[1] += cq * v.y;
+        acc[2] += cq * v.z;
+        acc[3] += cq * v.w;
+      }
+      *reinterpret_cast<float4 *>(f + (long long)head * niv + iv) = r4;
+      *reinterpret_cast<float4 *>(dp + iv) =
+          make_float4((float)(tk[0] - acc[0]), (float)(tk[1] - acc[1]), (float)(tk[2] - acc[2]),
+                      (float)(tk[3] - acc[3]));
+      *reinterpret_cast<double2 *>(t + iv) = make_double2(acc[0], acc[1]);
+      *reinterpret_cast<double2 *>(t + iv + 2) = make_double2(acc[2], acc[3]);
+      return;
+    }
     double acc[kMixPer], tk[kMixPer];
     R rk[kMixPer];
 #pragma unroll

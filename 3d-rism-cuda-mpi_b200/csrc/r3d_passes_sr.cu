@@ -18,6 +18,7 @@
 // The spectrum stays in natural k_y order (the transform sorts itself), so
 // these kernels pair with each other only.  Twiddles come from a per-CTA
 // shared-memory copy of the length's table.
+#include "r3d_async.cuh"
 #include "r3d_common.cuh"
 #include "r3d_fft_sr.cuh"
 
@@ -65,19 +66,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_fy_sr(Batch b) {
     for (int task = threadIdx.x; task < T; task += kThreads) {
       const int p = task % PC, j = task / PC;
       C a[R];
+      const C pj = pw[j];  // y = j + m L / R
 #pragma unroll
       for (int m = 0; m < R; ++m) {
         const int y = sr_in<L, R>(j, m);
         a[m] = R3D_IN(d, wb + (long long)y * hx + p, wn) ? w[(long long)y * hx + p] : C{0, 0};
-        if (!INV) a[m] = cmul(a[m], pw[y]);
+        if (!INV) a[m] = cmul(a[m], sr_half_twiddle<R>(pj, m));
       }
       if constexpr (pl.n == 1) {
         sr_pass<L, R, NS, DIR>(a, tw, j);
 #pragma unroll
         for (int m = 0; m < R; ++m) {
           const int y = sr_out<R, NS>(j, m);
-          if (R3D_IN(d, wb + (long long)y * hx + p, wn))
-            w[(long long)y * hx + p] = INV ? cmul(a[m], cconj(pw[y])) : a[m];
+          if (R3D_IN(d, wb + (long long)y * hx + p, wn))  // one pass: y = m
+            w[(long long)y * hx + p] = INV ? cmul(a[m], cconj(sr_half_twiddle<R>(pj, m))) : a[m];
         }
       } else {
         sr_pass<L, R, NS, DIR>(a, tw, j);
@@ -125,11 +127,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_fy_sr(Batch b) {
 #pragma unroll
       for (int m = 0; m < R; ++m) a[m] = buf[sr_in<L, R>(j, m) * PC + p];
       sr_pass<L, R, NS, DIR>(a, tw, j);
+      static_assert(!INV || NS * R == L, "the inverse's last pass writes y = j + m L / R");
+      const C pj = INV ? pw[j] : C{0, 0};
 #pragma unroll
       for (int m = 0; m < R; ++m) {
         const int y = sr_out<R, NS>(j, m);
         if (R3D_IN(d, wb + (long long)y * hx + p, wn))
-          w[(long long)y * hx + p] = INV ? cmul(a[m], cconj(pw[y])) : a[m];
+          w[(long long)y * hx + p] = INV ? cmul(a[m], cconj(sr_half_twiddle<R>(pj, m))) : a[m];
       }
     }
   }
@@ -550,75 +554,32 @@ __device__ __forceinline__ void sr_oz_point(C *c, const Desc &d, long long ax, l
   sr_oz_apply<R, NS>(c, sr_chi_row<R>(d, ax, ay, kz, gi));
 }
 
-// tile = PC x-columns at one k_y, all NS sites, all z; shared memory
-// [site][L = nz][PC] plus the twiddle table.  Forward z transform (half-
-// sample twiddle on load), OZ, inverse z transform (conjugate half-sample
-// twiddle on store).  OZREG: the forward transform's last pass, the OZ and
-// the inverse transform's first pass run on registers holding every site of
-// a task (one shared-memory round trip less, NS * R_last complex values per
-// thread); else the OZ is a pass of its own over the shared tile.
+// The z pass on a tile of PC x-columns at one k_y, all NS sites, all z;
+// shared memory [site][L = nz][PC] plus the twiddle table.  Forward z
+// transform (half-sample twiddle on load), OZ, inverse z transform
+// (conjugate half-sample twiddle on store).  OZREG: the forward transform's
+// last pass, the OZ and the inverse transform's first pass run on registers
+// holding every site of a task (one shared-memory round trip less, NS *
+// R_last complex values per thread); else the OZ is a pass of its own over
+// the shared tile.  Two kernels run it: one tile per CTA (k_zoz_sr), and one
+// persistent CTA per SM that streams its next tile in while it transforms
+// the current one (k_zoz_srp).
+
+// From the forward transform's second pass (its first has filled the tile)
+// through the inverse transform's second-to-last pass, on the shared tile.
 template <typename P, int L, int PC, int NS, int NT, bool OZREG>
-__global__ void __launch_bounds__(NT, (OZREG || NT > 256) ? 1 : 2) k_zoz_sr(Batch b) {
+__device__ __forceinline__ void sr_zoz_middle(typename Cx<typename P::R>::T *buf,
+                                              const typename Cx<typename P::R>::T *tw,
+                                              const Desc &d, int pt, long long ay,
+                                              long long gbase, long long zs) {
   using R = typename P::R;
   using C = typename Cx<R>::T;
   constexpr SrPlan pl = sr_plan(L);
   constexpr int RL = pl.r[pl.n - 1];  // forward last radix = inverse first
   constexpr int NSL = L / RL;         // N of the forward last pass
-  extern __shared__ __align__(16) char smem[];
-  C *buf = (C *)smem;  // [site][z (padded)][p]
-  C *tw = buf + NS * sr_zrows<L>() * PC;
-  const int si = find_solve(b, blockIdx.x);
-  const Desc &d = b.d[si];
-  if (d.ctl->status != RUNNING) return;
-  const int tile = blockIdx.x - b.prefix[si];
-  const int hx = d.hx, ptiles = hx / PC;
-  const int pt = tile % ptiles, y = tile / ptiles;
-  const long long zs = (long long)d.ny * hx;
-  const C *pw = (const C *)d.pwz;
-  C *w = (C *)d.w + (long long)y * hx + pt * PC;
-  const long long wn = d.n * d.Nhs, wb = (long long)y * hx + pt * PC;
-  (void)wn;
-  (void)wb;
-  for (int e = threadIdx.x; e < L; e += NT) tw[e] = ((const C *)d.twz)[e];
-  const long long ay = 2 * y - d.ny + 1;
-  const long long gbase = (long long)y * hx + pt * PC;
+  (void)NSL;
+  (void)RL;
   auto at = [&](int v, int z, int p) -> C & { return buf[sr_zi<L, PC>(v, z, p)]; };
-
-  // forward pass 0: global -> registers -> shared (the loads of up to 16
-  // values' worth of tasks are issued together: more loads in flight)
-  {
-    constexpr int R0 = pl.r[0], T = NS * PC * (L / R0), K0 = (T + NT - 1) / NT;
-    constexpr int KB = K0 * R0 <= 16 ? K0 : 1;
-#pragma unroll 1
-    for (int k0 = 0; k0 < K0; k0 += KB) {
-      C a[KB][R0];
-#pragma unroll
-      for (int kk = 0; kk < KB; ++kk) {
-        const int task = threadIdx.x + (k0 + kk) * NT;
-        if (k0 + kk < K0 && (T % NT == 0 || task < T)) {
-          const int p = task % PC, q = task / PC, j = q % (L / R0), v = q / (L / R0);
-#pragma unroll
-          for (int m = 0; m < R0; ++m) {
-            const long long gi = v * d.Nhs + sr_in<L, R0>(j, m) * zs + p;
-            a[kk][m] = R3D_IN(d, wb + gi, wn) ? w[gi] : C{0, 0};
-          }
-        }
-      }
-#pragma unroll
-      for (int kk = 0; kk < KB; ++kk) {
-        const int task = threadIdx.x + (k0 + kk) * NT;
-        if (k0 + kk < K0 && (T % NT == 0 || task < T)) {
-          const int p = task % PC, q = task / PC, j = q % (L / R0), v = q / (L / R0);
-#pragma unroll
-          for (int m = 0; m < R0; ++m) a[kk][m] = cmul(a[kk][m], pw[sr_in<L, R0>(j, m)]);
-          sr_pass<L, R0, 1, -1>(a[kk], tw, j);
-#pragma unroll
-          for (int m = 0; m < R0; ++m) at(v, sr_out<R0, 1>(j, m), p) = a[kk][m];
-        }
-      }
-    }
-    __syncthreads();
-  }
   if constexpr (pl.n == 3) sr_tile_pass<L, pl.r[1], sr_ns(L, 1, false), -1, NS, PC, NT>(buf, tw);
   if constexpr (OZREG && pl.n > 1) {
     // forward last pass -> OZ -> inverse first pass, every site of a task in
@@ -673,72 +634,242 @@ __global__ void __launch_bounds__(NT, (OZREG || NT > 256) ? 1 : 2) k_zoz_sr(Batc
        // every site's input (shared-memory broadcast within the group) and
        // writes its site's outputs after the group has read.
       constexpr int G = 32 / NS, TP = PC * (L / 2), NW = NT / 32;
+      // pairs a group takes, and how many of their chi rows are in flight
+      // at once (the rows come from L2: issued together, their latency is
+      // paid once per U pairs)
+      constexpr int IT = (TP + NW * G - 1) / (NW * G), U = IT < 4 ? IT : 4;
       const int lane = threadIdx.x & 31, q = lane % NS, grp = lane / NS;
       const bool lane_on = grp < G;
+      const int first = (threadIdx.x >> 5) * G + grp;
 #pragma unroll 1
-      for (int base = (threadIdx.x >> 5) * G; base < TP; base += NW * G) {
-        const int pair = base + grp;
-        const bool on = lane_on && pair < TP;
-        const int p = pair % PC, kz = pair / PC, kz2 = L - 1 - kz;
-        R x[NS];
-        C c1[NS], c2[NS];
-        if (on) {
-          const R *ch = sr_chi_row<R>(d, 4 * (pt * PC + p) - d.nx + 1, ay, kz,
-                                      (long long)kz * zs + gbase + p) + q * NS;
-          if constexpr (NS == 4 && sizeof(R) == 4) {
-            const float4 v4 = *reinterpret_cast<const float4 *>(ch);
-            x[0] = v4.x, x[1] = v4.y, x[2] = v4.z, x[3] = v4.w;
-          } else if constexpr (NS == 2 && sizeof(R) == 4) {
-            const float2 v2 = *reinterpret_cast<const float2 *>(ch);
-            x[0] = v2.x, x[1] = v2.y;
-          } else {
+      for (int i0 = 0; i0 < IT; i0 += U) {
+        R x[U][NS];
 #pragma unroll
-            for (int b = 0; b < NS; ++b) x[b] = ch[b];
-          }
+        for (int u = 0; u < U; ++u) {
+          const int pair = first + (i0 + u) * NW * G;
+          if (lane_on && i0 + u < IT && pair < TP) {
+            const int p = pair % PC, kz = pair / PC;
+            const R *ch = sr_chi_row<R>(d, 4 * (pt * PC + p) - d.nx + 1, ay, kz,
+                                        (long long)kz * zs + gbase + p) + q * NS;
+            if constexpr (NS == 4 && sizeof(R) == 4) {
+              const float4 v4 = *reinterpret_cast<const float4 *>(ch);
+              x[u][0] = v4.x, x[u][1] = v4.y, x[u][2] = v4.z, x[u][3] = v4.w;
+            } else if constexpr (NS == 2 && sizeof(R) == 4) {
+              const float2 v2 = *reinterpret_cast<const float2 *>(ch);
+              x[u][0] = v2.x, x[u][1] = v2.y;
+            } else {
 #pragma unroll
-          for (int b = 0; b < NS; ++b) {
-            c1[b] = at(b, kz, p);
-            c2[b] = at(b, kz2, p);
+              for (int b = 0; b < NS; ++b) x[u][b] = ch[b];
+            }
           }
         }
-        __syncwarp();
-        if (on) {
-          R h1r = 0, h1i = 0, h2r = 0, h2i = 0;
 #pragma unroll
-          for (int b = 0; b < NS; ++b) {
-            h1r += c1[b].x * x[b];
-            h1i += c1[b].y * x[b];
-            h2r += c2[b].x * x[b];
-            h2i += c2[b].y * x[b];
+        for (int u = 0; u < U; ++u) {
+          const int pair = first + (i0 + u) * NW * G;
+          const bool on = lane_on && i0 + u < IT && pair < TP;
+          const int p = pair % PC, kz = pair / PC, kz2 = L - 1 - kz;
+          C c1[NS], c2[NS];
+          if (on) {
+#pragma unroll
+            for (int b = 0; b < NS; ++b) {
+              c1[b] = at(b, kz, p);
+              c2[b] = at(b, kz2, p);
+            }
           }
-          at(q, kz, p) = C{h1r, h1i};
-          at(q, kz2, p) = C{h2r, h2i};
+          __syncwarp();
+          if (on) {
+            R h1r = 0, h1i = 0, h2r = 0, h2i = 0;
+#pragma unroll
+            for (int b = 0; b < NS; ++b) {
+              h1r += c1[b].x * x[u][b];
+              h1i += c1[b].y * x[u][b];
+              h2r += c2[b].x * x[u][b];
+              h2i += c2[b].y * x[u][b];
+            }
+            at(q, kz, p) = C{h1r, h1i};
+            at(q, kz2, p) = C{h2r, h2i};
+          }
+          __syncwarp();
         }
-        __syncwarp();
       }
     }
     __syncthreads();
     if constexpr (pl.n > 1) sr_tile_pass<L, RL, 1, 1, NS, PC, NT>(buf, tw);
   }
   if constexpr (pl.n == 3) sr_tile_pass<L, sr_radix(L, 1, true), sr_ns(L, 1, true), 1, NS, PC, NT>(buf, tw);
-  // inverse last pass: shared -> registers -> global
+}
+
+// The inverse transform's last pass: shared tile -> registers -> global
+// (w = the tile's first column of site 0, wb its offset in the spectrum).
+template <typename P, int L, int PC, int NS, int NT>
+__device__ __forceinline__ void sr_zoz_last(const typename Cx<typename P::R>::T *buf,
+                                            const typename Cx<typename P::R>::T *tw,
+                                            const Desc &d, typename Cx<typename P::R>::T *w,
+                                            const typename Cx<typename P::R>::T *pw,
+                                            long long wb, long long wn, long long zs) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  constexpr SrPlan pl = sr_plan(L);
+  auto at = [&](int v, int z, int p) -> const C & { return buf[sr_zi<L, PC>(v, z, p)]; };
+  (void)wb;
+  (void)wn;
+  (void)d;
   {
     constexpr int s = pl.n - 1;
     constexpr int R = sr_radix(L, s, true), NSs = sr_ns(L, s, true), T = NS * PC * (L / R);
+    static_assert(NSs * R == L, "the last pass writes z = j + m L / R");
     for (int task = threadIdx.x; task < T; task += NT) {
       const int p = task % PC, q = task / PC, j = q % (L / R), v = q / (L / R);
       C e[R];
 #pragma unroll
       for (int m = 0; m < R; ++m) e[m] = at(v, sr_in<L, R>(j, m), p);
       sr_pass<L, R, NSs, 1>(e, tw, j);
+      const C pj = pw[j];
 #pragma unroll
       for (int m = 0; m < R; ++m) {
         const int z = sr_out<R, NSs>(j, m);
         const long long gi = v * d.Nhs + z * zs + p;
-        if (R3D_IN(d, wb + gi, wn)) w[gi] = cmul(e[m], cconj(pw[z]));
+        if (R3D_IN(d, wb + gi, wn)) w[gi] = cmul(e[m], cconj(sr_half_twiddle<R>(pj, m)));
       }
     }
   }
+}
+
+template <typename P, int L, int PC, int NS, int NT, bool OZREG>
+__global__ void __launch_bounds__(NT, (OZREG || NT > 256) ? 1 : 2) k_zoz_sr(Batch b) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  constexpr SrPlan pl = sr_plan(L);
+  extern __shared__ __align__(16) char smem[];
+  C *buf = (C *)smem;  // [site][z (padded)][p]
+  C *tw = buf + NS * sr_zrows<L>() * PC;
+  const int si = find_solve(b, blockIdx.x);
+  const Desc &d = b.d[si];
+  if (d.ctl->status != RUNNING) return;
+  const int tile = blockIdx.x - b.prefix[si];
+  const int hx = d.hx, ptiles = hx / PC;
+  const int pt = tile % ptiles, y = tile / ptiles;
+  const long long zs = (long long)d.ny * hx;
+  const C *pw = (const C *)d.pwz;
+  C *w = (C *)d.w + (long long)y * hx + pt * PC;
+  const long long wn = d.n * d.Nhs, wb = (long long)y * hx + pt * PC;
+  (void)wn;
+  (void)wb;
+  for (int e = threadIdx.x; e < L; e += NT) tw[e] = ((const C *)d.twz)[e];
+  const long long ay = 2 * y - d.ny + 1;
+  const long long gbase = (long long)y * hx + pt * PC;
+  auto at = [&](int v, int z, int p) -> C & { return buf[sr_zi<L, PC>(v, z, p)]; };
+
+  // forward pass 0: global -> registers -> shared (the loads of up to 16
+  // values' worth of tasks are issued together: more loads in flight)
+  {
+    constexpr int R0 = pl.r[0], T = NS * PC * (L / R0), K0 = (T + NT - 1) / NT;
+    constexpr int KB = K0 * R0 <= 16 ? K0 : 1;
+#pragma unroll 1
+    for (int k0 = 0; k0 < K0; k0 += KB) {
+      C a[KB][R0];
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) {
+        const int task = threadIdx.x + (k0 + kk) * NT;
+        if (k0 + kk < K0 && (T % NT == 0 || task < T)) {
+          const int p = task % PC, q = task / PC, j = q % (L / R0), v = q / (L / R0);
+#pragma unroll
+          for (int m = 0; m < R0; ++m) {
+            const long long gi = v * d.Nhs + sr_in<L, R0>(j, m) * zs + p;
+            a[kk][m] = R3D_IN(d, wb + gi, wn) ? w[gi] : C{0, 0};
+          }
+        }
+      }
+#pragma unroll
+      for (int kk = 0; kk < KB; ++kk) {
+        const int task = threadIdx.x + (k0 + kk) * NT;
+        if (k0 + kk < K0 && (T % NT == 0 || task < T)) {
+          const int p = task % PC, q = task / PC, j = q % (L / R0), v = q / (L / R0);
+#pragma unroll
+          for (int m = 0; m < R0; ++m) a[kk][m] = cmul(a[kk][m], sr_half_twiddle<R0>(pw[j], m));
+          sr_pass<L, R0, 1, -1>(a[kk], tw, j);
+#pragma unroll
+          for (int m = 0; m < R0; ++m) at(v, sr_out<R0, 1>(j, m), p) = a[kk][m];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  sr_zoz_middle<P, L, PC, NS, NT, OZREG>(buf, tw, d, pt, ay, gbase, zs);
+  sr_zoz_last<P, L, PC, NS, NT>(buf, tw, d, w, pw, wb, wn, zs);
+}
+
+// Persistent z pass: gridDim.x CTAs (one per SM) walk the launch's tiles t =
+// blockIdx.x, blockIdx.x + gridDim.x, ...  A second tile buffer takes the
+// next tile's spectrum with 16-byte asynchronous copies (cp.async) while the
+// current tile is transformed, so that the DRAM reads of tile t + gridDim.x
+// overlap the transforms of tile t; the forward transform's first pass reads
+// the staged tile.  The OZ runs as a shared-memory pass (OZREG false).
+template <typename P, int L, int PC, int NS, int NT>
+__global__ void __launch_bounds__(NT, 1) k_zoz_srp(Batch b, int ntiles) {
+  using R = typename P::R;
+  using C = typename Cx<R>::T;
+  constexpr int TS = NS * sr_zrows<L>() * PC;  // complex values of one tile buffer
+  constexpr int CW = 16 / (int)sizeof(C);      // complex values of one 16-byte copy
+  constexpr int CH = PC / CW;                  // copies per row of a site
+  static_assert(PC % CW == 0, "tile rows of whole 16-byte copies");
+  extern __shared__ __align__(16) char smem[];
+  C *buf = (C *)smem, *stage = buf + TS, *tw = stage + TS;
+  // every solve of a launch has this launch's geometry: one twiddle table
+  for (int e = threadIdx.x; e < L; e += NT) tw[e] = ((const C *)b.d[0].twz)[e];
+  // the copies of tile t into stage (none for a solve that is not running)
+  auto fetch = [&](int t) {
+    const int si = find_solve(b, t);
+    const Desc &d = b.d[si];
+    if (d.ctl->status == RUNNING) {
+      const int tile = t - b.prefix[si];
+      const int hx = d.hx, ptiles = hx / PC, pt = tile % ptiles, y = tile / ptiles;
+      const long long zs = (long long)d.ny * hx;
+      const long long wb = (long long)y * hx + pt * PC, wn = d.n * d.Nhs;
+      const C *w = (const C *)d.w + wb;
+      (void)wn;
+      for (int c = threadIdx.x; c < NS * L * CH; c += NT) {
+        const int q = c % CH, row = c / CH, z = row % L, v = row / L;
+        const long long gi = v * d.Nhs + z * zs + q * CW;
+        if (R3D_IN(d, wb + gi, wn)) cp_async16(stage + sr_zi<L, PC>(v, z, q * CW), w + gi);
+      }
+    }
+    cp_async_commit();
+  };
+  if ((int)blockIdx.x < ntiles) fetch(blockIdx.x);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    cp_async_wait_all();
+    __syncthreads();  // stage holds tile t; the last tile's final pass has read buf
+    const int si = find_solve(b, t);
+    const Desc &d = b.d[si];
+    const bool run = d.ctl->status == RUNNING;  // the same for the whole CTA
+    const int tile = t - b.prefix[si];
+    const int hx = d.hx, ptiles = hx / PC, pt = tile % ptiles, y = tile / ptiles;
+    const long long zs = (long long)d.ny * hx;
+    const long long wb = (long long)y * hx + pt * PC, wn = d.n * d.Nhs;
+    const C *pw = (const C *)d.pwz;
+    if (run) {  // forward pass 0: stage -> registers -> buf
+      constexpr int R0 = sr_plan(L).r[0], T = NS * PC * (L / R0);
+      for (int task = threadIdx.x; task < T; task += NT) {
+        const int p = task % PC, q = task / PC, j = q % (L / R0), v = q / (L / R0);
+        C a[R0];
+        const C pj = pw[j];
+#pragma unroll
+        for (int m = 0; m < R0; ++m)
+          a[m] = cmul(stage[sr_zi<L, PC>(v, sr_in<L, R0>(j, m), p)], sr_half_twiddle<R0>(pj, m));
+        sr_pass<L, R0, 1, -1>(a, tw, j);
+#pragma unroll
+        for (int m = 0; m < R0; ++m) buf[sr_zi<L, PC>(v, sr_out<R0, 1>(j, m), p)] = a[m];
+      }
+    }
+    __syncthreads();  // stage is free for the next tile
+    if (t + (int)gridDim.x < ntiles) fetch(t + gridDim.x);
+    if (!run) continue;
+    sr_zoz_middle<P, L, PC, NS, NT, false>(buf, tw, d, pt, 2LL * y - d.ny + 1,
+                                           (long long)y * hx + pt * PC, zs);
+    sr_zoz_last<P, L, PC, NS, NT>(buf, tw, d, (C *)d.w + wb, pw, wb, wn, zs);
+  }
+  cp_async_wait_all();
 }
 
 // ------------------------------------------------------------ launchers
@@ -749,23 +880,45 @@ template <typename P>
 constexpr int sr_pc_y() {
   return sizeof(typename P::R) == 4 ? 16 : 8;
 }
+#ifndef R3D_SR_ZBASE32
+#define R3D_SR_ZBASE32 32
+#endif
+#ifndef R3D_SR_ZHI
+#define R3D_SR_ZHI 256
+#endif
 template <typename P>
 constexpr int sr_pc_z(int L, int ns) {
-  int base = (sizeof(typename P::R) == 4 ? 32 : 16) / (L >= 512 ? 2 : 1);
+  int base = (sizeof(typename P::R) == 4 ? R3D_SR_ZBASE32 : 16) / (L >= 512 ? 2 : 1);
   int pc = 1;
   while (pc * 2 * ns <= base) pc *= 2;
   return pc;
 }
 // threads of the z pass: register OZ: one OZ task (all sites) per thread,
-// 64..256; shared OZ: one task of the largest-radix pass per thread, 64..512
-// (a whole number of warps: the OZ pass deals pairs out by warp)
+// 64..256; shared OZ: one task of the largest-radix pass per thread, 64..256
+// (two CTAs per SM; measured faster than one CTA of 512 at 256^3 and 512^3
+// with four sites), a whole number of warps: the OZ pass deals pairs out by
+// warp
 template <typename P>
 constexpr int sr_threads_z(int L, int ns, bool ozreg) {
   int t = ozreg ? sr_pc_z<P>(L, ns) * (L / sr_plan(L).r[sr_plan(L).n - 1])
                 : ns * sr_pc_z<P>(L, ns) * (L / sr_max_radix(L));
   t = (t + 31) / 32 * 32;
-  const int hi = ozreg ? 256 : 512;
+  const int hi = ozreg ? 256 : R3D_SR_ZHI;
   return t < 64 ? 64 : (t > hi ? hi : t);
+}
+
+// threads of the persistent z pass: one task of the largest-radix pass per
+// thread, 64..512 whole warps
+template <typename P>
+constexpr int sr_threads_zp(int L, int ns) {
+  int t = ns * sr_pc_z<P>(L, ns) * (L / sr_max_radix(L));
+  t = (t + 31) / 32 * 32;
+  return t < 64 ? 64 : (t > 512 ? 512 : t);
+}
+// tile rows of the persistent z pass are whole 16-byte copies
+template <typename P>
+constexpr bool sr_zp_ok(int L, int ns) {
+  return sr_pc_z<P>(L, ns) % (16 / (int)sizeof(typename Cx<typename P::R>::T)) == 0;
 }
 
 #define R3D_SR_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(72) X(80) X(96) X(128) X(144) X(160) X(192) X(256) X(512)
@@ -776,6 +929,10 @@ size_t sr_smem_z(int L, int PC, int ns, size_t csz) {
   return csz * ((size_t)ns * (L + L / 16 + 1) * PC + L);
 }
 bool sr_length_supported(int L) { return sr_length_ok(L); }
+// the persistent z pass: two tile buffers and the twiddle table
+size_t sr_smem_zp(int L, int PC, int ns, size_t csz) {
+  return csz * (2 * (size_t)ns * (L + L / 16 + 1) * PC + L);
+}
 #endif
 
 template <typename K>
@@ -833,10 +990,81 @@ bool sr_launch_zoz(int L, int ns, bool ozreg, Batch b, int grid, size_t smem, cu
   }
 }
 
+// The persistent z pass over ntiles tiles with `grid` CTAs (false: no
+// kernel for the length and sites).
+template <typename P, int NS>
+static bool sr_launch_zozp_ns(int L, Batch b, int ntiles, int grid, size_t smem, cudaStream_t s) {
+#define R3D_SRZP(LL)                                                        \
+  if (L == LL) {                                                            \
+    if constexpr (sr_zp_ok<P>(LL, NS)) {                                    \
+      constexpr int PC = sr_pc_z<P>(LL, NS), NT = sr_threads_zp<P>(LL, NS);  \
+      k_zoz_srp<P, LL, PC, NS, NT><<<grid, NT, smem, s>>>(b, ntiles);       \
+      return true;                                                          \
+    }                                                                       \
+    return false;                                                           \
+  }
+  R3D_SR_LENGTHS(R3D_SRZP)
+#undef R3D_SRZP
+  return false;
+}
+template <typename P>
+bool sr_launch_zozp(int L, int ns, Batch b, int ntiles, int grid, size_t smem, cudaStream_t s) {
+  grid = grid < ntiles ? grid : ntiles;
+  if (grid < 1) return true;  // no tiles
+  switch (ns) {
+    case 1: return sr_launch_zozp_ns<P, 1>(L, b, ntiles, grid, smem, s);
+    case 2: return sr_launch_zozp_ns<P, 2>(L, b, ntiles, grid, smem, s);
+    case 3: return sr_launch_zozp_ns<P, 3>(L, b, ntiles, grid, smem, s);
+    case 4: return sr_launch_zozp_ns<P, 4>(L, b, ntiles, grid, smem, s);
+    default: return false;
+  }
+}
+// resident CTAs per SM of the persistent z pass (0: no kernel, or it does
+// not fit); its shared-memory attribute must be set (sr_allow_geometry)
+template <typename P, int NS>
+static int sr_occupancy_zozp_ns(int L, size_t smem) {
+  int nb = 0;
+#define R3D_SRZO(LL)                                                                       \
+  if (L == LL) {                                                                           \
+    if constexpr (sr_zp_ok<P>(LL, NS)) {                                                   \
+      constexpr int PC = sr_pc_z<P>(LL, NS), NT = sr_threads_zp<P>(LL, NS);                 \
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zoz_srp<P, LL, PC, NS, NT>, \
+                                                        NT, smem) != cudaSuccess) {       \
+        cudaGetLastError();                                                                \
+        nb = 0;                                                                            \
+      }                                                                                    \
+    }                                                                                      \
+  }
+  R3D_SR_LENGTHS(R3D_SRZO)
+#undef R3D_SRZO
+  return nb;
+}
+template <typename P>
+int sr_occupancy_zozp(int L, int ns, size_t smem) {
+  switch (ns) {
+    case 1: return sr_occupancy_zozp_ns<P, 1>(L, smem);
+    case 2: return sr_occupancy_zozp_ns<P, 2>(L, smem);
+    case 3: return sr_occupancy_zozp_ns<P, 3>(L, smem);
+    case 4: return sr_occupancy_zozp_ns<P, 4>(L, smem);
+    default: return 0;
+  }
+}
+template <typename P>
+int sr_zp_supported(int L, int ns) {
+  int ok = 0;
+#define R3D_SRZS(LL) \
+  if (L == LL) ok = ns == 1 ? sr_zp_ok<P>(LL, 1) : ns == 2 ? sr_zp_ok<P>(LL, 2) : ns == 3 ? sr_zp_ok<P>(LL, 3) : ns == 4 ? sr_zp_ok<P>(LL, 4) : 0;
+  R3D_SR_LENGTHS(R3D_SRZS)
+#undef R3D_SRZS
+  return ok;
+}
+
 template <typename P, int LL, int NS>
 static void sr_allow_zoz() {
   sr_allow(k_zoz_sr<P, LL, sr_pc_z<P>(LL, NS), NS, sr_threads_z<P>(LL, NS, false), false>);
   sr_allow(k_zoz_sr<P, LL, sr_pc_z<P>(LL, NS), NS, sr_threads_z<P>(LL, NS, true), true>);
+  if constexpr (sr_zp_ok<P>(LL, NS))
+    sr_allow(k_zoz_srp<P, LL, sr_pc_z<P>(LL, NS), NS, sr_threads_zp<P>(LL, NS)>);
 }
 
 // x passes: PC rows per tile, PC * (L / R_0) tasks filling the CTA
@@ -912,6 +1140,9 @@ template bool sr_launch_ix<PSR>(int, Batch, int, size_t, cudaStream_t, int);
 template bool sr_launch_fy<PSR>(int, int, Batch, int, size_t, cudaStream_t);
 template bool sr_launch_zoz<PSR>(int, int, bool, Batch, int, size_t, cudaStream_t);
 template void sr_allow_geometry<PSR>(int, int, int, int);
+template bool sr_launch_zozp<PSR>(int, int, Batch, int, int, size_t, cudaStream_t);
+template int sr_occupancy_zozp<PSR>(int, int, size_t);
+template int sr_zp_supported<PSR>(int, int);
 template int sr_pc_y_of<PSR>();
 template int sr_pc_z_of<PSR>(int, int);
 

@@ -29,9 +29,16 @@ def _make(R, refcase, deck, over, prec):
     return s
 
 
+@pytest.mark.parametrize("passes", ["table", "persistent_z"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_batch_equals_solo(refcase, tmp_path, prec):
+def test_batch_equals_solo(refcase, tmp_path, monkeypatch, prec, passes):
+    """passes: the committed variant table, or the Stockham x passes with the
+    persistent z pass (one CTA per SM walking the tiles of every solve of a
+    launch, skipping those of finished solves)."""
     import rism3d as R
+    if passes == "persistent_z":
+        monkeypatch.setenv("R3D_X_VARIANT", "4")
+        monkeypatch.setenv("R3D_YZ_VARIANT", "5")
     solo = []
     for i, (deck, over) in enumerate(SOLVES):
         s = _make(R, refcase, deck, over, prec)

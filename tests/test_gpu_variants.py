@@ -54,13 +54,14 @@ def test_x_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, varian
         s.close()
 
 
-@pytest.mark.parametrize("yz", ["0", "1", "2", "3", "4"])
+@pytest.mark.parametrize("yz", ["0", "1", "2", "3", "4", "5"])
 @pytest.mark.parametrize("case", ["s64nacl", "s_rect", "test1", "g80x72x96", "g80kh"])
 def test_yz_pass_variant_matches_reference(refcase, tmp_path, monkeypatch, yz, case):
     """Every y/z trio against the reference: 0 tile-per-CTA kernels, 1 and 2
     the tensor copy engine (digit-reversed ky layout of the spectrum between
     the passes), 3 and 4 the register-pass Stockham kernels (natural order;
-    the OZ on registers, or as a shared-memory pass of its own)."""
+    the OZ on registers, or as a shared-memory pass of its own), 5 the
+    latter with the persistent z pass that streams its next tile in)."""
     import rism3d as R
     monkeypatch.setenv("R3D_X_VARIANT", "0")
     monkeypatch.setenv("R3D_YZ_VARIANT", yz)
