@@ -285,6 +285,10 @@ struct r3d_ctx {
   // CUDA-event times of the last initialize: potential pair sums, k-space
   // Coulomb sum, long-range h term (refresh), whole initialize (host clock)
   double setup_ms[4] = {0, 0, 0, 0};
+  // refreshes of the FP64 reference during iterations since the last
+  // initialize, and their host-clock time (launch to completion)
+  int refreshes = 0;
+  double refresh_ms = 0;
   unsigned long long h2d = 0, d2h = 0;  // bytes copied each way
 };
 
@@ -1111,6 +1115,7 @@ static size_t refresh_bytes(const Desc &d) {
 // residual of the current t is unchanged in exact arithmetic.
 template <typename P>
 static int refresh(r3d_ctx *c, bool zero) {
+  const auto t_start = std::chrono::steady_clock::now();
   const Desc &d = c->desc;
   const int n = d.n;
   const long long N = d.Ns, Nh = d.Nhs;  // padded site strides
@@ -1167,6 +1172,11 @@ static int refresh(r3d_ctx *c, bool zero) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
   if (tmp != c->rtmp) cudaFreeAsync(tmp, s);
+  if (!zero) {
+    c->refreshes += 1;
+    c->refresh_ms += std::chrono::duration<double, std::milli>(
+                         std::chrono::steady_clock::now() - t_start).count();
+  }
   return R3D_OK;
 }
 
@@ -1678,6 +1688,13 @@ extern "C" int r3d_initialize(r3d_ctx *c) {
   c->setup_ms[3] =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   c->initialized = true;
+  return R3D_OK;
+}
+
+extern "C" int r3d_refresh_timing(const r3d_ctx *c, int *count, double *ms) {
+  if (!c || !count || !ms) return fail(nullptr, R3D_EINVAL, "bad arguments");
+  *count = c->refreshes;
+  *ms = c->refresh_ms;
   return R3D_OK;
 }
 

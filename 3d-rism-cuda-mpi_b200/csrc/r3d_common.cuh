@@ -111,4 +111,29 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
   return s;
 }
 
+// K block-wide sums behind one pair of barriers, each added in the same
+// order as block_sum (the warp's butterfly, then the warps in order), so the
+// results equal K block_sum calls bit for bit; valid in thread 0.  `red`
+// holds K * kThreads/32 doubles.
+template <int K>
+__device__ __forceinline__ void block_sums(double (&v)[K], double *red) {
+  constexpr int NW = kThreads / 32;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k * NW + wid] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double s = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[k * NW + i];
+      v[k] = s;
+    }
+}
+
 }  // namespace r3d

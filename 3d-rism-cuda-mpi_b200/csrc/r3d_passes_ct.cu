@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
   extern __shared__ __align__(16) char smem[];
   C *buf = (C *)smem;
   __shared__ int par[PC];
-  __shared__ double red[kThreads / 32];
+  __shared__ double red6[6 * (kThreads / 32)];
   __shared__ double sums[kPartials];
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
@@ -349,15 +349,12 @@ __global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
   int cur_v = -1;
   auto flush = [&]() {
     if (cur_v < 0) return;
-    double x;
-    x = block_sum(a_ss, red);
-    if (threadIdx.x == 0) sums[0] += x;
-    if (dots) {
-      double q[5] = {a0, a1, a2, a3, a4};
-      for (int k = 0; k < 5; ++k) {
-        x = block_sum(q[k], red);
-        if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
-      }
+    double q[6] = {a_ss, a0, a1, a2, a3, a4};
+    block_sums<6>(q, red6);
+    if (threadIdx.x == 0) {
+      sums[0] += q[0];
+      if (dots)
+        for (int k = 0; k < 5; ++k) sums[1 + 5 * cur_v + k] += q[1 + k];
     }
     a_ss = a0 = a1 = a2 = a3 = a4 = 0;
   };
@@ -460,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
   C *buf = (C *)smem;
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ int par[PC];
-  __shared__ double red[kThreads / 32];
+  __shared__ double red6[6 * (kThreads / 32)];
   __shared__ double sums[kPartials];
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
@@ -520,15 +517,12 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
     const long long row0 = (long long)(tile % tps) * PC;
     if (v != cur_v) {  // uniform: flush the previous site's sums
       if (cur_v >= 0) {
-        double x = block_sum(a_ss, red);
-        if (threadIdx.x == 0) sums[0] += x;
-        if (dots) {
-          const double q[5] = {a0, a1, a2, a3, a4};
-#pragma unroll
-          for (int k = 0; k < 5; ++k) {
-            x = block_sum(q[k], red);
-            if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
-          }
+        double q[6] = {a_ss, a0, a1, a2, a3, a4};
+        block_sums<6>(q, red6);
+        if (threadIdx.x == 0) {
+          sums[0] += q[0];
+          if (dots)
+            for (int k = 0; k < 5; ++k) sums[1 + 5 * cur_v + k] += q[1 + k];
         }
         a_ss = a0 = a1 = a2 = a3 = a4 = 0;
       }
@@ -592,15 +586,12 @@ __global__ void __launch_bounds__(kThreads, PC < (sizeof(typename P::R) == 4 ? 8
     return;
   }
   {
-    double x = block_sum(a_ss, red);
-    if (threadIdx.x == 0) sums[0] += x;
-    if (dots) {
-      const double q[5] = {a0, a1, a2, a3, a4};
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        x = block_sum(q[k], red);
-        if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
-      }
+    double q[6] = {a_ss, a0, a1, a2, a3, a4};
+    block_sums<6>(q, red6);
+    if (threadIdx.x == 0) {
+      sums[0] += q[0];
+      if (dots)
+        for (int k = 0; k < 5; ++k) sums[1 + 5 * cur_v + k] += q[1 + k];
     }
   }
   __syncthreads();
@@ -1257,8 +1248,10 @@ bool ct_launch_fxb(int L, int PC, Batch b, int grid, size_t smem, cudaStream_t s
 }
 
 // The mix-fused FX (mixed precision; false: no kernel for the length).
-// Rows per tile: 4 (2 for rows of 1024 reals).
-constexpr int mfx_pc(int L) { return L >= 512 ? 2 : 4; }
+// Rows per tile: 8 for rows of up to 128 reals (a tile of 4 short rows
+// leaves threads idle and pays the tile's barriers for few elements), 4, and
+// 2 for rows of 1024 reals.
+constexpr int mfx_pc(int L) { return L >= 512 ? 2 : L <= 64 ? 8 : 4; }
 template <typename P>
 bool ct_launch_mfx(int L, Batch b, int grid, size_t smem, cudaStream_t s, int per,
                    int allow_mix) {

@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kThreads) k_ix_sr(Batch b, int per) {
   extern __shared__ __align__(16) char smem[];
   C *buf = (C *)smem;  // [PC][LR]
   C *tw = buf + PC * LR;
-  __shared__ double red[kThreads / 32];
+  __shared__ double red6[6 * (kThreads / 32)];
   __shared__ double sums[kPartials];
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
@@ -303,15 +303,12 @@ __global__ void __launch_bounds__(kThreads) k_ix_sr(Batch b, int per) {
   int cur_v = -1;
   auto flush = [&]() {
     if (cur_v < 0) return;
-    double x = block_sum(a_ss, red);
-    if (threadIdx.x == 0) sums[0] += x;
-    if (dots) {
-      const double q[5] = {a0, a1, a2, a3, a4};
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        x = block_sum(q[k], red);
-        if (threadIdx.x == 0) sums[1 + 5 * cur_v + k] += x;
-      }
+    double q[6] = {a_ss, a0, a1, a2, a3, a4};
+    block_sums<6>(q, red6);
+    if (threadIdx.x == 0) {
+      sums[0] += q[0];
+      if (dots)
+        for (int k = 0; k < 5; ++k) sums[1 + 5 * cur_v + k] += q[1 + k];
     }
     a_ss = a0 = a1 = a2 = a3 = a4 = 0;
   };

@@ -32,7 +32,7 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_load_xvk", "r3d_set_problem", "r3d_set_closure", "r3d_set_mixer",
            "r3d_set_control", "r3d_initialize", "r3d_calculate", "r3d_anderson",
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
-           "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_step",
+           "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_refresh_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
            "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
@@ -113,6 +113,7 @@ def _load():
         "r3d_device_bytes": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_iter_timing": [vp, dp, ip],
         "r3d_setup_timing": [vp, dp],
+        "r3d_refresh_timing": [vp, ip, dp],
         "r3d_step": [vp, ci, dp],
         "r3d_profile_kernels": [vp, ci, ctypes.c_char_p, ci, dp, dp, ip],
         "r3d_status": [vp, ip, dp, ip],
@@ -286,6 +287,13 @@ class RISM3D:
         ms, k = ctypes.c_double(), ctypes.c_int()
         self._check(lib.r3d_iter_timing(self.h, ctypes.byref(ms), ctypes.byref(k)))
         return ms.value, k.value
+
+    def refresh_timing(self):
+        """(count, host ms) of the FP64 reference refreshes the iterations
+        made since initialize (mixed path; (0, 0) on the FP64 path)."""
+        k, ms = ctypes.c_int(), ctypes.c_double()
+        self._check(lib.r3d_refresh_timing(self.h, ctypes.byref(k), ctypes.byref(ms)))
+        return k.value, ms.value
 
     def setup_timing(self):
         """ms of the last initialize: potentials, k-space Coulomb, long-range

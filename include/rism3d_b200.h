@@ -162,6 +162,13 @@ int r3d_iter_timing(const r3d_ctx *ctx, double *ms_per_iter,
  * reference beyond its -DTEST timers (initialize.cu). */
 int r3d_setup_timing(const r3d_ctx *ctx, double *ms);
 
+/* Refreshes of the mixed path's FP64 long-range reference made by the
+ * iterations since r3d_initialize (c_ref frozen at the current t, h_ref
+ * recomputed in FP64), and their host-clock time in ms, launch to
+ * completion.  No counterpart in the reference (its iteration is FP64
+ * throughout); 0 on the FP64 path. */
+int r3d_refresh_timing(const r3d_ctx *ctx, int *count, double *ms);
+
 /* Advance the solve by exactly `nsteps` iterations (graph replays, no
  * convergence polling; converged or diverged solves do no further work) and
  * return their CUDA-event time in *ms.  No counterpart in the reference: the

@@ -148,12 +148,22 @@ def test_debug_build_index_checks_pass(refcase, tmp_path):
     assert out.returncode == 0, out.stderr[-3000:]
     got = json.loads(out.stdout.strip().splitlines()[-1])
     for key, (steps, status, xmu) in got.items():
-        prec = key.split("/")[0]
+        prec, xv, yz = key.split("/")
         assert status == "converged", key
-        s = R.RISM3D(precision=prec)
-        s.initialize(inp, xvk=xvk)
-        ref = s.iterate()
-        ref_xmu = s.thermo()[0]
-        s.close()
+        # the release build with the same pass variants
+        old = {k: os.environ.get(k) for k in ("R3D_X_VARIANT", "R3D_YZ_VARIANT")}
+        os.environ["R3D_X_VARIANT"], os.environ["R3D_YZ_VARIANT"] = xv, yz
+        try:
+            s = R.RISM3D(precision=prec)
+            s.initialize(inp, xvk=xvk)
+            ref = s.iterate()
+            ref_xmu = s.thermo()[0]
+            s.close()
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
         assert abs(steps - ref[0]) <= (1 if prec == "fp64" else 30), key
         np.testing.assert_allclose(xmu, ref_xmu, rtol=1e-6 if prec == "fp64" else 1e-4)
