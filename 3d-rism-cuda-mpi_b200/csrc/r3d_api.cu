@@ -693,7 +693,7 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
       pcb /= 2;
       sm = ct_smem_fxb(d.hx, pcb, cs, fp64 ? 8 : 4, 8);
     }
-    if (rowsN % pcb == 0 && sm <= kSmemMax) {
+    if (rowsN % pcb == 0 && d.ny >= pcb && sm <= kSmemMax) {  // a tile's rows wrap z once at most
       const int tiles = d.n * (rowsN / pcb);
       const int per_sm = bulk_per_sm(c->opts.device, fp64, 0, d.hx, pcb, sm);
       if (per_sm > 0) {
@@ -759,7 +759,7 @@ static int plan_geo(r3d_ctx *c, Desc &d, Geo &g, bool fp64, int nsites) {
   if (!fp64 && c->mixer == MIX_AN2 && d.ct_x && c->opts.device >= 0) {  // mix-fused FX
     const int pc = ct_mfx_pc(d.hx);
     const size_t sm = ct_smem_mfx(d.hx, pc);
-    if (rowsN % pc == 0 && sm <= kSmemMax) {
+    if (rowsN % pc == 0 && d.ny >= pc && sm <= kSmemMax) {  // rows wrap z once at most
       kernels_set_smem(false, kSmemMax);
       const int per_sm = ct_occupancy_mfx<PMix>(d.hx, sm);
       if (per_sm > 0) {

@@ -631,7 +631,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(128) char smem[];
   C *buf = (C *)smem;
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int par[PC];
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
   if (d.ctl->status != RUNNING) return;
@@ -675,13 +674,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int v = tile / tps;
     const long long row0 = (long long)(tile % tps) * PC;
     if (threadIdx.x == 0 && it + 1 < count) issue(tile + 1, st ^ 1);
-    if (threadIdx.x < PC) {
-      const long long row = row0 + threadIdx.x;
-      par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
-    }
+    // parity (y + z) & 1 of row row0 + r in registers (no shared array and
+    // no barrier): y0 and z0 of the tile's first row, y wrapping into the
+    // next z-plane at most once (the planner keeps PC <= ny)
+    const int y0 = (int)(row0 % ny), pz0 = (int)((y0 + row0 / ny) & 1);
     if (!mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls)) failed = true;
     phase ^= 1u << st;
-    __syncthreads();  // par
     const char *sb = smem + BUF + st * St::bytes;
     const T *ts = (const T *)(sb + St::t);
     const R *us = (const R *)(sb + St::u), *cs = (const R *)(sb + St::cref);
@@ -702,8 +700,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         c1 -= (double)cs[i1];
       }
       R f0 = (R)c0, f1 = (R)c1;
-      if ((m + par[r]) & 1) f0 = -f0;
-      if ((m + L + par[r]) & 1) f1 = -f1;
+      const int pr = (pz0 + r + (y0 + r >= ny ? 1 - ny : 0)) & 1;
+      if ((m + pr) & 1) f0 = -f0;
+      if ((m + L + pr) & 1) f1 = -f1;
       buf[digit_rev<L>(m) * LD + r] = cmul(C{f0, -f1}, pw[m]);
     }
     __syncthreads();
@@ -770,7 +769,6 @@ __global__ void __launch_bounds__(kThreads, 2)
   extern __shared__ __align__(128) char smem[];
   C *buf = (C *)smem;
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int par[PC];
   const int si = find_solve(b, blockIdx.x);
   const Desc &d = b.d[si];
   const Ctl *ctl = d.ctl;
@@ -831,13 +829,12 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int v = tile / tps;
     const long long row0 = (long long)(tile % tps) * PC;
     if (threadIdx.x == 0 && it + 1 < count) issue(tile + 1, st ^ 1);
-    if (threadIdx.x < PC) {
-      const long long row = row0 + threadIdx.x;
-      par[threadIdx.x] = (int)((row % ny + row / ny) & 1);
-    }
+    // parity (y + z) & 1 of row row0 + r in registers (no shared array and
+    // no barrier): y0 and z0 of the tile's first row, y wrapping into the
+    // next z-plane at most once (the planner keeps PC <= ny)
+    const int y0 = (int)(row0 % ny), pz0 = (int)((y0 + row0 / ny) & 1);
     if (!mbar_wait(&bar[st], (phase >> st) & 1, d.wait_polls)) failed = true;
     phase ^= 1u << st;
-    __syncthreads();  // par
     const char *sb = smem + BUF + st * St::bytes;
     const double *ts = (const double *)(sb + St::t);
     const R *us = (const R *)(sb + St::u), *cs = (const R *)(sb + St::cref);
@@ -888,8 +885,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         c1 -= (double)cs[i1];
       }
       R f0 = (R)c0, f1 = (R)c1;
-      if ((m + par[r]) & 1) f0 = -f0;
-      if ((m + L + par[r]) & 1) f1 = -f1;
+      const int pr = (pz0 + r + (y0 + r >= ny ? 1 - ny : 0)) & 1;
+      if ((m + pr) & 1) f0 = -f0;
+      if ((m + L + pr) & 1) f1 = -f1;
       buf[digit_rev<L>(m) * LD + r] = cmul(C{f0, -f1}, pw[m]);
     }
     __syncthreads();
