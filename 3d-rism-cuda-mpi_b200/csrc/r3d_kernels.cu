@@ -750,11 +750,15 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int g = 0; g < G; ++g) acc[g] += sv[g] * d.irho[v];
     }
-    block_sums<G>(acc, red);
-    if (threadIdx.x == 0)
+    // one block sum per used slot (a block_sums<G> here raised the kernel
+    // to 170 registers and halved its resident CTAs)
 #pragma unroll
-      for (int g = 0; g < G; ++g)
-        if (g < ng) part[1 + i0 + g] = acc[g];
+    for (int g = 0; g < G; ++g) {
+      if (g < ng) {
+        const double s = block_sum(acc[g], red);
+        if (threadIdx.x == 0) part[1 + i0 + g] = s;
+      }
+    }
   }
 }
 

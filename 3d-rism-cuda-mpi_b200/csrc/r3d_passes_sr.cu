@@ -67,11 +67,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_fy_sr(Batch b) {
       const int p = task % PC, j = task / PC;
       C a[R];
       const C pj = pw[j];  // y = j + m L / R
+      // all R loads issued before any of them is used (more loads in flight),
+      // then the forward transform's half-sample twiddles
 #pragma unroll
       for (int m = 0; m < R; ++m) {
         const int y = sr_in<L, R>(j, m);
         a[m] = R3D_IN(d, wb + (long long)y * hx + p, wn) ? w[(long long)y * hx + p] : C{0, 0};
-        if (!INV) a[m] = cmul(a[m], sr_half_twiddle<R>(pj, m));
+      }
+      if (!INV) {
+#pragma unroll
+        for (int m = 0; m < R; ++m) a[m] = cmul(a[m], sr_half_twiddle<R>(pj, m));
       }
       if constexpr (pl.n == 1) {
         sr_pass<L, R, NS, DIR>(a, tw, j);
