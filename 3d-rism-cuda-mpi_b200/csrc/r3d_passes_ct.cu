@@ -317,8 +317,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(typename P::R) == 4 ? 3 : 2)
 #define R3D_PRAGMA(x) _Pragma(#x)
 #define R3D_UNROLL_N(n) R3D_PRAGMA(unroll n)
 #define R3D_UNROLL(n) R3D_UNROLL_N(n)
+// rows of up to 128 reals: four resident CTAs (64 registers) instead of two,
+// since at those lengths the kernel waits on its global loads
 template <typename P, int L, int PC, int MODE>
-__global__ void __launch_bounds__(kThreads, R3D_IX_MINB)
+__global__ void __launch_bounds__(kThreads, L <= 64 ? 4 : R3D_IX_MINB)
     k_ix_ct(Batch b, typename P::R *dst, int per) {
   using R = typename P::R;
   using T = typename P::T;
@@ -757,8 +759,10 @@ size_t ct_smem_mfx(int L, int PC) {
 #endif
 
 #if !R3D_CT_FP64
+// three resident CTAs for rows of up to 96 reals (their staged tiles fit three
+// times in shared memory), two otherwise
 template <int L, int PC>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, L <= 48 ? 3 : 2)
     k_mfx_bulk(Batch b, int per, int allow_mix) {
   using P = PMix;
   using R = float;
