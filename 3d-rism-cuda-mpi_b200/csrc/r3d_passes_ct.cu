@@ -759,10 +759,10 @@ size_t ct_smem_mfx(int L, int PC) {
 #endif
 
 #if !R3D_CT_FP64
-// three resident CTAs for rows of up to 96 reals (their staged tiles fit three
-// times in shared memory), two otherwise
+// two resident CTAs (three, at 80 registers, spilled and ran 30 % slower at
+// rows of 96 reals)
 template <int L, int PC>
-__global__ void __launch_bounds__(kThreads, L <= 48 ? 3 : 2)
+__global__ void __launch_bounds__(kThreads, 2)
     k_mfx_bulk(Batch b, int per, int allow_mix) {
   using P = PMix;
   using R = float;
