@@ -18,6 +18,7 @@
 #include <cstring>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rism3d_b200.h"
@@ -290,6 +291,9 @@ struct r3d_ctx {
   int refreshes = 0;
   double refresh_ms = 0;
   unsigned long long h2d = 0, d2h = 0;  // bytes copied each way
+  // pinned staging chunks of the grid copies to caller memory (first use)
+  void *pin[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
 // ------------------------------------------------------------------ utils
@@ -455,6 +459,10 @@ extern "C" int r3d_destroy(r3d_ctx *c) {
   cudaSetDevice(c->opts.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_all(c);
+  for (int k = 0; k < 2; ++k) {
+    if (c->pin[k]) cudaFreeHost(c->pin[k]);
+    if (c->pin_ev[k]) cudaEventDestroy(c->pin_ev[k]);
+  }
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return R3D_OK;
@@ -2102,6 +2110,54 @@ static int t_of_residual(r3d_ctx *c, const Ctl &h, const void **out) {
   return R3D_OK;
 }
 
+// Device -> caller host memory (pageable, as a numpy array is) through two
+// pinned staging chunks: the DMA of chunk i + 1 runs while chunk i is copied
+// from its staging buffer to the destination, split over several host
+// threads (which also share the first-touch page faults of a fresh
+// destination).  A direct pageable copy of a 256^3 x 4-site FP64 grid went
+// through the driver's own staging at a fraction of the link's rate.
+constexpr size_t kPinChunk = 32u << 20;
+static int copy_out(r3d_ctx *c, void *host, const void *dsrc, size_t bytes, cudaStream_t s) {
+  if (bytes < (4u << 20)) {  // small: one ordinary copy
+    CK(copy_d2h(c, host, dsrc, bytes, s));
+    CK(cudaStreamSynchronize(s));
+    return R3D_OK;
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (!c->pin[k]) CK(cudaMallocHost(&c->pin[k], kPinChunk));
+    if (!c->pin_ev[k]) CK(cudaEventCreateWithFlags(&c->pin_ev[k], cudaEventDisableTiming));
+  }
+  const size_t n = (bytes + kPinChunk - 1) / kPinChunk;
+  const int nt = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  auto dma = [&](size_t i) -> cudaError_t {
+    const size_t off = i * kPinChunk, len = std::min(kPinChunk, bytes - off);
+    cudaError_t e = cudaMemcpyAsync(c->pin[i & 1], (const char *)dsrc + off, len,
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(c->pin_ev[i & 1], s);
+    return e;
+  };
+  CK(dma(0));
+  for (size_t i = 0; i < n; ++i) {
+    // chunk i + 1 into the other buffer, whose previous chunk (i - 1) has
+    // already been copied out
+    if (i + 1 < n) CK(dma(i + 1));
+    CK(cudaEventSynchronize(c->pin_ev[i & 1]));
+    const size_t off = i * kPinChunk, len = std::min(kPinChunk, bytes - off);
+    const char *src = (const char *)c->pin[i & 1];
+    char *dst = (char *)host + off;
+    const size_t part = (len / nt + 63) / 64 * 64;
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) {
+      const size_t a = std::min(len, t * part), b = std::min(len, (t + 1) * part);
+      if (a < b) th.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+    }
+    std::memcpy(dst, src, std::min(len, part));
+    for (auto &x : th) x.join();
+  }
+  c->d2h += bytes;
+  return R3D_OK;
+}
+
 static int ensure_scratch(r3d_ctx *c, size_t bytes) {
   if (c->scratch_bytes >= bytes) return R3D_OK;
   if (c->scratch) {
@@ -2239,8 +2295,7 @@ extern "C" int r3d_get_grid(r3d_ctx *c, int which, double *host) {
       return fail(c, R3D_EINVAL, "unknown grid");
   }
   CK(cudaGetLastError());
-  CK(copy_d2h(c, host, c->scratch, count * 8, s));
-  CK(cudaStreamSynchronize(s));
+  if ((rc = copy_out(c, host, c->scratch, count * 8, s))) return rc;
   if (which == R3D_GRID_FK) {  // transform units -> physical beta phi_L(k)
     const Problem &p = c->prob;
     const double dv = p.box[0] * p.box[1] * p.box[2] / (double)d.N;

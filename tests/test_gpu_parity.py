@@ -142,6 +142,24 @@ def test_mixed_precision_within_tolerance(R, refcase, case, tmp_path):
     assert_xmu_mixed(got, ref)
 
 
+def test_refresh_timing_counts_the_mixed_refreshes(R, refcase):
+    """r3d_refresh_timing: a mixed solve to RMS 1e-6 refreshes its FP64
+    long-range reference several times (from RMS 3e-2, then at every factor
+    0.3), each taking host time; the FP64 path has none."""
+    inp, xvk = refcase("s64nacl")
+    got = {}
+    for prec in ("mixed", "fp64"):
+        s = _solver(R, inp, xvk, prec=prec)
+        assert s.refresh_timing() == (0, 0.0)
+        steps, rms, status = s.iterate()
+        assert status == "converged"
+        got[prec] = s.refresh_timing()
+        s.close()
+    count, ms = got["mixed"]
+    assert 5 <= count <= 20 and ms > 0, got
+    assert got["fp64"] == (0, 0.0)
+
+
 def test_mixed_maxstep_results_are_of_the_last_evaluation(R, refcase):
     """A solve stopped by maxstep mixes at its last step too, so its results
     (g, thermo) belong to the t before that mix.  The mixed path keeps the AN2
