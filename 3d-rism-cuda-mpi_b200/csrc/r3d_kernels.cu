@@ -1108,9 +1108,11 @@ __global__ void __launch_bounds__(kThreads)
           if (r2[j] >= 1.0e-10) {  // r >= 1e-5 A
             const double qr = azq.y * ir[j];
             const double ra = r2[j] * ir[j];
-            const double em = ra <= 38.0 ? exp(-ra) : 0.0;
             e[j] += qr;
-            f[j] = fma(qr, 1.0 - em, f[j]);
+            if (ra <= 38.0)  // a branch, so that far pairs skip the exponential
+              f[j] = fma(qr, 1.0 - exp(-ra), f[j]);
+            else
+              f[j] += qr;  // = fma(qr, 1 - 0, f)
           } else {
             f[j] += azq.y;
           }
