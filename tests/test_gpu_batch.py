@@ -91,3 +91,56 @@ def test_batch_rejects_bad_members(refcase):
     b.close()
     a.close()
     m.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_48_grid_matches_oracle_and_batches(solvents, tmp_path, prec):
+    """48^3 cells (the smallest grid the batched screen's configuration
+    names, which its solute-plus-buffer rule never reaches): two small
+    solutes solved alone match the oracle (FP64: steps within 1, mu_ex per
+    site within 1e-6 kcal/mol; mixed: within 0.01 kcal/mol), and batched
+    they end exactly where they end alone."""
+    import oracle as O
+    import rism3d as R
+    import synthetic as S
+    xvk = solvents["h2o_vv"]
+    decks = [S.small(str(tmp_path), nu=8 + 4 * k, grid=48, box=24.0, solvent=xvk, seed=30 + k,
+                     name=f"g48_{k}") for k in range(2)]
+    kt_per_kcal = 4184.0 / (8.314462618 * 300.0)  # 1 kcal/mol in kT at the table's 300 K
+    tol = (1e-6 if prec == "fp64" else 1e-2) * kt_per_kcal
+    solo = []
+    for k, inp in enumerate(decks):
+        s = R.RISM3D(precision=prec)
+        s.initialize(inp, xvk=xvk)
+        steps, rms, status = s.iterate()
+        xmu = s.thermo()[0]
+        p = tmp_path / f"solo{k}.xmu"
+        s.output(str(p))
+        solo.append((steps, status, p.read_text()))
+        s.close()
+        o = O.Oracle(inp, xvk=xvk)
+        o.initialize()
+        osteps, orms, ostatus = o.iterate()
+        oxmu = o.thermo()[0]
+        assert status == ostatus == "converged", (status, ostatus)
+        if prec == "fp64":
+            assert abs(steps - osteps) <= 1, (steps, osteps)
+        assert max(abs(a - b) for a, b in zip(xmu, oxmu)) < tol, (xmu, oxmu)
+    ctxs = []
+    for inp in decks:
+        s = R.RISM3D(precision=prec)
+        s.initialize(inp, xvk=xvk)
+        ctxs.append(s)
+    b = R.Batch()
+    for s in ctxs:
+        b.add(s)
+    b.iterate()
+    for k, s in enumerate(ctxs):
+        steps, rms, status = s.status()
+        assert (steps, status) == solo[k][:2]
+        p = tmp_path / f"batch{k}.xmu"
+        s.output(str(p))
+        assert p.read_text() == solo[k][2]
+    b.close()
+    for s in ctxs:
+        s.close()
