@@ -218,3 +218,178 @@ def allreduce_sums(values, group=None):
     t = torch.tensor(np.asarray(values, dtype=np.float64))
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return t.numpy()
+
+
+# ------------------------------------------------------ a distributed solve
+# The reference splits one solve over MPI ranks: every array of RISM3D is cut
+# in pencils, the transforms of calculate() move them with Alltoall, and the
+# RMS (cal_rms.cu:23) and the AN2 dot products (anderson.cu:95) are summed
+# over ranks with Allreduce, so that every rank takes the same convergence
+# and mixing decisions (iterate.cu:48-82).  Here rank r keeps its z-slab of
+# the real-space arrays (u, phi_L(r), t, g, the residual and the AN2 slots)
+# and its y-slab of the k-space ones (chi and phi_L(k) on its half-spectrum
+# points); one evaluation is
+#   closure and c = g - 1 - t + q_v beta phi_L(r) on the z-slab (trm1mt),
+#   x and y transforms, all-to-all, z transform,
+#   C - q_v beta phi_L(k) and the OZ sum H_v = sum_v' chi_vv' (...) on the
+#   y-slab (mqvfk, oz), inverse z, all-to-all, inverse y and x,
+#   R = h + 1 - g and its partial sums on the z-slab (tr, cal_rms),
+# with the reference's FP64 arithmetic.  k-space arrays are in the transform
+# units of the stages: the closed-form shifted transform divided by dv C(k)
+# (C(k) = -i (-1)^(jx + jy + jz + (nx + ny + nz)/2), k_x index 2p), so that
+# h = (2 / N) times the inverse stages' output.
+
+KH, HNC, PSE = 0, 1, 2
+
+
+class NumpyOps:
+    """Pointwise steps of one evaluation on numpy arrays (CPU ranks)."""
+
+    @staticmethod
+    def closure_c(clos, pse_n, du, t, fr, qv):
+        """g = closure(-u + t) (calculate_cuda.cu:1-16, PSE-n), c = g - 1 - t +
+        q_v fr (trm1mt), per site."""
+        earg = -du + t
+        if clos == HNC:
+            g = np.exp(earg)
+        else:
+            pos = earg >= 0.0
+            if clos == KH or pse_n == 1:
+                gp = 1.0 + earg
+            else:
+                term = np.ones_like(earg)
+                gp = np.ones_like(earg)
+                for i in range(1, pse_n + 1):
+                    term = term * earg / i
+                    gp = gp + term
+            g = np.where(pos, gp, np.exp(np.minimum(earg, 0.0)))
+        c = g - 1.0 - t + qv[:, None, None, None] * fr[None]
+        return g, c
+
+    @staticmethod
+    def oz(spec, chi, fk, qv):
+        """mqvfk and oz (calculate_cuda.cu:39-52) on the y-slab: H_v =
+        sum_v' chi_vv' (C_v' - q_v' fk)."""
+        cs = spec - qv[:, None, None, None] * fk[None]
+        return np.einsum("abzyp,bzyp->azyp", chi, cs)
+
+    @staticmethod
+    def residual(h, g, rp, dots):
+        """R = h + 1 - g (tr), sum R^2 and, when dots, the five AN2 theta dots
+        per site against the two stored residuals (anderson_cuda.cu:25-67)."""
+        r = h + 1.0 - g
+        sums = [float(np.sum(r * r))]
+        if dots:
+            for v in range(r.shape[0]):
+                t1 = r[v] - rp[0][v]
+                t2 = r[v] - rp[1][v]
+                sums += [float(np.sum(r[v] * t1)), float(np.sum(r[v] * t2)),
+                         float(np.sum(t1 * t1)), float(np.sum(t1 * t2)), float(np.sum(t2 * t2))]
+        return r, sums
+
+    @staticmethod
+    def mix(t, r, tp, rp, binary, coef, m):
+        """newdt0 (coef None: t += R) or newdt (anderson_cuda.cu:1-22); the
+        current t and R go to slot `binary`."""
+        if coef is None:
+            tp[binary] = t.copy()
+            rp[binary] = r.copy()
+            return t + r
+        s1, s2 = coef
+        u = t + s1 * (tp[0] - t) + s2 * (tp[1] - t)
+        w = t + r + s1 * (tp[0] + rp[0] - t - r) + s2 * (tp[1] + rp[1] - t - r)
+        tp[binary] = t.copy()
+        rp[binary] = r.copy()
+        return u + m * (w - u)
+
+
+def leg2(a, c):
+    """leg (anderson.cu:105-130) for n = 2: Gaussian elimination, no pivoting."""
+    a = list(a)
+    c = list(c)
+    p = a[0]
+    a[1] /= p
+    c[0] /= p
+    r = c[0]
+    q = a[2]
+    a[3] -= q * a[1]
+    c[1] -= q * r
+    x1 = c[1] / a[3]
+    x0 = c[0] - a[1] * x1
+    return x0, x1
+
+
+class DistSolve:
+    """One 3D-RISM solve split over the ranks of a torch.distributed group
+    (FP64, AN2 mixing; the reference's RISM3D::iterate over MPI ranks).
+
+    Rank `rank` passes its slabs: du, t [n][nzl][ny][nx] (beta u and the
+    initial t of its z-slab), fr [nzl][ny][nx] (beta phi_L(r)), chi
+    [n][n][nz][nyl][nx/2] and fk [nz][nyl][nx/2] (its y-slab, transform
+    units).  `stages` transforms (NumpyStages or CudaStages), `ops` the
+    pointwise steps (NumpyOps), `xp` the array module those work on."""
+
+    def __init__(self, plan, rank, du, t, fr, chi, fk, qv, rhov, closure=(KH, 1),
+                 mixer=(2, 0.6, 0.2), tol=1e-6, maxstep=10000, stages=None, ops=None,
+                 group=None):
+        self.plan, self.rank, self.group = plan, rank, group
+        self.du, self.t, self.fr, self.chi, self.fk = du, t, fr, chi, fk
+        self.qv = np.asarray(qv, dtype=np.float64)
+        self.irho = 1.0 / np.asarray(rhov, dtype=np.float64)
+        self.clos, self.pse_n = closure
+        self.count, self.m, self.mp = int(mixer[0]), float(mixer[1]), float(mixer[2])
+        self.tol, self.maxstep = tol, maxstep
+        self.stages = stages or NumpyStages()
+        self.ops = ops or NumpyOps()
+        self.n = len(self.qv)
+        self.N = plan.nx * plan.ny * plan.nz
+        self.tp = [np.zeros_like(t), np.zeros_like(t)]
+        self.rp = [np.zeros_like(t), np.zeros_like(t)]
+        self.r = None
+        self.g = None
+
+    def calculate(self, dots):
+        """One evaluation; returns the RMS over the whole grid and the AN2
+        dots summed over ranks (cal_rms.cu:14-26, anderson.cu:81-102)."""
+        n, plan, rank = self.n, self.plan, self.rank
+        g, c = self.ops.closure_c(self.clos, self.pse_n, self.du, self.t, self.fr, self.qv)
+        spec = np.stack([forward(c[v], plan, rank, self.stages, self.group) for v in range(n)])
+        hk = self.ops.oz(spec, self.chi, self.fk, self.qv)
+        h = np.stack([inverse(hk[v], plan, rank, self.stages, self.group) for v in range(n)])
+        h *= 2.0 / self.N
+        self.r, sums = self.ops.residual(h, g, self.rp, dots)
+        self.g = g
+        tot = allreduce_sums(sums, self.group)
+        rms = float(np.sqrt(tot[0] / (self.N * n)))
+        return rms, tot[1:]
+
+    def iterate(self):
+        """RISM3D::iterate (iterate.cu:48-82) with AN2::initialize at its
+        start: (steps, rms, 'converged' | 'maxstep' | 'diverged')."""
+        binary, count_left = 0, self.count
+        rms, step = 0.0, 0
+        for step in range(1, self.maxstep + 1):
+            rms, dsum = self.calculate(dots=count_left <= 0)
+            if not np.isfinite(rms):
+                return step, rms, "diverged"
+            if rms <= self.tol:
+                return step, rms, "converged"
+            if count_left > 0:  # newdt0
+                count_left -= 1
+                coef = None
+            else:  # cal_theta over sites, leg, the mp bias
+                c, a = [0.0, 0.0], [0.0, 0.0, 0.0, 0.0]
+                for v in range(self.n):
+                    s = dsum[5 * v:5 * v + 5]
+                    c[0] += s[0] * self.irho[v]
+                    c[1] += s[1] * self.irho[v]
+                    a[0] += s[2] * self.irho[v]
+                    a[1] += s[3] * self.irho[v]
+                    a[3] += s[4] * self.irho[v]
+                a[2] = a[1]
+                x0, x1 = leg2(a, c)
+                coef = (x0 + self.mp * (0 if binary == 0 else 1),
+                        x1 + self.mp * (1 if binary == 0 else 0))
+            self.t = self.ops.mix(self.t, self.r, self.tp, self.rp, binary, coef, self.m)
+            binary = 1 - binary
+        return step, rms, "maxstep"

@@ -155,3 +155,66 @@ def test_gpu_stages_match_with_two_emulated_ranks():
             parts.append(sends[s][off:off + counts[r]])
         back = cs.inverse_xy(to_t(slabs.unpack_y2z(np.concatenate(parts), plan, r))).cpu().numpy()
         np.testing.assert_allclose(back, f[plan.zslab(r)] * f.size / 2, atol=1e-9 * f.size)
+
+
+SOLVE_SCRIPT = r"""
+import json, sys
+import numpy as np
+sys.path.insert(0, %(pkg)r)
+sys.path.insert(0, %(oracle)r)
+import replicas, slabs
+import oracle as O
+g = replicas.Group("gloo", timeout_s=120)
+o = O.Oracle(%(inp)r, xvk=%(xvk)r)
+o.initialize()
+(nx, ny, nz), box, _ = o.grid()
+plan = slabs.SlabPlan(nz, ny, nx, g.world)
+du, t0, fr, fk, chi = (o.get(k) for k in ("u", "t", "fr", "fk", "chi"))
+sol = o.solvent()
+# k-space arrays in the stages' units: the closed-form transform over dv C(k)
+dv = float(np.prod(box)) / (nx * ny * nz)
+kz, ky, p = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx // 2), indexing="ij")
+sigma = (-1.0) ** (2 * p + ky + kz + ((nx + ny + nz) // 2))
+fk_s = (1j * sigma * fk[:, :, 0::2] / dv)[:, plan.yslab(g.rank)]
+chi_s = chi[:, :, :, :, 0::2][:, :, :, plan.yslab(g.rank)]
+zs = plan.zslab(g.rank)
+ds = slabs.DistSolve(plan, g.rank, du[:, zs].copy(), t0[:, zs].copy(), fr[zs].copy(),
+                     chi_s.copy(), fk_s.copy(), sol["qv"], sol["rhov"])
+steps, rms, status = ds.iterate()
+with open(%(out)r + str(g.rank) + ".json", "w") as fo:
+    json.dump({"steps": steps, "rms": rms, "status": status, "z": [plan.z0[g.rank], plan.nzl[g.rank]],
+               "t": ds.t.tolist()}, fo)
+g.close()
+"""
+
+
+def test_distributed_solve_on_two_gloo_ranks(tmp_path):
+    """One solve split over two ranks (z-slabs for the real-space arrays,
+    y-slabs for the k-space ones; the reference's RISM3D::iterate over MPI
+    ranks, with the RMS and AN2 dots summed over ranks) takes the oracle's
+    iterations to the oracle's t: same step count and RMS, t within
+    1e-9."""
+    import oracle as O
+    import synthetic as S
+    from conftest import unpack
+    xvk = unpack("h2o_vv.xvk.gz", str(tmp_path))
+    inp = S.small(str(tmp_path), nu=8, grid=32, box=16.0, solvent=xvk, name="dist")
+    script = tmp_path / "solve.py"
+    out_stem = str(tmp_path / "solve")
+    script.write_text(SOLVE_SCRIPT % {"pkg": PKG, "oracle": os.path.join(ROOT, "oracle"),
+                                      "inp": inp, "xvk": xvk, "out": out_stem})
+    code = (f"import sys; sys.path.insert(0, {PKG!r}); import replicas; "
+            f"sys.exit(replicas.launch(2, [{str(script)!r}], timeout_s=300))")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr[-3000:]
+    res = [json.load(open(out_stem + f"{r}.json")) for r in range(2)]
+    o = O.Oracle(inp, xvk=xvk)
+    o.initialize()
+    steps, rms, status = o.iterate()
+    t = o.get("t")
+    for r in res:
+        assert (r["steps"], r["status"]) == (steps, status)
+        assert r["rms"] == pytest.approx(rms, rel=1e-8)
+        z0, nzl = r["z"]
+        np.testing.assert_allclose(np.array(r["t"]), t[:, z0:z0 + nzl], atol=1e-9)
