@@ -2285,11 +2285,24 @@ extern "C" int r3d_get_grid(r3d_ctx *c, int which, double *host) {
         launch_gh<PMix>(d, tg, g, hh, s);
       break;
     }
-    case R3D_GRID_FK: {
+    case R3D_GRID_FK: case R3D_GRID_FKT: {
       count = 2 * d.Nh;
       if ((rc = ensure_scratch(c, count * 8))) return rc;
       launch_to_double<P64>(c->fk, c->scratch, count, 0, s);  // FP64 always
       break;
+    }
+    case R3D_GRID_CHI: {  // the shell table (FP64, times 2/N) through each point's shell
+      const int n = d.n, chis = d.chis;
+      std::vector<uint32_t> kidx((size_t)d.Nh);
+      std::vector<double> tab((size_t)c->nshell * chis);
+      CK(copy_d2h(c, kidx.data(), c->kidx, kidx.size() * 4, s));
+      CK(copy_d2h(c, tab.data(), c->chi64, tab.size() * 8, s));
+      CK(cudaStreamSynchronize(s));
+      const double un = (double)d.N / 2.0;
+      for (int q = 0; q < n * n; ++q)
+        for (long long i = 0; i < d.Nh; ++i)
+          host[(size_t)q * d.Nh + i] = tab[(size_t)kidx[i] * chis + q] * un;
+      return R3D_OK;
     }
     default:
       return fail(c, R3D_EINVAL, "unknown grid");

@@ -24,7 +24,7 @@ KH, HNC, PSE = 0, 1, 2
 MIX_AN2, MIX_ANM = 0, 1
 CONVERGED, MAXSTEP, DIVERGED = 0, 1, 2
 STATUS = {CONVERGED: "converged", MAXSTEP: "maxstep", DIVERGED: "diverged"}
-GRID = {"u": 0, "t": 1, "g": 2, "h": 3, "R": 4, "fr": 5, "fk": 6}
+GRID = {"u": 0, "t": 1, "g": 2, "h": 3, "R": 4, "fr": 5, "fk": 6, "fkt": 7, "chi": 8}
 ERRORS = {1: "EINVAL", 2: "EIO", 3: "ECUDA", 4: "ENOMEM", 5: "ESTATE", 6: "EBUDGET"}
 
 # every entry point include/rism3d_b200.h declares
@@ -34,7 +34,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
            "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_refresh_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
-           "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
+           "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_dist_closure", "r3d_dist_oz",
+           "r3d_dist_residual", "r3d_dist_mix", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
            "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
            "r3d_server_destroy", "r3d_write_guv", "r3d_write_huv", "r3d_write_cuv",
@@ -122,6 +123,10 @@ def _load():
         "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
         "r3d_fft3d_noalloc": [ci, ci, ci, ci, dp, ci, vp, vp, vp],
         "r3d_slab_transform": [ci, ci, ci, ci, ci, vp, vp, vp],
+        "r3d_dist_closure": [ci, ci, ctypes.c_longlong, ci, ci, vp, vp, vp, dp, vp, vp, vp],
+        "r3d_dist_oz": [ci, ci, ctypes.c_longlong, vp, vp, dp, vp, vp],
+        "r3d_dist_residual": [ci, ci, ctypes.c_longlong, cd, vp, vp, vp, vp, ci, vp, vp, vp],
+        "r3d_dist_mix": [ci, ctypes.c_longlong, vp, vp, vp, vp, vp, vp, ci, ci, cd, cd, cd, vp],
         "r3d_batch_create": [ci, ctypes.POINTER(vp)],
         "r3d_batch_add": [vp, vp],
         "r3d_batch_iterate": [vp, ip, dp],
@@ -343,10 +348,14 @@ class RISM3D:
         nx, ny, nz = inf["grid"]
         n = inf["natv"]
         k = GRID[which]
-        if k == GRID["fk"]:
+        if k in (GRID["fk"], GRID["fkt"]):
             out = np.zeros(2 * (nx // 2) * ny * nz)
             self._check(lib.r3d_get_grid(self.h, k, _dp(out)))
             return (out[0::2] + 1j * out[1::2]).reshape(nz, ny, nx // 2)
+        if k == GRID["chi"]:
+            out = np.zeros(n * n * (nx // 2) * ny * nz)
+            self._check(lib.r3d_get_grid(self.h, k, _dp(out)))
+            return out.reshape(n, n, nz, ny, nx // 2)
         out = np.zeros((1 if k == GRID["fr"] else n) * nx * ny * nz)
         self._check(lib.r3d_get_grid(self.h, k, _dp(out)))
         return out.reshape(nz, ny, nx) if k == GRID["fr"] else out.reshape(n, nz, ny, nx)

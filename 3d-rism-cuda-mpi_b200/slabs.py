@@ -182,6 +182,8 @@ def all_to_all(send, send_counts, recv_counts, group):
     """One all-to-all of complex128 numpy buffers (as float64 pairs)."""
     import torch
     import torch.distributed as dist
+    if not dist.is_initialized():  # one rank, no process group: nothing moves
+        return np.ascontiguousarray(send)
     s = torch.from_numpy(np.ascontiguousarray(send).view(np.float64))
     r = torch.empty(2 * sum(recv_counts), dtype=torch.float64)
     dist.all_to_all_single(r, s, output_split_sizes=[2 * c for c in recv_counts],
@@ -215,6 +217,8 @@ def allreduce_sums(values, group=None):
     (cal_rms.cu:23, anderson.cu:95)."""
     import torch
     import torch.distributed as dist
+    if not dist.is_initialized():  # one rank, no process group
+        return np.asarray(values, dtype=np.float64)
     t = torch.tensor(np.asarray(values, dtype=np.float64))
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return t.numpy()
@@ -274,10 +278,31 @@ class NumpyOps:
         return np.einsum("abzyp,bzyp->azyp", chi, cs)
 
     @staticmethod
-    def residual(h, g, rp, dots):
-        """R = h + 1 - g (tr), sum R^2 and, when dots, the five AN2 theta dots
-        per site against the two stored residuals (anderson_cuda.cu:25-67)."""
-        r = h + 1.0 - g
+    def forward(c, plan, rank, stages, group):
+        return forward(c, plan, rank, stages, group)
+
+    @staticmethod
+    def inverse(h, plan, rank, stages, group):
+        return inverse(h, plan, rank, stages, group)
+
+    @staticmethod
+    def stack(xs):
+        return np.stack(xs)
+
+    @staticmethod
+    def zeros_like(x):
+        return np.zeros_like(x)
+
+    @staticmethod
+    def allreduce(sums, group):
+        return allreduce_sums(sums, group)
+
+    @staticmethod
+    def residual(h, scale, g, rp, dots):
+        """R = scale h + 1 - g (tr), sum R^2 and, when dots, the five AN2
+        theta dots per site against the two stored residuals
+        (anderson_cuda.cu:25-67)."""
+        r = h * scale + 1.0 - g
         sums = [float(np.sum(r * r))]
         if dots:
             for v in range(r.shape[0]):
@@ -343,23 +368,24 @@ class DistSolve:
         self.ops = ops or NumpyOps()
         self.n = len(self.qv)
         self.N = plan.nx * plan.ny * plan.nz
-        self.tp = [np.zeros_like(t), np.zeros_like(t)]
-        self.rp = [np.zeros_like(t), np.zeros_like(t)]
+        self.tp = [self.ops.zeros_like(t), self.ops.zeros_like(t)]
+        self.rp = [self.ops.zeros_like(t), self.ops.zeros_like(t)]
         self.r = None
         self.g = None
 
     def calculate(self, dots):
         """One evaluation; returns the RMS over the whole grid and the AN2
         dots summed over ranks (cal_rms.cu:14-26, anderson.cu:81-102)."""
-        n, plan, rank = self.n, self.plan, self.rank
-        g, c = self.ops.closure_c(self.clos, self.pse_n, self.du, self.t, self.fr, self.qv)
-        spec = np.stack([forward(c[v], plan, rank, self.stages, self.group) for v in range(n)])
-        hk = self.ops.oz(spec, self.chi, self.fk, self.qv)
-        h = np.stack([inverse(hk[v], plan, rank, self.stages, self.group) for v in range(n)])
-        h *= 2.0 / self.N
-        self.r, sums = self.ops.residual(h, g, self.rp, dots)
+        n, plan, rank, ops = self.n, self.plan, self.rank, self.ops
+        g, c = ops.closure_c(self.clos, self.pse_n, self.du, self.t, self.fr, self.qv)
+        spec = ops.stack([ops.forward(c[v], plan, rank, self.stages, self.group)
+                          for v in range(n)])
+        hk = ops.oz(spec, self.chi, self.fk, self.qv)
+        h = ops.stack([ops.inverse(hk[v], plan, rank, self.stages, self.group)
+                       for v in range(n)])
+        self.r, sums = ops.residual(h, 2.0 / self.N, g, self.rp, dots)
         self.g = g
-        tot = allreduce_sums(sums, self.group)
+        tot = ops.allreduce(sums, self.group)
         rms = float(np.sqrt(tot[0] / (self.N * n)))
         return rms, tot[1:]
 
@@ -393,3 +419,121 @@ class DistSolve:
             self.t = self.ops.mix(self.t, self.r, self.tp, self.rp, binary, coef, self.m)
             binary = 1 - binary
         return step, rms, "maxstep"
+
+
+class CudaOps:
+    """The same steps on one GPU (torch float64 tensors; complex spectra as
+    [..., 2] pairs): the pointwise ones by the library's r3d_dist_* kernels,
+    the transforms by r3d_slab_transform (`stages`: CudaStages), the
+    all-to-alls and sums by NCCL through torch.distributed (device
+    tensors)."""
+
+    def __init__(self, lib, device=0):
+        import torch
+        self.lib, self.device = lib, device
+        self.sums = torch.zeros(R3D_DIST_SUMS_DOUBLES, dtype=torch.float64,
+                                device=f"cuda:{device}")
+
+    def _stream(self):
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(self.lib.r3d_last_error(None).decode())
+
+    @staticmethod
+    def _p(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    @staticmethod
+    def _q(qv):
+        a = np.ascontiguousarray(qv, dtype=np.float64)
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a
+
+    def closure_c(self, clos, pse_n, du, t, fr, qv):
+        import torch
+        g, c = torch.empty_like(t), torch.empty_like(t)
+        qp, keep = self._q(qv)
+        self._check(self.lib.r3d_dist_closure(self.device, t.shape[0], t[0].numel(), clos, pse_n,
+                                              self._p(du), self._p(t), self._p(fr), qp,
+                                              self._p(g), self._p(c), self._stream()))
+        return g, c
+
+    @staticmethod
+    def _a2a(send, send_counts, recv_counts, group):
+        import torch
+        import torch.distributed as dist
+        if not dist.is_initialized():
+            return send
+        recv = torch.empty(2 * sum(recv_counts), dtype=send.dtype, device=send.device)
+        dist.all_to_all_single(recv, send, output_split_sizes=[2 * k for k in recv_counts],
+                               input_split_sizes=[2 * k for k in send_counts], group=group)
+        return recv
+
+    def forward(self, c, plan, rank, stages, group):
+        import torch
+        spec_z = stages.forward_xy(c.contiguous())
+        send = torch.cat([spec_z[:, plan.yslab(s)].reshape(-1) for s in range(plan.world)])
+        recv = self._a2a(send, plan.send_counts_z2y(rank), plan.recv_counts_z2y(rank), group)
+        parts = torch.split(recv, [2 * k for k in plan.recv_counts_z2y(rank)])
+        spec_y = torch.cat([p.view(plan.nzl[s], plan.nyl[rank], plan.hx, 2)
+                            for s, p in enumerate(parts)], dim=0).contiguous()
+        return stages.forward_z(spec_y)
+
+    def inverse(self, h, plan, rank, stages, group):
+        import torch
+        spec_y = stages.inverse_z(h.contiguous())
+        send = torch.cat([spec_y[plan.zslab(s)].reshape(-1) for s in range(plan.world)])
+        recv = self._a2a(send, plan.recv_counts_z2y(rank), plan.send_counts_z2y(rank), group)
+        parts = torch.split(recv, [2 * k for k in plan.send_counts_z2y(rank)])
+        spec_z = torch.cat([p.view(plan.nzl[rank], plan.nyl[s], plan.hx, 2)
+                            for s, p in enumerate(parts)], dim=1).contiguous()
+        return stages.inverse_xy(spec_z)
+
+    @staticmethod
+    def stack(xs):
+        import torch
+        return torch.stack(xs).contiguous()
+
+    @staticmethod
+    def zeros_like(x):
+        import torch
+        return torch.zeros_like(x)
+
+    def oz(self, spec, chi, fk, qv):
+        qp, keep = self._q(qv)
+        nk = spec[0].numel() // 2
+        self._check(self.lib.r3d_dist_oz(self.device, spec.shape[0], nk, self._p(chi),
+                                         self._p(fk), qp, self._p(spec), self._stream()))
+        return spec
+
+    def residual(self, h, scale, g, rp, dots):
+        import torch
+        r = torch.empty_like(g)
+        self._check(self.lib.r3d_dist_residual(self.device, g.shape[0], g[0].numel(), scale,
+                                               self._p(h), self._p(g), self._p(rp[0]),
+                                               self._p(rp[1]), 1 if dots else 0, self._p(r),
+                                               self._p(self.sums), self._stream()))
+        n = g.shape[0]
+        return r, self.sums[:1 + 5 * n] if dots else self.sums[:1]
+
+    @staticmethod
+    def allreduce(sums, group):
+        import torch.distributed as dist
+        s = sums.clone()
+        if dist.is_initialized():
+            dist.all_reduce(s, group=group)
+        return s.cpu().numpy()
+
+    def mix(self, t, r, tp, rp, binary, coef, m):
+        picard = coef is None
+        s1, s2 = (0.0, 0.0) if picard else coef
+        self._check(self.lib.r3d_dist_mix(self.device, t.numel(), self._p(t), self._p(r),
+                                          self._p(tp[0]), self._p(tp[1]), self._p(rp[0]),
+                                          self._p(rp[1]), binary, 1 if picard else 0, s1, s2,
+                                          m, self._stream()))
+        return t
+
+
+R3D_DIST_SUMS_DOUBLES = 1 + 5 * 16 + 16 * 296 * 6  # include/rism3d_b200.h

@@ -58,6 +58,13 @@ extern "C" {
 #define R3D_GRID_FR 5  /* beta*phi_L(r) (one grid)                      */
 #define R3D_GRID_FK 6  /* beta*phi_L(k) on the stored half spectrum,
                           complex interleaved [z][y][p], k_x index 2p   */
+#define R3D_GRID_FKT 7 /* the same in the transform units of the
+                          iteration's passes and of r3d_slab_transform
+                          (divided by dv C(k)): what a solve split over
+                          GPUs subtracts from q_v-scaled c(k)           */
+#define R3D_GRID_CHI 8 /* chi_vv'(|k|) on the stored half spectrum,
+                          [v][v'][z][y][p] (the solvent susceptibility
+                          the OZ step of calculate_cuda.cu:39-52 uses)  */
 
 typedef struct r3d_ctx r3d_ctx;
 
@@ -277,6 +284,41 @@ int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
  * left out; stages 0-1 then 2-3 return the grid times nx ny nz / 2). */
 int r3d_slab_transform(int device, int stage, int nx, int ny, int nz, double *d_spec,
                        double *d_real, void *stream);
+
+/* One rank's pointwise steps of a solve split over GPUs (slabs.py's DistSolve
+ * runs the iteration: these, r3d_slab_transform, NCCL all-to-alls between
+ * the slab layouts and all-reduces of the sums).  They are the steps of the
+ * reference's calculate() and AN2 mixer on the rank's own pencil
+ * (calculate_cuda.cu: trm1mt, mqvfk, oz, tr; anderson_cuda.cu:1-67), whose
+ * sums cal_rms.cu:23 and anderson.cu:95 reduce over ranks.  FP64 device
+ * buffers on `device`; each call is asynchronous on `stream` (NULL: the
+ * default stream) and returns the launch status.  n <= 16 sites; qv (host,
+ * n values) the site charges.
+ *   r3d_dist_closure   z-slab: g = closure(-u + t), c = g - 1 - t + q_v fr
+ *                      (u, t, g, c [n][nloc]; fr [nloc])
+ *   r3d_dist_oz        y-slab, in place: spec_v <- sum_v' chi_vv' (spec_v' -
+ *                      q_v' fk) (spec [n][nk] complex, chi [n][n][nk], fk
+ *                      [nk] complex in transform units: R3D_GRID_FKT)
+ *   r3d_dist_residual  z-slab: R = scale h + 1 - g and its sums into d_sums
+ *                      ([0] sum R^2, [1 + 5v + k] the five AN2 theta dots of
+ *                      site v when dots != 0); d_sums holds
+ *                      R3D_DIST_SUMS_DOUBLES doubles (work space after the
+ *                      sums)
+ *   r3d_dist_mix       newdt0 (picard != 0: t += R) or newdt with the AN2
+ *                      coefficients s1, s2 and damping m; t and R go to slot
+ *                      `binary` (tp0/tp1, rp0/rp1) first */
+#define R3D_DIST_SUMS_DOUBLES (1 + 5 * 16 + 16 * 296 * 6)
+int r3d_dist_closure(int device, int n, long long nloc, int closure, int pse_n,
+                     const double *d_u, const double *d_t, const double *d_fr,
+                     const double *qv, double *d_g, double *d_c, void *stream);
+int r3d_dist_oz(int device, int n, long long nk, const double *d_chi, const double *d_fk,
+                const double *qv, double *d_spec, void *stream);
+int r3d_dist_residual(int device, int n, long long nloc, double scale, const double *d_h,
+                      const double *d_g, const double *d_rp0, const double *d_rp1, int dots,
+                      double *d_r, double *d_sums, void *stream);
+int r3d_dist_mix(int device, long long count, double *d_t, const double *d_r, double *d_tp0,
+                 double *d_tp1, double *d_rp0, double *d_rp1, int binary, int picard,
+                 double s1, double s2, double m, void *stream);
 
 /* ---- batches of independent solves --------------------------------------
  * The reference runs one solve per process (main.cu:63-65).  A batch iterates

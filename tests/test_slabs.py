@@ -218,3 +218,45 @@ def test_distributed_solve_on_two_gloo_ranks(tmp_path):
         assert r["rms"] == pytest.approx(rms, rel=1e-8)
         z0, nzl = r["z"]
         np.testing.assert_allclose(np.array(r["t"]), t[:, z0:z0 + nzl], atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
+    """The distributed solve's GPU path at one rank: its setup read from a
+    library FP64 context (u, t, phi_L(r), phi_L(k) in transform units, chi on
+    the half spectrum), its pointwise steps by the r3d_dist_* kernels and its
+    transforms by r3d_slab_transform.  It ends where that context's own FP64
+    solve ends (steps within 1, t within 1e-8) and where the numpy path on
+    the same inputs ends."""
+    import torch
+    import oracle as O
+    import rism3d as R
+    import synthetic as S
+    xvk = solvents["h2o_vv"]
+    inp = S.small(str(tmp_path), nu=8, grid=32, box=16.0, solvent=xvk, name="dgpu")
+    sol = O.Oracle(inp, xvk=xvk).solvent()  # the sites' charges and densities
+    s = R.RISM3D(precision="fp64")
+    s.initialize(inp, xvk=xvk)
+    du, t0, fr, fkt, chi = (s.get(k) for k in ("u", "t", "fr", "fkt", "chi"))
+    steps, rms, status = s.iterate()
+    t_ref = s.get("t")
+    s.close()
+    nz, ny, nx = fr.shape
+    plan = slabs.SlabPlan(nz, ny, nx, 1)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to("cuda:0")
+
+    fk2 = np.stack([fkt.real, fkt.imag], -1)
+    ds = slabs.DistSolve(plan, 0, dev(du), dev(t0), dev(fr), dev(chi), dev(fk2), sol["qv"],
+                         sol["rhov"], stages=slabs.CudaStages(R.lib, 0),
+                         ops=slabs.CudaOps(R.lib, 0))
+    dsteps, drms, dstatus = ds.iterate()
+    assert (status, dstatus) == ("converged", "converged")
+    assert abs(dsteps - steps) <= 1, (dsteps, steps)
+    t_gpu = ds.t.cpu().numpy()
+    np.testing.assert_allclose(t_gpu, t_ref, atol=1e-8)
+    dn = slabs.DistSolve(plan, 0, du, t0, fr, chi, fkt, sol["qv"], sol["rhov"])
+    nsteps, nrms, nstatus = dn.iterate()
+    assert (nsteps, nstatus) == (dsteps, dstatus)
+    np.testing.assert_allclose(dn.t, t_gpu, atol=1e-10)
