@@ -240,6 +240,7 @@ def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
     du, t0, fr, fkt, chi = (s.get(k) for k in ("u", "t", "fr", "fkt", "chi"))
     steps, rms, status = s.iterate()
     t_ref = s.get("t")
+    xmu_ref = s.thermo()[0]
     s.close()
     nz, ny, nx = fr.shape
     plan = slabs.SlabPlan(nz, ny, nx, 1)
@@ -260,3 +261,88 @@ def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
     nsteps, nrms, nstatus = dn.iterate()
     assert (nsteps, nstatus) == (dsteps, dstatus)
     np.testing.assert_allclose(dn.t, t_gpu, atol=1e-10)
+    # the results of the split solve: its final t in a library context, one
+    # evaluation for that t's residual, then the thermodynamics
+    ref_xmu = xmu_ref
+    o = R.RISM3D(precision="fp64")
+    o.initialize(inp, xvk=xvk)
+    o.set_t(t_gpu)
+    o.calculate()
+    xmu = o.thermo()[0]
+    o.close()
+    kt_per_kcal = 4184.0 / (8.314462618 * 300.0)
+    assert np.abs(np.asarray(xmu) - np.asarray(ref_xmu)).max() < 1e-6 * kt_per_kcal
+
+
+PACK_SCRIPT = r"""
+import json, sys
+import numpy as np
+import torch
+sys.path.insert(0, %(pkg)r)
+import replicas, slabs
+g = replicas.Group("gloo", timeout_s=60)
+
+
+class TorchCpuStages:  # NumpyStages on torch CPU tensors, complex as [..., 2]
+    st = slabs.NumpyStages()
+
+    @staticmethod
+    def _c(t):
+        a = t.numpy()
+        return a[..., 0] + 1j * a[..., 1]
+
+    @staticmethod
+    def _t(a):
+        return torch.from_numpy(np.stack([a.real, a.imag], -1).copy())
+
+    def forward_xy(self, real):
+        return self._t(self.st.forward_xy(real.numpy()))
+
+    def forward_z(self, spec):
+        return self._t(self.st.forward_z(self._c(spec)))
+
+    def inverse_z(self, spec):
+        return self._t(self.st.inverse_z(self._c(spec)))
+
+    def inverse_xy(self, spec):
+        return torch.from_numpy(self.st.inverse_xy(self._c(spec)).copy())
+
+
+nz, ny, nx = %(shape)r
+f = np.random.default_rng(3).standard_normal((nz, ny, nx))
+plan = slabs.SlabPlan(nz, ny, nx, g.world)
+ops = slabs.CudaOps.__new__(slabs.CudaOps)  # its packing and all-to-alls only
+st = TorchCpuStages()
+mine = ops.forward(torch.from_numpy(f[plan.zslab(g.rank)].copy()), plan, g.rank, st, None)
+back = ops.inverse(mine.clone(), plan, g.rank, st, None)
+with open(%(out)r + str(g.rank) + ".json", "w") as fo:
+    json.dump({"y": [plan.y0[g.rank], plan.nyl[g.rank]], "z": [plan.z0[g.rank], plan.nzl[g.rank]],
+               "spec": mine.numpy().tolist(), "back": back.numpy().tolist()}, fo)
+g.close()
+"""
+
+
+def test_cuda_ops_packing_on_two_gloo_ranks(tmp_path):
+    """The GPU ops' own slab packing and all-to-alls (torch tensors, the
+    layout the CUDA stages use) on two ranks, run with torch CPU tensors and
+    the numpy stages: each rank gets its y-slab of the full transform and,
+    inverted, its z-slab back (times N/2)."""
+    script = tmp_path / "pack.py"
+    out_stem = str(tmp_path / "pack")
+    script.write_text(PACK_SCRIPT % {"pkg": PKG, "shape": SHAPE, "out": out_stem})
+    code = (f"import sys; sys.path.insert(0, {PKG!r}); import replicas; "
+            f"sys.exit(replicas.launch(2, [{str(script)!r}], timeout_s=120))")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    f = _grid()
+    raw = _full_raw(f)
+    for r in range(2):
+        res = json.load(open(out_stem + f"{r}.json"))
+        y0, nyl = res["y"]
+        z0, nzl = res["z"]
+        spec = np.array(res["spec"])
+        np.testing.assert_allclose(spec[..., 0] + 1j * spec[..., 1], raw[:, y0:y0 + nyl, :],
+                                   atol=1e-9 * np.abs(raw).max())
+        np.testing.assert_allclose(np.array(res["back"]), f[z0:z0 + nzl] * f.size / 2,
+                                   atol=1e-8 * f.size)
