@@ -519,6 +519,10 @@ def run_gpu(args, group):
         if not args.no_serve:
             serve = run_served(local)
 
+    large = None
+    if rank == 0 and world == 1 and not custom and not c3 and not args.no_large:
+        large = run_large_iterations(local, prec, group)
+
     refcuda = None
     if rank == 0 and world == 1 and not custom and not args.no_reference_cuda:
         refcuda = reference_cuda(inp, xvk, maxstep=30 if c3 else None)
@@ -591,6 +595,7 @@ def run_gpu(args, group):
             "mixed_vs_fp64": mvf,
             "reference_cuda": refcuda,
             "setup": setup,
+            "large_single_solve": large,
             "batched_screen": batch,
             "served": serve,
             "xrism_solvents": xrism,
@@ -600,6 +605,40 @@ def run_gpu(args, group):
         print(json.dumps(line), flush=True)
     shutil.rmtree(tmp, ignore_errors=True)
     shutil.rmtree(_SOLVENT_DIR, ignore_errors=True)
+
+
+# ------------------------------------------- the 512^3 solve's iterations
+def run_large_iterations(local, prec, group):
+    """Device-resident iteration throughput of the large single solve (512^3,
+    12,877-atom globule, 0.2 M NaCl water, KH, history-10 Anderson 0.3), the
+    same measurement as the headline's value: graph replays of whole
+    iterations, at least MIN_TIMED_MS, tolerance disabled.  (bench.py
+    --config c3 runs that configuration end to end with the FP64 comparison.)"""
+    import rism3d as R
+    import synthetic
+    d = tempfile.mkdtemp(prefix="r3dlarge_")
+    _solvents(d)
+    inp = synthetic.config("c3", d, solvent=SOLV["nacl02"])
+    s = R.RISM3D(device=local, precision=prec)
+    s.load(inp, xvk=os.path.join(d, SOLV["nacl02"]))
+    s.set_mixer(R.MIX_ANM, 10, 0.3)
+    s.set_control(convergence=1e-300, maxstep=10 ** 9)
+    s.initialize()
+    setup = s.setup_timing()
+    s.step(3)
+    ms, timed, reps = timed_steps(group, s, 10)
+    st = s.status()
+    s.close()
+    shutil.rmtree(d, ignore_errors=True)
+    ms_iter = ms / timed
+    b = 8 if prec == "fp64" else 4
+    sec8 = sec8d_bytes(512 ** 3, 4, b, 10)["iteration"]
+    peak, kind = peak_hbm()
+    return {"workload": WORKLOAD_C3, "precision": prec, "ms_per_iter": ms_iter,
+            "steps_timed": timed, "state": st[2],
+            "iteration_bytes_sec8d": sec8, "achieved_gbs": sec8 / (ms_iter * 1e-3) / 1e9,
+            "frac_of_peak": sec8 / (ms_iter * 1e-3) / 1e9 / peak, "peak_gbs": peak,
+            "peak_kind": kind, "initialize_ms": setup["initialize_ms"]}
 
 
 # ------------------------------------------------- batched and served solves
@@ -852,6 +891,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 512^3 iteration throughput in the headline line")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip the reference's own CUDA build")
     ap.add_argument("--solvent", choices=["configuration", "shipped"], default="configuration",
