@@ -422,8 +422,11 @@ def run_gpu(args, group):
         out = one_solve(f"w{r}", prec)
         out["total"] = group.allmax(out["total"])
         warm.append(out)
-    e2e_s = sum(w["total"] for w in warm) / len(warm)
-    last = warm[-1]
+    # the median warm solve (host page faults and allocation make single
+    # solves vary by up to ~20 %); its own phases and counts are reported
+    order = sorted(range(len(warm)), key=lambda i: warm[i]["total"])
+    last = warm[order[len(order) // 2]]
+    e2e_s = last["total"]
 
     # ---- device-resident iteration throughput --------------------------
     s = R.RISM3D(device=local, precision=prec)
@@ -571,7 +574,8 @@ def run_gpu(args, group):
                     "h2d_bytes_per_step": last["h2d"] / max(last["steps"], 1),
                     "d2h_bytes_per_step": last["d2h"] / max(last["steps"], 1),
                     "solve_s": e2e_s, "solves_per_s": world / e2e_s,
-                    "solves_timed": len(warm), "cold_solve_s": cold_s,
+                    "solves_timed": len(warm), "solve_s_is": "median of the warm solves",
+                    "cold_solve_s": cold_s,
                     "warm_solves_s": [w["total"] for w in warm],
                     "phases_s": last["phases"]},
             "gpu_launches": kpi * timed,
@@ -886,7 +890,7 @@ def main():
                     help="c3: the 512^3 single solve instead of the headline workload")
     ap.add_argument("--grid", type=int, default=256, help="profiling only: grid size")
     ap.add_argument("--atoms", type=int, default=2000, help="profiling only: solute atoms")
-    ap.add_argument("--e2e-reps", type=int, default=3, help="warm end-to-end solves timed")
+    ap.add_argument("--e2e-reps", type=int, default=5, help="warm end-to-end solves timed")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
