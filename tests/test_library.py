@@ -75,3 +75,23 @@ def test_bad_inputs_are_errors_not_exits(R, tmp_path, solvents):
     with R.RISM3D(device=-1) as s:
         with pytest.raises(R.R3DError, match="EIO"):
             s.load(str(tmp_path / "missing.inp"))
+
+
+def test_split_solve_steps_reject_bad_arguments(R):
+    """The split solve's per-rank steps (r3d_dist_*) check their arguments on
+    the host, before any device work: too many sites, empty slabs, missing
+    buffers, an unknown closure and a slot other than 0 / 1 are R3D_EINVAL
+    with a message (no GPU needed)."""
+    import ctypes
+    lib = R.lib
+    qv = np.zeros(17)
+    qp = qv.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    buf = ctypes.c_void_p(16)  # never dereferenced: the checks come first
+    EINVAL = 1
+    assert lib.r3d_dist_closure(0, 17, 8, 0, 1, buf, buf, buf, qp, buf, buf, None) == EINVAL
+    assert lib.r3d_dist_closure(0, 2, 0, 0, 1, buf, buf, buf, qp, buf, buf, None) == EINVAL
+    assert lib.r3d_dist_closure(0, 2, 8, 7, 1, buf, buf, buf, qp, buf, buf, None) == EINVAL
+    assert lib.r3d_dist_oz(0, 2, 8, None, buf, qp, buf, None) == EINVAL
+    assert lib.r3d_dist_residual(0, 2, 8, 1.0, buf, buf, None, None, 1, buf, buf, None) == EINVAL
+    assert lib.r3d_dist_mix(0, 8, buf, buf, buf, buf, buf, buf, 2, 0, 0.0, 0.0, 0.5, None) == EINVAL
+    assert b"r3d_dist" in lib.r3d_last_error(None)
