@@ -175,6 +175,71 @@ __global__ void k_dist_mix(long long count, double *t, const double *r, double *
   }
 }
 
+// history-m Anderson: up to kDistHist stored residuals per call
+constexpr int kDistHist = 16;
+struct Slots {
+  const double *p[kDistHist];
+};
+
+// <r, r> and <r, f_i> per CTA of site v, one pass over r and the f_i:
+// part[((v * kDistBlocks + cta) * (kDistHist + 1)) + k]
+__global__ void __launch_bounds__(kDistThreads)
+    k_dist_anm_dots(long long nloc, const double *r, Slots f, int m, double *part) {
+  __shared__ double red[kDistThreads / 32];
+  const int v = blockIdx.y;
+  const long long off = (long long)v * nloc;
+  double a[kDistHist + 1];
+#pragma unroll
+  for (int k = 0; k <= kDistHist; ++k) a[k] = 0.0;
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nloc;
+       j += (long long)gridDim.x * blockDim.x) {
+    const double rr = r[off + j];
+    a[0] += rr * rr;
+#pragma unroll
+    for (int k = 0; k < kDistHist; ++k)
+      if (k < m) a[1 + k] += rr * f.p[k][off + j];
+  }
+  double *o = part + ((long long)v * gridDim.x + blockIdx.x) * (kDistHist + 1);
+#pragma unroll
+  for (int k = 0; k <= kDistHist; ++k) {
+    if (k <= m) {  // the same for every thread of the CTA
+      const double s = block_sum(a[k], red);
+      if (threadIdx.x == 0) o[k] = s;
+    }
+  }
+}
+
+// the partials in a fixed order, site by site with the weights 1 / rho_v
+__global__ void k_dist_anm_sums(int n, int m, Charges irho, const double *part, double *sums) {
+  __shared__ double red[kDistThreads / 32];
+  for (int k = 0; k <= m; ++k) {
+    double tot = 0.0;
+    for (int v = 0; v < n; ++v) {
+      double s = 0.0;
+      for (int i = threadIdx.x; i < kDistBlocks; i += blockDim.x)
+        s += part[((long long)v * kDistBlocks + i) * (kDistHist + 1) + k];
+      s = block_sum(s, red);
+      tot += s * irho.q[v];  // meaningful in thread 0
+    }
+    if (threadIdx.x == 0) sums[k] = tot;
+  }
+}
+
+// t_new = w0 t + sum a_i x_i + beta (w0 r + sum a_i f_i)
+__global__ void k_dist_anm_mix(long long count, const double *t, const double *r, Slots x,
+                               Slots f, Charges alpha, int m, double w0, double beta,
+                               double *tn) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    double xb = w0 * t[i], fb = w0 * r[i];
+    for (int k = 0; k < m; ++k) {
+      xb += alpha.q[k] * x.p[k][i];
+      fb += alpha.q[k] * f.p[k][i];
+    }
+    tn[i] = xb + beta * fb;
+  }
+}
+
 bool charges(int n, const double *qv, Charges &c) {
   if (n < 1 || n > kMaxSites || !qv) return false;
   for (int v = 0; v < n; ++v) c.q[v] = qv[v];
@@ -237,5 +302,50 @@ extern "C" int r3d_dist_mix(int device, long long count, double *d_t, const doub
   if (ds.err != cudaSuccess) return dist_fail(R3D_ECUDA, cudaGetErrorString(ds.err));
   k_dist_mix<<<grid_for(count), kDistThreads, 0, (cudaStream_t)stream>>>(
       count, d_t, d_r, d_tp0, d_tp1, d_rp0, d_rp1, binary, picard, s1, s2, m);
+  return launched();
+}
+
+extern "C" int r3d_dist_anm_dots(int device, int n, long long nloc, const double *d_r, int m,
+                                 const double *const *d_hist, const double *irho,
+                                 double *d_sums, void *stream) {
+  Charges w;
+  if (!charges(n, irho, w) || nloc < 1 || !d_r || !d_sums || m < 0 || m > kDistHist ||
+      (m > 0 && !d_hist))
+    return dist_fail(R3D_EINVAL, "anm_dots: bad arguments");
+  Slots f{};
+  for (int k = 0; k < m; ++k) {
+    if (!d_hist[k]) return dist_fail(R3D_EINVAL, "anm_dots: NULL history slot");
+    f.p[k] = d_hist[k];
+  }
+  DeviceScope ds(device);
+  if (ds.err != cudaSuccess) return dist_fail(R3D_ECUDA, cudaGetErrorString(ds.err));
+  cudaStream_t s = (cudaStream_t)stream;
+  double *part = d_sums + 1 + kDistHist;
+  k_dist_anm_dots<<<dim3(kDistBlocks, n), kDistThreads, 0, s>>>(nloc, d_r, f, m, part);
+  k_dist_anm_sums<<<1, kDistThreads, 0, s>>>(n, m, w, part, d_sums);
+  return launched();
+}
+
+extern "C" int r3d_dist_anm_mix(int device, long long count, const double *d_t,
+                                const double *d_r, int m, const double *const *d_x,
+                                const double *const *d_f, const double *alpha, double beta,
+                                double *d_tn, void *stream) {
+  Charges a{};
+  if (count < 1 || !d_t || !d_r || !d_tn || m < 0 || m > kDistHist ||
+      (m > 0 && (!d_x || !d_f || !alpha)))
+    return dist_fail(R3D_EINVAL, "anm_mix: bad arguments");
+  Slots x{}, f{};
+  double w0 = 1.0;
+  for (int k = 0; k < m; ++k) {
+    if (!d_x[k] || !d_f[k]) return dist_fail(R3D_EINVAL, "anm_mix: NULL history slot");
+    x.p[k] = d_x[k];
+    f.p[k] = d_f[k];
+    a.q[k] = alpha[k];
+    w0 -= alpha[k];
+  }
+  DeviceScope ds(device);
+  if (ds.err != cudaSuccess) return dist_fail(R3D_ECUDA, cudaGetErrorString(ds.err));
+  k_dist_anm_mix<<<grid_for(count), kDistThreads, 0, (cudaStream_t)stream>>>(
+      count, d_t, d_r, x, f, a, m, w0, beta, d_tn);
   return launched();
 }

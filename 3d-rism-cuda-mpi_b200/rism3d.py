@@ -35,7 +35,8 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_refresh_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
            "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_dist_closure", "r3d_dist_oz",
-           "r3d_dist_residual", "r3d_dist_mix", "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
+           "r3d_dist_residual", "r3d_dist_mix", "r3d_dist_anm_dots", "r3d_dist_anm_mix",
+           "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
            "r3d_server_poll", "r3d_server_wait", "r3d_server_write_xmu", "r3d_server_release",
            "r3d_server_destroy", "r3d_write_guv", "r3d_write_huv", "r3d_write_cuv",
@@ -127,6 +128,9 @@ def _load():
         "r3d_dist_oz": [ci, ci, ctypes.c_longlong, vp, vp, dp, vp, vp],
         "r3d_dist_residual": [ci, ci, ctypes.c_longlong, cd, vp, vp, vp, vp, ci, vp, vp, vp],
         "r3d_dist_mix": [ci, ctypes.c_longlong, vp, vp, vp, vp, vp, vp, ci, ci, cd, cd, cd, vp],
+        "r3d_dist_anm_dots": [ci, ci, ctypes.c_longlong, vp, ci, ctypes.POINTER(vp), dp, vp, vp],
+        "r3d_dist_anm_mix": [ci, ctypes.c_longlong, vp, vp, ci, ctypes.POINTER(vp),
+                             ctypes.POINTER(vp), dp, cd, vp, vp],
         "r3d_batch_create": [ci, ctypes.POINTER(vp)],
         "r3d_batch_add": [vp, vp],
         "r3d_batch_iterate": [vp, ip, dp],

@@ -313,6 +313,30 @@ class NumpyOps:
         return r, sums
 
     @staticmethod
+    def anm_dots(r, hist, irho):
+        """<r, r> and <r, f_i> for the stored residuals f_i, each summed over
+        this rank's points of every site with the weight 1 / rho_v."""
+        out = []
+        for f in [r] + list(hist):
+            out.append(float(sum(np.sum(r[v] * f[v]) * irho[v] for v in range(r.shape[0]))))
+        return out
+
+    @staticmethod
+    def anm_mix(t, r, hx, hf, alpha, beta):
+        """t_{k+1} = w0 t + sum a_i x_i + beta (w0 f + sum a_i f_i), w0 = 1 -
+        sum a_i, over the stored pairs (x_i, f_i)."""
+        w0 = 1.0 - float(np.sum(alpha))
+        xb, fb = w0 * t, w0 * r
+        for a, x, f in zip(alpha, hx, hf):
+            xb = xb + a * x
+            fb = fb + a * f
+        return xb + beta * fb
+
+    @staticmethod
+    def copy(x):
+        return x.copy()
+
+    @staticmethod
     def mix(t, r, tp, rp, binary, coef, m):
         """newdt0 (coef None: t += R) or newdt (anderson_cuda.cu:1-22); the
         current t and R go to slot `binary`."""
@@ -326,6 +350,32 @@ class NumpyOps:
         tp[binary] = t.copy()
         rp[binary] = r.copy()
         return u + m * (w - u)
+
+
+def solve_pp(A, b):
+    """Dense solve with partial pivoting (the history-m Anderson solve);
+    None when singular or not finite."""
+    A = [list(row) for row in A]
+    b = list(b)
+    m = len(b)
+    for k in range(m):
+        piv = max(range(k, m), key=lambda i: abs(A[i][k]))
+        if not abs(A[piv][k]) > 1e-300:
+            return None
+        if piv != k:
+            A[k], A[piv] = A[piv], A[k]
+            b[k], b[piv] = b[piv], b[k]
+        for i in range(k + 1, m):
+            f = A[i][k] / A[k][k]
+            for j in range(k, m):
+                A[i][j] -= f * A[k][j]
+            b[i] -= f * b[k]
+    for k in range(m - 1, -1, -1):
+        acc = b[k]
+        for j in range(k + 1, m):
+            acc -= A[k][j] * b[j]
+        b[k] = acc / A[k][k]
+    return b if all(np.isfinite(b)) else None
 
 
 def leg2(a, c):
@@ -356,7 +406,7 @@ class DistSolve:
 
     def __init__(self, plan, rank, du, t, fr, chi, fk, qv, rhov, closure=(KH, 1),
                  mixer=(2, 0.6, 0.2), tol=1e-6, maxstep=10000, stages=None, ops=None,
-                 group=None):
+                 group=None, anderson=None):
         self.plan, self.rank, self.group = plan, rank, group
         self.du, self.t, self.fr, self.chi, self.fk = du, t, fr, chi, fk
         self.qv = np.asarray(qv, dtype=np.float64)
@@ -372,6 +422,15 @@ class DistSolve:
         self.rp = [self.ops.zeros_like(t), self.ops.zeros_like(t)]
         self.r = None
         self.g = None
+        # history-m Anderson (history H, damping) instead of AN2 when given:
+        # the stored pairs (x_i, f_i) and the Gram matrix of the f_i (their
+        # weighted dots, summed over ranks), kept as pairs enter the ring
+        self.anderson = anderson
+        if anderson:
+            H = max(1, int(anderson[0]))
+            self.hx = [self.ops.zeros_like(t) for _ in range(H)]
+            self.hf = [self.ops.zeros_like(t) for _ in range(H)]
+            self.gram = np.zeros((H, H))
 
     def calculate(self, dots):
         """One evaluation; returns the RMS over the whole grid and the AN2
@@ -389,9 +448,49 @@ class DistSolve:
         rms = float(np.sqrt(tot[0] / (self.N * n)))
         return rms, tot[1:]
 
+    def _anderson_step(self, hhead, hcount):
+        """One history-m Anderson update: alpha minimises ||f_k + sum
+        alpha_i (f_i - f_k)|| (weights 1 / rho_v) over the stored pairs, t_{k+1}
+        = t_k + sum alpha_i (x_i - t_k) + beta (f_k + sum alpha_i (f_i - f_k));
+        then (t_k, f_k) replaces the oldest pair."""
+        H, beta = len(self.hx), float(self.anderson[1])
+        slots = [(hhead - 1 - i) % H for i in range(hcount)]
+        d = self.ops.allreduce(self.ops.anm_dots(self.r, [self.hf[q] for q in slots], self.irho),
+                               self.group)
+        d0, di = d[0], d[1:]
+        if hcount > 0:
+            A = [[d0 - di[i] - di[j] + self.gram[slots[i], slots[j]] for j in range(hcount)]
+                 for i in range(hcount)]
+            alpha = solve_pp(A, [d0 - di[i] for i in range(hcount)]) or [0.0] * hcount
+            tn = self.ops.anm_mix(self.t, self.r, [self.hx[q] for q in slots],
+                                  [self.hf[q] for q in slots], alpha, beta)
+        else:
+            tn = self.ops.anm_mix(self.t, self.r, [], [], [], beta)
+        self.hx[hhead] = self.ops.copy(self.t)
+        self.hf[hhead] = self.ops.copy(self.r)
+        for i, q in enumerate(slots):
+            if q != hhead:
+                self.gram[hhead, q] = self.gram[q, hhead] = di[i]
+        self.gram[hhead, hhead] = d0
+        self.t = tn
+
     def iterate(self):
         """RISM3D::iterate (iterate.cu:48-82) with AN2::initialize at its
         start: (steps, rms, 'converged' | 'maxstep' | 'diverged')."""
+        if self.anderson:
+            H = len(self.hx)
+            hhead = hcount = 0
+            rms, step = 0.0, 0
+            for step in range(1, self.maxstep + 1):
+                rms, _ = self.calculate(dots=False)
+                if not np.isfinite(rms):
+                    return step, rms, "diverged"
+                if rms <= self.tol:
+                    return step, rms, "converged"
+                self._anderson_step(hhead, hcount)
+                hhead = (hhead + 1) % H
+                hcount = min(hcount + 1, H)
+            return step, rms, "maxstep"
         binary, count_left = 0, self.count
         rms, step = 0.0, 0
         for step in range(1, self.maxstep + 1):
@@ -431,8 +530,8 @@ class CudaOps:
     def __init__(self, lib, device=0):
         import torch
         self.lib, self.device = lib, device
-        self.sums = torch.zeros(R3D_DIST_SUMS_DOUBLES, dtype=torch.float64,
-                                device=f"cuda:{device}")
+        self.sums = torch.zeros(max(R3D_DIST_SUMS_DOUBLES, R3D_DIST_ANM_SUMS_DOUBLES),
+                                dtype=torch.float64, device=f"cuda:{device}")
 
     def _stream(self):
         import torch
@@ -526,6 +625,44 @@ class CudaOps:
             dist.all_reduce(s, group=group)
         return s.cpu().numpy()
 
+    @staticmethod
+    def _ptrs(ts):
+        arr = (ctypes.c_void_p * max(1, len(ts)))(*[t.data_ptr() for t in ts])
+        return arr
+
+    def anm_dots(self, r, hist, irho):
+        """The weighted dots of the history-m mixer on the device (up to 16
+        stored residuals per call); returns a device tensor of 1 + m sums."""
+        out, m = [], len(hist)
+        w = np.ascontiguousarray(irho, dtype=np.float64)
+        wp = w.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        for k0 in range(0, max(m, 1), 16):
+            part = hist[k0:k0 + 16]
+            self._check(self.lib.r3d_dist_anm_dots(self.device, r.shape[0], r[0].numel(),
+                                                   self._p(r), len(part), self._ptrs(part), wp,
+                                                   self._p(self.sums), self._stream()))
+            s = self.sums[:1 + len(part)].clone()
+            out.append(s if k0 == 0 else s[1:])
+        import torch
+        return torch.cat(out)
+
+    def anm_mix(self, t, r, hx, hf, alpha, beta):
+        import torch
+        tn = torch.empty_like(t)
+        m = len(alpha)
+        if m > 16:
+            raise ValueError("history-m Anderson of the split solve: at most 16 stored pairs")
+        a = np.ascontiguousarray(alpha if m else [0.0], dtype=np.float64)
+        self._check(self.lib.r3d_dist_anm_mix(self.device, t.numel(), self._p(t), self._p(r), m,
+                                              self._ptrs(hx), self._ptrs(hf),
+                                              a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                              beta, self._p(tn), self._stream()))
+        return tn
+
+    @staticmethod
+    def copy(x):
+        return x.clone()
+
     def mix(self, t, r, tp, rp, binary, coef, m):
         picard = coef is None
         s1, s2 = (0.0, 0.0) if picard else coef
@@ -537,3 +674,4 @@ class CudaOps:
 
 
 R3D_DIST_SUMS_DOUBLES = 1 + 5 * 16 + 16 * 296 * 6  # include/rism3d_b200.h
+R3D_DIST_ANM_SUMS_DOUBLES = 1 + 16 + 16 * 296 * 17

@@ -319,6 +319,23 @@ int r3d_dist_residual(int device, int n, long long nloc, double scale, const dou
 int r3d_dist_mix(int device, long long count, double *d_t, const double *d_r, double *d_tp0,
                  double *d_tp1, double *d_rp0, double *d_rp1, int binary, int picard,
                  double s1, double s2, double m, void *stream);
+/* The history-m Anderson mixer of the split solve (the library's own
+ * extension of AN2; no counterpart in the reference):
+ *   r3d_dist_anm_dots  d_sums[0] = <R, R>, d_sums[1 + i] = <R, f_i> for the m
+ *                      stored residuals d_hist[i] (host array of device
+ *                      pointers, m <= 16), each summed over the rank's points
+ *                      of every site with the weights irho[v] = 1 / rho_v
+ *                      (host); d_sums holds R3D_DIST_ANM_SUMS_DOUBLES doubles
+ *   r3d_dist_anm_mix   d_tn = w0 t + sum alpha_i x_i + beta (w0 R + sum
+ *                      alpha_i f_i), w0 = 1 - sum alpha_i (alpha: host, m
+ *                      values; d_x / d_f: host arrays of device pointers) */
+#define R3D_DIST_ANM_SUMS_DOUBLES (1 + 16 + 16 * 296 * 17)
+int r3d_dist_anm_dots(int device, int n, long long nloc, const double *d_r, int m,
+                      const double *const *d_hist, const double *irho, double *d_sums,
+                      void *stream);
+int r3d_dist_anm_mix(int device, long long count, const double *d_t, const double *d_r, int m,
+                     const double *const *d_x, const double *const *d_f, const double *alpha,
+                     double beta, double *d_tn, void *stream);
 
 /* ---- batches of independent solves --------------------------------------
  * The reference runs one solve per process (main.cu:63-65).  A batch iterates

@@ -165,7 +165,10 @@ sys.path.insert(0, %(oracle)r)
 import replicas, slabs
 import oracle as O
 g = replicas.Group("gloo", timeout_s=120)
+anderson = %(anderson)r
 o = O.Oracle(%(inp)r, xvk=%(xvk)r)
+if anderson:
+    o.set_mixer(1, *anderson)
 o.initialize()
 (nx, ny, nz), box, _ = o.grid()
 plan = slabs.SlabPlan(nz, ny, nx, g.world)
@@ -179,7 +182,7 @@ fk_s = (1j * sigma * fk[:, :, 0::2] / dv)[:, plan.yslab(g.rank)]
 chi_s = chi[:, :, :, :, 0::2][:, :, :, plan.yslab(g.rank)]
 zs = plan.zslab(g.rank)
 ds = slabs.DistSolve(plan, g.rank, du[:, zs].copy(), t0[:, zs].copy(), fr[zs].copy(),
-                     chi_s.copy(), fk_s.copy(), sol["qv"], sol["rhov"])
+                     chi_s.copy(), fk_s.copy(), sol["qv"], sol["rhov"], anderson=anderson)
 steps, rms, status = ds.iterate()
 with open(%(out)r + str(g.rank) + ".json", "w") as fo:
     json.dump({"steps": steps, "rms": rms, "status": status, "z": [plan.z0[g.rank], plan.nzl[g.rank]],
@@ -188,12 +191,13 @@ g.close()
 """
 
 
-def test_distributed_solve_on_two_gloo_ranks(tmp_path):
+@pytest.mark.parametrize("anderson", [None, (10, 0.3)])
+def test_distributed_solve_on_two_gloo_ranks(tmp_path, anderson):
     """One solve split over two ranks (z-slabs for the real-space arrays,
     y-slabs for the k-space ones; the reference's RISM3D::iterate over MPI
-    ranks, with the RMS and AN2 dots summed over ranks) takes the oracle's
-    iterations to the oracle's t: same step count and RMS, t within
-    1e-9."""
+    ranks, with the RMS and the mixer's dots summed over ranks) takes the
+    oracle's iterations to the oracle's t: same step count and RMS, t within
+    1e-9; with AN2 and with history-10 Anderson."""
     import oracle as O
     import synthetic as S
     from conftest import unpack
@@ -202,7 +206,8 @@ def test_distributed_solve_on_two_gloo_ranks(tmp_path):
     script = tmp_path / "solve.py"
     out_stem = str(tmp_path / "solve")
     script.write_text(SOLVE_SCRIPT % {"pkg": PKG, "oracle": os.path.join(ROOT, "oracle"),
-                                      "inp": inp, "xvk": xvk, "out": out_stem})
+                                      "inp": inp, "xvk": xvk, "out": out_stem,
+                                      "anderson": anderson})
     code = (f"import sys; sys.path.insert(0, {PKG!r}); import replicas; "
             f"sys.exit(replicas.launch(2, [{str(script)!r}], timeout_s=300))")
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
@@ -210,6 +215,8 @@ def test_distributed_solve_on_two_gloo_ranks(tmp_path):
     assert out.returncode == 0, out.stderr[-3000:]
     res = [json.load(open(out_stem + f"{r}.json")) for r in range(2)]
     o = O.Oracle(inp, xvk=xvk)
+    if anderson:
+        o.set_mixer(1, *anderson)
     o.initialize()
     steps, rms, status = o.iterate()
     t = o.get("t")
@@ -221,7 +228,8 @@ def test_distributed_solve_on_two_gloo_ranks(tmp_path):
 
 
 @pytest.mark.gpu
-def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
+@pytest.mark.parametrize("anderson", [None, (10, 0.3)])
+def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents, anderson):
     """The distributed solve's GPU path at one rank: its setup read from a
     library FP64 context (u, t, phi_L(r), phi_L(k) in transform units, chi on
     the half spectrum), its pointwise steps by the r3d_dist_* kernels and its
@@ -236,7 +244,10 @@ def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
     inp = S.small(str(tmp_path), nu=8, grid=32, box=16.0, solvent=xvk, name="dgpu")
     sol = O.Oracle(inp, xvk=xvk).solvent()  # the sites' charges and densities
     s = R.RISM3D(precision="fp64")
-    s.initialize(inp, xvk=xvk)
+    s.load(inp, xvk=xvk)
+    if anderson:
+        s.set_mixer(R.MIX_ANM, *anderson)
+    s.initialize()
     du, t0, fr, fkt, chi = (s.get(k) for k in ("u", "t", "fr", "fkt", "chi"))
     steps, rms, status = s.iterate()
     t_ref = s.get("t")
@@ -251,13 +262,14 @@ def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
     fk2 = np.stack([fkt.real, fkt.imag], -1)
     ds = slabs.DistSolve(plan, 0, dev(du), dev(t0), dev(fr), dev(chi), dev(fk2), sol["qv"],
                          sol["rhov"], stages=slabs.CudaStages(R.lib, 0),
-                         ops=slabs.CudaOps(R.lib, 0))
+                         ops=slabs.CudaOps(R.lib, 0), anderson=anderson)
     dsteps, drms, dstatus = ds.iterate()
     assert (status, dstatus) == ("converged", "converged")
     assert abs(dsteps - steps) <= 1, (dsteps, steps)
     t_gpu = ds.t.cpu().numpy()
     np.testing.assert_allclose(t_gpu, t_ref, atol=1e-8)
-    dn = slabs.DistSolve(plan, 0, du, t0, fr, chi, fkt, sol["qv"], sol["rhov"])
+    dn = slabs.DistSolve(plan, 0, du, t0, fr, chi, fkt, sol["qv"], sol["rhov"],
+                         anderson=anderson)
     nsteps, nrms, nstatus = dn.iterate()
     assert (nsteps, nstatus) == (dsteps, dstatus)
     np.testing.assert_allclose(dn.t, t_gpu, atol=1e-10)
@@ -265,7 +277,10 @@ def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents):
     # evaluation for that t's residual, then the thermodynamics
     ref_xmu = xmu_ref
     o = R.RISM3D(precision="fp64")
-    o.initialize(inp, xvk=xvk)
+    o.load(inp, xvk=xvk)
+    if anderson:
+        o.set_mixer(R.MIX_ANM, *anderson)
+    o.initialize()
     o.set_t(t_gpu)
     o.calculate()
     xmu = o.thermo()[0]
