@@ -1,6 +1,6 @@
 """Parity of the CUDA solver with the CPU oracle on the two features the
-reference does not have: the history-m Anderson mixer (BASELINE's C1/C3 use
-history 10) and the PSE-n closure.  Fixtures come from the oracle
+reference does not have: the history-m Anderson mixer (the 64^3 water and
+512^3 configurations use history 10) and the PSE-n closure.  Fixtures come from the oracle
 (tests/golden/make_oracle_fixtures.py).  FP64: same step count within 2,
 .xmu values within 1e-6 kcal/mol, g within 1e-8 relative; mixed: SFE within
 0.01 kcal/mol and PMV within 0.1 A^3."""
