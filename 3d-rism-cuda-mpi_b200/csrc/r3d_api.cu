@@ -2539,6 +2539,16 @@ extern "C" int r3d_info(const r3d_ctx *c, int *grid3, int *natv, long long *ngri
   return R3D_OK;
 }
 
+extern "C" int r3d_solvent_sites(const r3d_ctx *c, double *qv, double *rhov) {
+  if (!c || !qv || !rhov) return fail(nullptr, R3D_EINVAL, "bad arguments");
+  if (!c->prob.has_solvent) return fail(nullptr, R3D_ESTATE, "no solvent loaded");
+  for (int v = 0; v < c->prob.natv; ++v) {
+    qv[v] = c->prob.qv[v];
+    rhov[v] = c->prob.rhov[v];
+  }
+  return R3D_OK;
+}
+
 extern "C" int r3d_device_bytes(const r3d_ctx *c, unsigned long long *bytes) {
   if (!c || !bytes) return R3D_EINVAL;
   if (c->initialized) {

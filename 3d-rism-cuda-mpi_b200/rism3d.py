@@ -32,7 +32,7 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_load_xvk", "r3d_set_problem", "r3d_set_closure", "r3d_set_mixer",
            "r3d_set_control", "r3d_initialize", "r3d_calculate", "r3d_anderson",
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
-           "r3d_info", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_refresh_timing", "r3d_step",
+           "r3d_info", "r3d_solvent_sites", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_refresh_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
            "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_dist_closure", "r3d_dist_oz",
            "r3d_dist_residual", "r3d_dist_mix", "r3d_dist_anm_dots", "r3d_dist_anm_mix",
@@ -112,6 +112,7 @@ def _load():
         "r3d_get_grid": [vp, ci, dp],
         "r3d_set_t": [vp, dp],
         "r3d_info": [vp, ip, ip, ctypes.POINTER(ctypes.c_longlong), ip],
+        "r3d_solvent_sites": [vp, dp, dp],
         "r3d_device_bytes": [vp, ctypes.POINTER(ctypes.c_ulonglong)],
         "r3d_iter_timing": [vp, dp, ip],
         "r3d_setup_timing": [vp, dp],
@@ -286,6 +287,13 @@ class RISM3D:
         N = ctypes.c_longlong()
         self._check(lib.r3d_info(self.h, g, ctypes.byref(n), ctypes.byref(N), ctypes.byref(nu)))
         return dict(grid=tuple(g), natv=n.value, ngrid=N.value, nu=nu.value)
+
+    def solvent_sites(self):
+        """(q_v, rho_v) of the solvent's site classes (after load)."""
+        n = self.info()["natv"]
+        qv, rhov = np.zeros(n), np.zeros(n)
+        self._check(lib.r3d_solvent_sites(self.h, _dp(qv), _dp(rhov)))
+        return qv, rhov
 
     def device_bytes(self):
         b = ctypes.c_ulonglong()

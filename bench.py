@@ -853,6 +853,69 @@ def run_served(local, rates=(10.0, 30.0, 100.0), count=48):
                              "p50": err[len(err) // 2] if err else None, "n": len(err)}}
 
 
+# ---------------------------------------- one solve split over the ranks
+def run_split(args, group):
+    """The 256^3 deck (FP64, KH, AN2) as one solve split over the ranks
+    (slabs.DistSolve: z-slabs / y-slabs, NCCL all-to-alls, the r3d_dist_*
+    steps and r3d_slab_transform per rank): CUDA-event time of K evaluation
+    + mix steps, max over ranks.  Every rank reads its setup from a library
+    context of the whole deck (untimed)."""
+    import numpy as np
+    import torch
+    import rism3d as R
+    import slabs
+    rank, world, local = group.rank, group.world, group.local
+    prepare_solvents(args.solvent, device=local)
+    tmp = tempfile.mkdtemp(prefix=f"r3dsplit{rank}_")
+    inp, xvk = make_deck(tmp)
+    s = R.RISM3D(device=local, precision="fp64")
+    s.load(inp, xvk=xvk)
+    s.initialize()
+    du, t0, fr, fkt, chi = (s.get(k) for k in ("u", "t", "fr", "fkt", "chi"))
+    qv, rhov = s.solvent_sites()
+    s.close()
+    nz, ny, nx = fr.shape
+    plan = slabs.SlabPlan(nz, ny, nx, world)
+    zs, ys = plan.zslab(rank), plan.yslab(rank)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(f"cuda:{local}")
+
+    arrays = (dev(du[:, zs]), dev(t0[:, zs]), dev(fr[zs]), dev(chi[:, :, :, ys]),
+              dev(np.stack([fkt.real, fkt.imag], -1)[:, ys]))
+    del du, t0, fr, fkt, chi
+
+    def run(k):  # k evaluations (tolerance 0: none stops early)
+        ds = slabs.DistSolve(plan, rank, *[a.clone() for a in arrays], qv, rhov,
+                             closure=(slabs.KH, 1), mixer=(2, 0.6, 0.2), tol=0.0, maxstep=k,
+                             stages=slabs.CudaStages(R.lib, local), ops=slabs.CudaOps(R.lib, local),
+                             group=None)
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        steps, rms, status = ds.iterate()
+        e1.record()
+        torch.cuda.synchronize(local)
+        return e0.elapsed_time(e1), steps
+
+    run(max(3, args.warmup))
+    group.barrier()
+    ms, steps = run(args.steps)
+    ms = group.allmax(ms)
+    shutil.rmtree(tmp, ignore_errors=True)
+    if rank == 0:
+        n = len(qv)
+        a2a = 2 * n * (nx // 2) * ny * nz * 16 * (world - 1) / world / world
+        print(json.dumps({
+            "impl": "b200-split", "metric": "iterations/s of one FP64 solve split over the GPUs",
+            "value": steps / (ms * 1e-3), "unit": "iter/s", "n_gpus": world, "steps": steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "strong", "dtype": "f64", "data": "synthetic (seeded 2000-atom globule)",
+            "config": {"workload": WORKLOAD + " (FP64, AN2), one solve split over the ranks",
+                       "grid": nx, "sites": n, "slabs": world},
+            "nvlink_bytes_per_rank_per_step": a2a}), flush=True)
+
+
 # ------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
     if rank != 0:
@@ -895,6 +958,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched screen")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison")
+    ap.add_argument("--split", action="store_true",
+                    help="time the 256^3 FP64 solve split over the ranks instead (slabs.DistSolve)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 512^3 iteration throughput in the headline line")
     ap.add_argument("--no-reference-cuda", action="store_true",
@@ -923,7 +988,10 @@ def main():
         return 0
     group = replicas.Group("nccl" if world > 1 else "none")
     try:
-        run_gpu(args, group)
+        if args.split:
+            run_split(args, group)
+        else:
+            run_gpu(args, group)
     finally:
         group.close()
     return 0

@@ -154,6 +154,11 @@ int r3d_set_t(r3d_ctx *ctx, const double *host);
 /* Problem facts. */
 int r3d_info(const r3d_ctx *ctx, int *grid3, int *natv, long long *ngrid,
              int *nu);
+/* Charges (e) and number densities (molecules/A^3) of the solvent's site
+ * classes, natv values each, in the order of the grids' sites: the q_v and
+ * rho_v of Solvent::read (solvent_read.cc:30-85) after r3d_load_xvk.  What a
+ * solve split over GPUs (slabs.py's DistSolve) takes besides the grids. */
+int r3d_solvent_sites(const r3d_ctx *ctx, double *qv, double *rhov);
 /* Device bytes the context holds (after initialize) or will need (before). */
 int r3d_device_bytes(const r3d_ctx *ctx, unsigned long long *bytes);
 /* CUDA-event time of the last r3d_iterate loop, ms per iteration, and the

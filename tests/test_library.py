@@ -95,3 +95,21 @@ def test_split_solve_steps_reject_bad_arguments(R):
     assert lib.r3d_dist_residual(0, 2, 8, 1.0, buf, buf, None, None, 1, buf, buf, None) == EINVAL
     assert lib.r3d_dist_mix(0, 8, buf, buf, buf, buf, buf, buf, 2, 0, 0.0, 0.0, 0.5, None) == EINVAL
     assert b"r3d_dist" in lib.r3d_last_error(None)
+
+
+def test_solvent_sites_match_the_oracle(R, refcase):
+    """r3d_solvent_sites: the site classes' charges and densities the library
+    read from the .xvk (what a split solve takes besides the grids) equal the
+    oracle's reading of the same table; before a solvent is loaded it is
+    R3D_ESTATE."""
+    import oracle as O
+    inp, xvk = refcase("s64nacl")
+    with R.RISM3D(device=-1) as s:
+        with pytest.raises(R.R3DError, match="ESTATE"):
+            s.solvent_sites()
+        s.load(inp, xvk=xvk)
+        qv, rhov = s.solvent_sites()
+    sol = O.Oracle(inp, xvk=xvk).solvent()
+    np.testing.assert_allclose(qv, sol["qv"], rtol=1e-15)
+    np.testing.assert_allclose(rhov, sol["rhov"], rtol=1e-15)
+    assert len(qv) == 4

@@ -245,6 +245,12 @@ def test_gpu_distributed_solve_on_one_rank(tmp_path, solvents, anderson):
     sol = O.Oracle(inp, xvk=xvk).solvent()  # the sites' charges and densities
     s = R.RISM3D(precision="fp64")
     s.load(inp, xvk=xvk)
+    qv, rhov = s.solvent_sites()  # the library reads the same values
+    np.testing.assert_allclose(qv, sol["qv"], rtol=1e-15)
+    np.testing.assert_allclose(rhov, sol["rhov"], rtol=1e-15)
+    s.close()
+    s = R.RISM3D(precision="fp64")
+    s.load(inp, xvk=xvk)
     if anderson:
         s.set_mixer(R.MIX_ANM, *anderson)
     s.initialize()
