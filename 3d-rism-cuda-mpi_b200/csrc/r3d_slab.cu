@@ -62,9 +62,10 @@ int slab_fail(int code, const std::string &m) {
 }
 }  // namespace
 
-extern "C" int r3d_slab_transform(int device, int stage, int nx, int ny, int nz, double *d_spec,
-                                  double *d_real, void *stream) {
-  if (stage < 0 || stage > 3 || !d_spec || ((stage == 0 || stage == 3) && !d_real))
+extern "C" int r3d_slab_transform_sites(int device, int stage, int nsites, int nx, int ny,
+                                        int nz, double *d_spec, double *d_real, void *stream) {
+  if (stage < 0 || stage > 3 || !d_spec || ((stage == 0 || stage == 3) && !d_real) ||
+      nsites < 1 || nsites > kMaxSites)
     return slab_fail(R3D_EINVAL, "bad arguments");
   if (nx < 4 || (nx & 1) || ny < 1 || nz < 1 || device < 0 || device >= 64)
     return slab_fail(R3D_EINVAL, "nx must be even and >= 4, ny and nz >= 1");
@@ -73,7 +74,7 @@ extern "C" int r3d_slab_transform(int device, int stage, int nx, int ny, int nz,
   d.nx = nx;
   d.ny = ny;
   d.nz = nz;
-  d.n = 1;
+  d.n = nsites;  // sites one after another: [site][slab]
   d.hx = hx;
   d.N = d.Ns = (long long)nx * ny * nz;
   d.Nh = d.Nhs = (long long)hx * ny * nz;
@@ -83,20 +84,23 @@ extern "C" int r3d_slab_transform(int device, int stage, int nx, int ny, int nz,
   if (d.nrad_x < 0 || d.nrad_y < 0 || d.nrad_z < 0)
     return slab_fail(R3D_EINVAL, "grid sizes must factor into primes <= 13");
   const size_t cs = sizeof(double2), budget = 100 * 1024;
+  // an x tile and a z tile hold every site (their shared memory grows with
+  // nsites); a y tile holds one site
   int S = 16;
-  while (S > 1 && ((ny * nz) % S || smem_x(hx, 1, S, cs) > budget)) S >>= 1;
+  while (S > 1 && ((ny * nz) % S || smem_x(hx, nsites, S, cs) > budget)) S >>= 1;
   int Py = 8;
   while (Py > 1 && (hx % Py || smem_y(ny, Py, cs) > budget)) Py >>= 1;
   int Pz = 4;
-  while (Pz > 1 && (hx % Pz || smem_z(nz, 1, Pz, cs) > budget)) Pz >>= 1;
-  const size_t smx = smem_x(hx, 1, S, cs), smy = smem_y(ny, Py, cs), smz = smem_z(nz, 1, Pz, cs);
+  while (Pz > 1 && (hx % Pz || smem_z(nz, nsites, Pz, cs) > budget)) Pz >>= 1;
+  const size_t smx = smem_x(hx, nsites, S, cs), smy = smem_y(ny, Py, cs),
+               smz = smem_z(nz, nsites, Pz, cs);
   if (smx > 220 * 1024 || smy > 220 * 1024 || smz > 220 * 1024)
     return slab_fail(R3D_EINVAL, "slab too large for one CTA's shared memory");
   d.rows = S;
   d.ycols = Py;
   d.zcols = Pz;
   d.tiles_x = (ny * nz) / S;
-  d.tiles_y = nz * (hx / Py);
+  d.tiles_y = nsites * nz * (hx / Py);
   d.tiles_z = ny * (hx / Pz);
   d.w = d_spec;
 
@@ -153,4 +157,9 @@ extern "C" int r3d_slab_transform(int device, int stage, int nx, int ny, int nz,
   if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess)
     return slab_fail(R3D_ECUDA, cudaGetErrorString(e));
   return R3D_OK;
+}
+
+extern "C" int r3d_slab_transform(int device, int stage, int nx, int ny, int nz, double *d_spec,
+                                  double *d_real, void *stream) {
+  return r3d_slab_transform_sites(device, stage, 1, nx, ny, nz, d_spec, d_real, stream);
 }

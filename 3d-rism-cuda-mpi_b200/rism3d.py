@@ -34,7 +34,7 @@ EXPORTS = ["r3d_create", "r3d_destroy", "r3d_last_error", "r3d_set_ad", "r3d_loa
            "r3d_iterate", "r3d_thermo", "r3d_write_xmu", "r3d_get_grid", "r3d_set_t",
            "r3d_info", "r3d_solvent_sites", "r3d_device_bytes", "r3d_iter_timing", "r3d_setup_timing", "r3d_refresh_timing", "r3d_step",
            "r3d_profile_kernels", "r3d_status", "r3d_transfer_bytes", "r3d_fft3d",
-           "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_dist_closure", "r3d_dist_oz",
+           "r3d_fft3d_noalloc", "r3d_slab_transform", "r3d_slab_transform_sites", "r3d_dist_closure", "r3d_dist_oz",
            "r3d_dist_residual", "r3d_dist_mix", "r3d_dist_anm_dots", "r3d_dist_anm_mix",
            "r3d_batch_create", "r3d_batch_add", "r3d_batch_iterate",
            "r3d_batch_info", "r3d_batch_destroy", "r3d_server_create", "r3d_server_submit",
@@ -125,6 +125,7 @@ def _load():
         "r3d_fft3d": [ci, ci, ci, ci, ci, dp, ci, dp, dp],
         "r3d_fft3d_noalloc": [ci, ci, ci, ci, dp, ci, vp, vp, vp],
         "r3d_slab_transform": [ci, ci, ci, ci, ci, vp, vp, vp],
+        "r3d_slab_transform_sites": [ci, ci, ci, ci, ci, ci, vp, vp, vp],
         "r3d_dist_closure": [ci, ci, ctypes.c_longlong, ci, ci, vp, vp, vp, dp, vp, vp, vp],
         "r3d_dist_oz": [ci, ci, ctypes.c_longlong, vp, vp, dp, vp, vp],
         "r3d_dist_residual": [ci, ci, ctypes.c_longlong, cd, vp, vp, vp, vp, ci, vp, vp, vp],

@@ -152,6 +152,41 @@ class CudaStages:
         if rc:
             raise RuntimeError(self.lib.r3d_last_error(None).decode())
 
+    def _call_n(self, stage, n, nx, ny, nz, spec, real):
+        import torch
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        rc = self.lib.r3d_slab_transform_sites(self.device, stage, n, nx, ny, nz,
+                                               ctypes.c_void_p(spec.data_ptr()),
+                                               ctypes.c_void_p(real.data_ptr())
+                                               if real is not None else None, ctypes.c_void_p(s))
+        if rc:
+            raise RuntimeError(self.lib.r3d_last_error(None).decode())
+
+    # every site at once: [site][...] tensors, one call per stage
+    def forward_xy_all(self, real):
+        import torch
+        n, nzl, ny, nx = real.shape
+        spec = torch.empty((n, nzl, ny, nx // 2, 2), dtype=torch.float64, device=real.device)
+        self._call_n(0, n, nx, ny, nzl, spec, real.contiguous())
+        return spec
+
+    def forward_z_all(self, spec):
+        n, nz, nyl, hx, _ = spec.shape
+        self._call_n(1, n, 2 * hx, nyl, nz, spec, None)
+        return spec
+
+    def inverse_z_all(self, spec):
+        n, nz, nyl, hx, _ = spec.shape
+        self._call_n(2, n, 2 * hx, nyl, nz, spec, None)
+        return spec
+
+    def inverse_xy_all(self, spec):
+        import torch
+        n, nzl, ny, hx, _ = spec.shape
+        real = torch.empty((n, nzl, ny, 2 * hx), dtype=torch.float64, device=spec.device)
+        self._call_n(3, n, 2 * hx, ny, nzl, spec, real)
+        return real
+
     def forward_xy(self, real):
         import torch
         nzl, ny, nx = real.shape
@@ -437,11 +472,17 @@ class DistSolve:
         dots summed over ranks (cal_rms.cu:14-26, anderson.cu:81-102)."""
         n, plan, rank, ops = self.n, self.plan, self.rank, self.ops
         g, c = ops.closure_c(self.clos, self.pse_n, self.du, self.t, self.fr, self.qv)
-        spec = ops.stack([ops.forward(c[v], plan, rank, self.stages, self.group)
-                          for v in range(n)])
+        if hasattr(ops, "forward_all"):  # every site per stage call and all-to-all
+            spec = ops.forward_all(c, plan, rank, self.stages, self.group)
+        else:
+            spec = ops.stack([ops.forward(c[v], plan, rank, self.stages, self.group)
+                              for v in range(n)])
         hk = ops.oz(spec, self.chi, self.fk, self.qv)
-        h = ops.stack([ops.inverse(hk[v], plan, rank, self.stages, self.group)
-                       for v in range(n)])
+        if hasattr(ops, "inverse_all"):
+            h = ops.inverse_all(hk, plan, rank, self.stages, self.group)
+        else:
+            h = ops.stack([ops.inverse(hk[v], plan, rank, self.stages, self.group)
+                           for v in range(n)])
         self.r, sums = ops.residual(h, 2.0 / self.N, g, self.rp, dots)
         self.g = g
         tot = ops.allreduce(sums, self.group)
@@ -589,6 +630,34 @@ class CudaOps:
         spec_z = torch.cat([p.view(plan.nzl[rank], plan.nyl[s], plan.hx, 2)
                             for s, p in enumerate(parts)], dim=1).contiguous()
         return stages.inverse_xy(spec_z)
+
+    def forward_all(self, c, plan, rank, stages, group):
+        """Every site's forward transform with one call per stage and one
+        all-to-all: [n][nzl][ny][nx] -> [n][nz][nyl][nx/2][2]."""
+        import torch
+        n = c.shape[0]
+        spec_z = stages.forward_xy_all(c.contiguous())
+        send = torch.cat([spec_z[:, :, plan.yslab(s)].reshape(-1) for s in range(plan.world)])
+        recv = self._a2a(send, [n * k for k in plan.send_counts_z2y(rank)],
+                         [n * k for k in plan.recv_counts_z2y(rank)], group)
+        parts = torch.split(recv, [2 * n * k for k in plan.recv_counts_z2y(rank)])
+        spec_y = torch.cat([p.view(n, plan.nzl[s], plan.nyl[rank], plan.hx, 2)
+                            for s, p in enumerate(parts)], dim=1).contiguous()
+        return stages.forward_z_all(spec_y)
+
+    def inverse_all(self, h, plan, rank, stages, group):
+        """Every site's inverse transform: [n][nz][nyl][nx/2][2] -> its z-slab
+        real grids [n][nzl][ny][nx] (times N/2)."""
+        import torch
+        n = h.shape[0]
+        spec_y = stages.inverse_z_all(h.contiguous())
+        send = torch.cat([spec_y[:, plan.zslab(s)].reshape(-1) for s in range(plan.world)])
+        recv = self._a2a(send, [n * k for k in plan.recv_counts_z2y(rank)],
+                         [n * k for k in plan.send_counts_z2y(rank)], group)
+        parts = torch.split(recv, [2 * n * k for k in plan.send_counts_z2y(rank)])
+        spec_z = torch.cat([p.view(n, plan.nzl[rank], plan.nyl[s], plan.hx, 2)
+                            for s, p in enumerate(parts)], dim=2).contiguous()
+        return stages.inverse_xy_all(spec_z)
 
     @staticmethod
     def stack(xs):

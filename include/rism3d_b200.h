@@ -289,6 +289,11 @@ int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
  * left out; stages 0-1 then 2-3 return the grid times nx ny nz / 2). */
 int r3d_slab_transform(int device, int stage, int nx, int ny, int nz, double *d_spec,
                        double *d_real, void *stream);
+/* The same stages for nsites grids (solvent sites) in one call, each buffer
+ * holding them one after another ([site][slab]); r3d_slab_transform is the
+ * one-site case. */
+int r3d_slab_transform_sites(int device, int stage, int nsites, int nx, int ny, int nz,
+                             double *d_spec, double *d_real, void *stream);
 
 /* One rank's pointwise steps of a solve split over GPUs (slabs.py's DistSolve
  * runs the iteration: these, r3d_slab_transform, NCCL all-to-alls between

@@ -157,6 +157,38 @@ def test_gpu_stages_match_with_two_emulated_ranks():
         np.testing.assert_allclose(back, f[plan.zslab(r)] * f.size / 2, atol=1e-9 * f.size)
 
 
+@pytest.mark.gpu
+def test_gpu_stages_take_every_site_in_one_call():
+    """r3d_slab_transform_sites on three sites, on the slab shapes of one of
+    two ranks (8 of 16 z-planes, 6 of 12 y-rows), equals r3d_slab_transform
+    site by site in each of the four stages."""
+    import torch
+    import rism3d as R
+    nz, ny, nx, n = 16, 12, 32, 3
+    rng = np.random.default_rng(11)
+    cs = slabs.CudaStages(R.lib, 0)
+
+    def close(a, b):
+        np.testing.assert_allclose(a.cpu().numpy(), b.cpu().numpy(),
+                                   atol=1e-12 * float(b.abs().max()))
+
+    real = torch.from_numpy(rng.standard_normal((n, nz // 2, ny, nx))).cuda()
+    allx = cs.forward_xy_all(real)
+    assert allx.shape == (n, nz // 2, ny, nx // 2, 2)
+    for v in range(n):
+        close(allx[v], cs.forward_xy(real[v]))
+    spec = torch.from_numpy(rng.standard_normal((n, nz, ny // 2, nx // 2, 2))).cuda()
+    fz, iz = cs.forward_z_all(spec.clone()), cs.inverse_z_all(spec.clone())
+    for v in range(n):
+        close(fz[v], cs.forward_z(spec[v].clone()))
+        close(iz[v], cs.inverse_z(spec[v].clone()))
+    specx = torch.from_numpy(rng.standard_normal((n, nz // 2, ny, nx // 2, 2))).cuda()
+    back = cs.inverse_xy_all(specx.clone())
+    assert back.shape == (n, nz // 2, ny, nx)
+    for v in range(n):
+        close(back[v], cs.inverse_xy(specx[v].clone()))
+
+
 SOLVE_SCRIPT = r"""
 import json, sys
 import numpy as np
@@ -328,6 +360,18 @@ class TorchCpuStages:  # NumpyStages on torch CPU tensors, complex as [..., 2]
     def inverse_xy(self, spec):
         return torch.from_numpy(self.st.inverse_xy(self._c(spec)).copy())
 
+    def forward_xy_all(self, real):
+        return torch.stack([self.forward_xy(r) for r in real])
+
+    def forward_z_all(self, spec):
+        return torch.stack([self.forward_z(x) for x in spec])
+
+    def inverse_z_all(self, spec):
+        return torch.stack([self.inverse_z(x) for x in spec])
+
+    def inverse_xy_all(self, spec):
+        return torch.stack([self.inverse_xy(x) for x in spec])
+
 
 nz, ny, nx = %(shape)r
 f = np.random.default_rng(3).standard_normal((nz, ny, nx))
@@ -336,9 +380,14 @@ ops = slabs.CudaOps.__new__(slabs.CudaOps)  # its packing and all-to-alls only
 st = TorchCpuStages()
 mine = ops.forward(torch.from_numpy(f[plan.zslab(g.rank)].copy()), plan, g.rank, st, None)
 back = ops.inverse(mine.clone(), plan, g.rank, st, None)
+# two sites at once (the grid and its negative): one all-to-all per direction
+two = torch.from_numpy(np.stack([f[plan.zslab(g.rank)], -f[plan.zslab(g.rank)]]).copy())
+both = ops.forward_all(two, plan, g.rank, st, None)
+back2 = ops.inverse_all(both.clone(), plan, g.rank, st, None)
 with open(%(out)r + str(g.rank) + ".json", "w") as fo:
     json.dump({"y": [plan.y0[g.rank], plan.nyl[g.rank]], "z": [plan.z0[g.rank], plan.nzl[g.rank]],
-               "spec": mine.numpy().tolist(), "back": back.numpy().tolist()}, fo)
+               "spec": mine.numpy().tolist(), "back": back.numpy().tolist(),
+               "both": both.numpy().tolist(), "back2": back2.numpy().tolist()}, fo)
 g.close()
 """
 
@@ -367,3 +416,10 @@ def test_cuda_ops_packing_on_two_gloo_ranks(tmp_path):
                                    atol=1e-9 * np.abs(raw).max())
         np.testing.assert_allclose(np.array(res["back"]), f[z0:z0 + nzl] * f.size / 2,
                                    atol=1e-8 * f.size)
+        both = np.array(res["both"])
+        for k, sign in enumerate((1.0, -1.0)):
+            np.testing.assert_allclose(both[k, ..., 0] + 1j * both[k, ..., 1],
+                                       sign * raw[:, y0:y0 + nyl, :],
+                                       atol=1e-9 * np.abs(raw).max())
+            np.testing.assert_allclose(np.array(res["back2"])[k],
+                                       sign * f[z0:z0 + nzl] * f.size / 2, atol=1e-8 * f.size)
