@@ -885,11 +885,38 @@ def run_split(args, group):
               dev(np.stack([fkt.real, fkt.imag], -1)[:, ys]))
     del du, t0, fr, fkt, chi
 
-    def run(k):  # k evaluations (tolerance 0: none stops early)
+    class PhaseOps:
+        """CudaOps with CUDA events around each step, summed per step name
+        (the untimed breakdown run only)."""
+
+        def __init__(self, inner):
+            self.inner, self.ev = inner, []
+
+        def __getattr__(self, name):
+            f = getattr(self.inner, name)
+            if not callable(f):
+                return f
+
+            def timed(*a, **kw):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                out = f(*a, **kw)
+                e1.record()
+                self.ev.append((name, e0, e1))
+                return out
+            return timed
+
+        def totals(self):
+            tot = {}
+            for name, e0, e1 in self.ev:
+                tot[name] = tot.get(name, 0.0) + e0.elapsed_time(e1)
+            return tot
+
+    def run(k, ops=None):  # k evaluations (tolerance 0: none stops early)
         ds = slabs.DistSolve(plan, rank, *[a.clone() for a in arrays], qv, rhov,
                              closure=(slabs.KH, 1), mixer=(2, 0.6, 0.2), tol=0.0, maxstep=k,
-                             stages=slabs.CudaStages(R.lib, local), ops=slabs.CudaOps(R.lib, local),
-                             group=None)
+                             stages=slabs.CudaStages(R.lib, local),
+                             ops=ops or slabs.CudaOps(R.lib, local), group=None)
         torch.cuda.synchronize(local)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -902,6 +929,11 @@ def run_split(args, group):
     group.barrier()
     ms, steps = run(args.steps)
     ms = group.allmax(ms)
+    # where a step's time goes: the same steps again, each op between events
+    po = PhaseOps(slabs.CudaOps(R.lib, local))
+    pms, psteps = run(args.steps, po)
+    phases = {k: v / psteps for k, v in sorted(po.totals().items())}
+    phases["host and other"] = pms / psteps - sum(phases.values())
     shutil.rmtree(tmp, ignore_errors=True)
     if rank == 0:
         n = len(qv)
@@ -913,7 +945,11 @@ def run_split(args, group):
             "scaling": "strong", "dtype": "f64", "data": "synthetic (seeded 2000-atom globule)",
             "config": {"workload": WORKLOAD + " (FP64, AN2), one solve split over the ranks",
                        "grid": nx, "sites": n, "slabs": world},
-            "nvlink_bytes_per_rank_per_step": a2a}), flush=True)
+            "nvlink_bytes_per_rank_per_step": a2a,
+            "phases_ms_per_step": {"rank0": phases,
+                                   "note": "a second run of the same steps with CUDA events "
+                                           "around each op of slabs.CudaOps (not the timed run)"}}),
+              flush=True)
 
 
 # ------------------------------------------------------- reference arm
