@@ -289,9 +289,11 @@ int r3d_fft3d_noalloc(int device, int nx, int ny, int nz, const double *box,
  * left out; stages 0-1 then 2-3 return the grid times nx ny nz / 2). */
 int r3d_slab_transform(int device, int stage, int nx, int ny, int nz, double *d_spec,
                        double *d_real, void *stream);
-/* The same stages for nsites grids (solvent sites) in one call, each buffer
- * holding them one after another ([site][slab]); r3d_slab_transform is the
- * one-site case. */
+/* The same stages for nsites grids (solvent sites, 1 <= nsites <= 16) in one
+ * call, each buffer holding them one after another ([site][slab]);
+ * r3d_slab_transform is the one-site case.  A site count outside that range,
+ * or slabs whose tiles for every site do not fit one CTA's shared memory, is
+ * R3D_EINVAL. */
 int r3d_slab_transform_sites(int device, int stage, int nsites, int nx, int ny, int nz,
                              double *d_spec, double *d_real, void *stream);
 

@@ -78,8 +78,8 @@ def test_bad_inputs_are_errors_not_exits(R, tmp_path, solvents):
 
 
 def test_split_solve_steps_reject_bad_arguments(R):
-    """The split solve's per-rank steps (r3d_dist_*) check their arguments on
-    the host, before any device work: too many sites, empty slabs, missing
+    """The split solve's per-rank steps (r3d_dist_* and the slab stages) check
+    their arguments on the host, before any device work: too many sites, empty slabs, missing
     buffers, an unknown closure and a slot other than 0 / 1 are R3D_EINVAL
     with a message (no GPU needed)."""
     import ctypes
@@ -95,6 +95,13 @@ def test_split_solve_steps_reject_bad_arguments(R):
     assert lib.r3d_dist_residual(0, 2, 8, 1.0, buf, buf, None, None, 1, buf, buf, None) == EINVAL
     assert lib.r3d_dist_mix(0, 8, buf, buf, buf, buf, buf, buf, 2, 0, 0.0, 0.0, 0.5, None) == EINVAL
     assert b"r3d_dist" in lib.r3d_last_error(None)
+    # the slab stages: a site count outside 1..16, an unknown stage, an odd x
+    # extent and a missing real buffer are rejected before any device work
+    assert lib.r3d_slab_transform_sites(0, 0, 0, 32, 12, 8, buf, buf, None) == EINVAL
+    assert lib.r3d_slab_transform_sites(0, 0, 17, 32, 12, 8, buf, buf, None) == EINVAL
+    assert lib.r3d_slab_transform_sites(0, 4, 2, 32, 12, 8, buf, buf, None) == EINVAL
+    assert lib.r3d_slab_transform_sites(0, 1, 2, 31, 12, 8, buf, None, None) == EINVAL
+    assert lib.r3d_slab_transform_sites(0, 3, 2, 32, 12, 8, buf, None, None) == EINVAL
 
 
 def test_solvent_sites_match_the_oracle(R, refcase):
